@@ -1,0 +1,288 @@
+"""Throughput of the HyQMOM explicit step on B200: cell-steps/s.
+
+A "step" is one time step of simulation_runner over the whole grid.  Default
+workload: crossing jets 160 x 160 x 80 (2,048,000 cells, 573 MB of FP64
+state), Ma=1, Kn=1, CFL=0.7, plain eigen-solve.  The state (573 MB) and the
+flux buffers exceed L2 (126 MB), so no L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU: independent replicas (one domain per rank, no data-path
+collective); value = all ranks' cell-steps / max-over-ranks time.
+--impl reference: the CPU restatement of the reference's step (the oracle,
+OpenMP on all host cores) on bounded samples of the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hyqmom.jl_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "cell-steps/s on 1 B200: plain eig vs learned warm-start, <=1e-8 rel vs FP64 ref"
+UNIT = "cell-steps/s"
+
+# FP64 operations per cell-step of the plain path (oracle op counter, +,-,*,/
+# and sqrt/cbrt/exp counted 1 each), crossing jets 160x160x80 Ma=1 Kn=1, first
+# step, averaged over a 160x160x8 slab through the jets; recomputed by
+# `python bench.py --count-ops`.
+F_ALG = 201144.5
+B_ALG = 2 * 35 * 8  # bytes per cell-step: state read once, written once
+
+
+def workload(name="c2"):
+    from hyqmom import ic
+    if name == "c2":
+        p = ic.default_params(Nx=160, Ny=160, Nz=80, Ma=1.0, Kn=1.0, CFL=0.7, tmax=1e9, nnmax=200)
+    elif name == "c5":
+        p = ic.default_params(Nx=256, Ny=256, Nz=128, Ma=1.0, Kn=0.01, CFL=0.7, tmax=1e9, nnmax=500)
+    elif name == "c1":
+        p = ic.default_params(Nx=20, Ny=20, Nz=20, Ma=0.0, Kn=1.0, CFL=0.7, tmax=1e9, nnmax=100)
+    else:
+        raise ValueError(name)
+    return ic.with_jets(p, "crossing")
+
+
+def sample_slab(p, nz=8):
+    """A bounded sample of the workload: an nz-layer z-slab through the jets."""
+    from hyqmom import ic
+    M = ic.initial_state(p)
+    z0 = p["Nz"] // 2 - nz // 2
+    return np.asfortranarray(M[:, :, z0:z0 + nz, :])
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self._stop = index, [], threading.Event()
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in self.rows for q in range(4) if len(r) > 3 + q and "Active" in r[3 + q]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def fp64_peak_tflops(torch):
+    """Measured FP64 FMA throughput of this GPU (dense double matmul: the
+    non-tensor FP64 ceiling of B200 is the same DFMA pipe cuBLAS DGEMM uses)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def cpu_baseline(p, seconds=15.0):
+    """The oracle (CPU restatement, OpenMP, all host threads) on a slab sample."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    from hyqmom import ic
+    M = sample_slab(p, nz=8)
+    q = dict(p, Nz=M.shape[2], **ic.grid_spacing(p))
+    cells = M.shape[0] * M.shape[1] * M.shape[2]
+    t0 = time.perf_counter()
+    steps, t = 0, 0.0
+    while True:
+        _, t, _ = ol.step(M, q, t)
+        steps += 1
+        if time.perf_counter() - t0 > seconds or steps >= 3:
+            break
+    el = time.perf_counter() - t0
+    return {"value": cells * steps / el, "unit": UNIT, "cores": int(ol.load().hyqo_num_threads()), "kind": "port",
+            "sample": f"{steps} step(s) of a {M.shape[0]}x{M.shape[1]}x{M.shape[2]} z-slab through the jets of the "
+                      f"same IC ({cells} cells), oracle C++ restatement, OpenMP"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    p = workload(args.config)
+    base = cpu_baseline(p, seconds=20.0)
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (reference crossing-jets IC generator)",
+            "config": {"workload": f"crossing jets {p['Nx']}x{p['Ny']}x{p['Nz']} Ma={p['Ma']} Kn={p['Kn']} CFL={p['CFL']}",
+                       "sample": base["sample"]},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference Julia CPU path unavailable (no julia in the image); timed: the oracle restatement"}
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    torch.cuda.set_device(local_rank)
+    from hyqmom import ic
+    from hyqmom.runner import Solver
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    p = workload(args.config)
+    cells = p["Nx"] * p["Ny"] * p["Nz"]
+    M0 = ic.initial_state(p)
+    s = Solver(p, device=local_rank)
+    stream = torch.cuda.ExternalStream(s.stream)
+    s.set_state(M0)
+    s.advance(args.warmup)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    barrier()
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.advance_async(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+    ms = e0.elapsed_time(e1)
+    st = s.stats()
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * cells * args.steps / (ms * 1e-3)
+
+    # per-kernel device time (individual launches, same stream)
+    s.set_state(M0)
+    s.advance(args.warmup)
+    import ctypes
+    kms = (ctypes.c_float * 4)()
+    ksteps = max(1, min(args.steps, 3))
+    s._chk(s._lib.hyq_advance_timed(s._h, ksteps, kms))
+    kern = {"phase_A": kms[0] / ksteps, "cfl": kms[1] / ksteps, "hll": kms[2] / ksteps, "phase_EF": kms[3] / ksteps}
+
+    # end to end through the public API: pinned host state in, one step, state out
+    Mh = torch.from_numpy(np.ascontiguousarray(M0.reshape(-1, order="F"))).pin_memory()
+    Mo = torch.empty_like(Mh).pin_memory()
+    s.set_state(M0)
+    s.advance(1)
+    e2e_steps = max(1, min(args.steps, 5))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tt, nn = 0.0, 0
+    for _ in range(e2e_steps):
+        s._chk(s._lib.hyq_set_state(s._h, ctypes.c_void_p(Mh.data_ptr())))
+        s.set_clock(tt, nn)
+        tt, nn, _ = s.advance(1)
+        s._chk(s._lib.hyq_get_state(s._h, ctypes.c_void_p(Mo.data_ptr())))
+    e2e_s = time.perf_counter() - t0
+    e2e = {"value": world * cells * e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": Mh.numel() * 8,
+           "d2h_bytes_per_step": Mo.numel() * 8}
+    s.close()
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    fp64 = fp64_peak_tflops(torch)
+    falg = F_ALG
+    a_ms = kern["phase_A"] + kern["phase_EF"]
+    achieved = (falg * cells / (ms / args.steps * 1e-3) / 1e12) if falg else None
+    roof = {"bound": "fp64", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
+            "frac": (achieved / fp64) if (achieved and fp64) else None, "traffic": None,
+            "peak_source": "measured in this run: FP64 DGEMM 8192^3 (cuBLAS via torch), best of 3",
+            "dominant_kernel": "k_phase_A", "kernel_ms": kern,
+            "hbm_achieved_gbs": B_ALG * cells / (ms / args.steps * 1e-3) / 1e9}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (reference crossing-jets IC generator)",
+            "config": {"workload": f"crossing jets {p['Nx']}x{p['Ny']}x{p['Nz']} Ma={p['Ma']} Kn={p['Kn']} CFL={p['CFL']}, plain eig",
+                       "cells": cells, "parallelism": f"replicas x{world}", "l2": "state 573 MB > L2, no flush needed",
+                       "steps_done": st["nn"]},
+            "gpu_launches": 4 * args.steps, "e2e": e2e, "roofline": roof, "clocks": sampler.summary()}
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(p, seconds=15.0)
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def count_ops():
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as ol
+    from hyqmom import ic
+    p = workload("c2")
+    M = sample_slab(p, nz=8)
+    q = dict(p, Nz=M.shape[2], **ic.grid_spacing(p))
+    cells = M.shape[0] * M.shape[1] * M.shape[2]
+    dt = 1e-3
+    out = ol.count_ops(M, q, dt)
+    per = (out[0] + out[1]) / cells + out[2]
+    print(json.dumps({"cells": cells, "phase_A_ops_per_cell": out[0] / cells, "phase_EF_ops_per_cell": out[1] / cells,
+                      "hll_ops_per_cell": out[2], "F_alg": per}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c5"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--count-ops", action="store_true")
+    args = ap.parse_args()
+    if args.count_ops:
+        return count_ops()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    run_gpu(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

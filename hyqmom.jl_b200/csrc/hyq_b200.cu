@@ -1,0 +1,398 @@
+// libhyqmom_b200.so: kernels and C-ABI of the HyQMOM explicit step on B200.
+//
+// One step = four launches on the context stream, captured once in a CUDA
+// graph and replayed:
+//   k_phase_A    per cell: closure + realizability, x/y/z flux-Jacobian
+//                eigenvalues, closure of the realized moments, 1-D closure
+//                speeds; writes Fx, Fy, Fz, the realized state and 6 speeds,
+//                and a NaN-propagating per-block max |speed|
+//                (src/simulation_runner.jl:352-383)
+//   k_cfl        one block: global max -> dt, t += dt, nn += 1 on the device
+//                (src/simulation_runner.jl:402-433, 496)
+//   k_hll        per (cell, moment): x, y, z HLL updates with pas_HLL's copy
+//                boundary handling, combined as Mx + My + Mz - 2M
+//                (src/numerics/apply_flux_update_3d.jl:30-213,
+//                 src/numerics/pas_HLL.jl:238-298, flux_HLL.jl:318-330,
+//                 src/simulation_runner.jl:498-520)
+//   k_phase_EF   per cell: realizability pass and BGK collision
+//                (src/simulation_runner.jl:526-557)
+// The loop predicate `t < tmax && nn < nnmax` is evaluated on the device, so
+// any number of steps can be queued without a host round trip.
+//
+// State: moment-major SoA, M[c + N*n], c = i + Nx*(j + Ny*k) (Julia order).
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstring>
+#include <cstdlib>
+#include <string>
+#include "hyq_cell.cuh"
+#include "hyq_step.cuh"
+#include "../../include/hyqmom.h"
+
+using namespace hyq;
+using namespace hyqk;
+
+namespace {
+
+__global__ void __launch_bounds__(1024) k_cfl(const double* __restrict__ blockmax, const StepConst sc, DevClock* clk) {
+  const bool active = (clk->t < sc.tmax) && (clk->nn < sc.nnmax);
+  __syncthreads();
+  if (!active) {
+    if (threadIdx.x == 0) clk->active = 0;
+    return;
+  }
+  double v = 0.0;
+  for (int b = threadIdx.x; b < sc.nblocksA; b += 1024) v = nanmax(v, blockmax[b]);
+  const double vmax = block_nanmax<1024>(v);
+  if (threadIdx.x == 0) {
+    double dt = jmin(sc.CFL * jmin(jmin(sc.dx, sc.dy), sc.dz) / vmax, jmin(sc.dtmax, sc.Kn));
+    dt = jmin(dt, sc.tmax - clk->t);
+    clk->vmax = vmax;
+    clk->dt = dt;
+    clk->t = clk->t + dt;
+    clk->nn = clk->nn + 1;
+    clk->active = 1;
+  }
+}
+
+// One directional HLL update of moment n of cell (i) along a line of Np
+// cells with stride `st`, at cell offset c0 of the line start.
+__device__ __forceinline__ double hll_line(const double* __restrict__ M, const double* __restrict__ F, const double* __restrict__ vmin,
+                                           const double* __restrict__ vmax, long long base, long long st, int Np, int i, double r) {
+  if (Np == 2) return M[base + st];  // pas_HLL with Np = 2 returns [M2, M2]
+  const int ip = i < 1 ? 1 : (i > Np - 2 ? Np - 2 : i);
+  // face j between cells j and j+1; Flux_j for j = ip-1 and ip
+  auto wface = [&](int j, double& ll, double& lr, double& ws) {
+    // W* at face j (j in 1..Np-2); j == 0 uses W*[1] with zero speeds
+    const int jj = j < 1 ? 1 : j;
+    const double a = vmin[base + st * jj], b = vmin[base + st * (jj + 1)];
+    const double c = vmax[base + st * jj], d = vmax[base + st * (jj + 1)];
+    const double l1 = jmin(a, b), l2 = jmax(c, d);
+    double w = 0.0;
+    if (fabs(l1 - l2) > 1e-10) {
+      const double mj = M[base + st * jj], mj1 = M[base + st * (jj + 1)];
+      const double fj = F[base + st * jj], fj1 = F[base + st * (jj + 1)];
+      w = (l1 * mj - l2 * mj1) / (l1 - l2) - (fj - fj1) / (l1 - l2);
+    }
+    ws = w;
+    if (j == 0) { ll = 0.0; lr = 0.0; } else { ll = l1; lr = l2; }
+  };
+  auto flux = [&](int j) {
+    double ll, lr, ws;
+    wface(j, ll, lr, ws);
+    // boundary-modified fluxes: F[0] := F[1], F[Np-1] := F[Np-2]
+    const int fa = j < 1 ? 1 : j;
+    const int fb = (j + 1 > Np - 2) ? Np - 2 : j + 1;
+    const double Fa = F[base + st * fa], Fb = F[base + st * fb];
+    const double Ma_ = M[base + st * j], Mb = M[base + st * (j + 1)];
+    return 0.5 * (Fa + Fb) - 0.5 * (fabs(ll) * (ws - Ma_) - fabs(lr) * (ws - Mb));
+  };
+  const double f1 = flux(ip), f0 = flux(ip - 1);
+  return M[base + st * ip] - r * (f1 - f0);
+}
+
+__global__ void __launch_bounds__(BS_HLL) k_hll(const double* __restrict__ M, const double* __restrict__ Fx, const double* __restrict__ Fy,
+                                                 const double* __restrict__ Fz, const double* __restrict__ vp, double* __restrict__ Mout,
+                                                 const StepConst sc, const DevClock* clk) {
+  if (!clk->active) return;
+  const long long N = sc.N;
+  const long long c = (long long)blockIdx.x * BS_HLL + threadIdx.x;
+  const int n = blockIdx.y;
+  if (c >= N) return;
+  const double dt = clk->dt;
+  const int Nx = sc.Nx, Ny = sc.Ny, Nz = sc.Nz;
+  const int i = int(c % Nx);
+  const int j = int((c / Nx) % Ny);
+  const int k = int(c / ((long long)Nx * Ny));
+  const long long mo = N * n;
+  const double* Mn = M + mo;
+  // x: line base at (0, j, k), stride 1
+  const double mx = hll_line(Mn, Fx + mo, vp, vp + N, c - i, 1, Nx, i, dt / sc.dx);
+  const double my = hll_line(Mn, Fy + mo, vp + 2 * N, vp + 3 * N, c - (long long)j * Nx, Nx, Ny, j, dt / sc.dy);
+  const double mz = (Nz == 1) ? Mn[c] : hll_line(Mn, Fz + mo, vp + 4 * N, vp + 5 * N, c - (long long)k * Nx * Ny, (long long)Nx * Ny, Nz, k, dt / sc.dz);
+  Mout[c + mo] = mx + my + mz - 2.0 * Mn[c];
+}
+
+__global__ void k_set_clock(DevClock* clk, double t, long long nn) {
+  clk->t = t; clk->nn = nn; clk->dt = 0.0; clk->vmax = 0.0; clk->active = 0; clk->status = 0;
+}
+
+
+}  // namespace
+
+// ------------------------------------------------------------------ C-ABI
+struct hyq_ctx {
+  hyq_params p;
+  StepConst sc;
+  long long N;
+  int device;
+  double *M = nullptr, *Mtmp = nullptr, *Fx = nullptr, *Fy = nullptr, *Fz = nullptr, *vp = nullptr, *blockmax = nullptr;
+  DevClock* clk = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::string err;
+};
+
+namespace {
+thread_local std::string g_err;
+
+int fail(hyq_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg; else g_err = msg;
+  return code;
+}
+int cuda_fail(hyq_ctx* ctx, cudaError_t e, const char* what) {
+  return fail(ctx, HYQ_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define HQ_CHECK(ctx, call)                                       \
+  do {                                                            \
+    cudaError_t e_ = (call);                                      \
+    if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call);    \
+  } while (0)
+
+
+void enqueue_step(hyq_ctx* ctx, cudaStream_t s) {
+  const long long N = ctx->N;
+  launch_phase_A(ctx->sc, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s);
+  k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
+  dim3 gh(grid_of(N, BS_HLL), 35);
+  k_hll<<<gh, BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
+  launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->clk, s);
+}
+}  // namespace
+
+extern "C" {
+
+int hyq_abi_version(void) { return HYQ_ABI_VERSION; }
+
+const char* hyq_last_error(const hyq_ctx* ctx) { return ctx ? ctx->err.c_str() : g_err.c_str(); }
+
+int hyq_create(const hyq_params* p, hyq_ctx** out) {
+  if (!p || !out) return fail(nullptr, HYQ_EINVAL, "null argument");
+  *out = nullptr;
+  if (p->Nx < 2 || p->Ny < 2 || p->Nz < 1)
+    return fail(nullptr, HYQ_EINVAL, "grid must have Nx >= 2, Ny >= 2, Nz >= 1 (pas_HLL needs two cells per row)");
+  if (!(p->CFL > 0) || !(p->Kn > 0) || !(p->dtmax > 0))
+    return fail(nullptr, HYQ_EINVAL, "CFL, Kn and dtmax must be positive");
+  hyq_ctx* ctx = new hyq_ctx();
+  ctx->p = *p;
+  ctx->device = p->device;
+  cudaError_t e = cudaSetDevice(p->device);
+  if (e != cudaSuccess) { int r = cuda_fail(nullptr, e, "cudaSetDevice"); delete ctx; return r; }
+  const long long N = (long long)p->Nx * p->Ny * p->Nz;
+  ctx->N = N;
+  StepConst& sc = ctx->sc;
+  sc.N = N; sc.Nx = p->Nx; sc.Ny = p->Ny; sc.Nz = p->Nz; sc.flag2D = p->flag2D; sc.positivity = p->positivity;
+  sc.nnmax = p->nnmax; sc.tmax = p->tmax; sc.Kn = p->Kn; sc.Ma = p->Ma; sc.CFL = p->CFL; sc.dtmax = p->dtmax;
+  sc.dx = (p->xmax - p->xmin) / p->Nx; sc.dy = (p->ymax - p->ymin) / p->Ny; sc.dz = (p->zmax - p->zmin) / p->Nz;
+  sc.nblocksA = grid_of(N, BS_A);
+  const size_t b35 = sizeof(double) * 35 * (size_t)N;
+  auto alloc = [&](double** ptr, size_t bytes) { return cudaMalloc((void**)ptr, bytes); };
+  if (alloc(&ctx->M, b35) != cudaSuccess || alloc(&ctx->Mtmp, b35) != cudaSuccess || alloc(&ctx->Fx, b35) != cudaSuccess ||
+      alloc(&ctx->Fy, b35) != cudaSuccess || alloc(&ctx->Fz, b35) != cudaSuccess ||
+      alloc(&ctx->vp, sizeof(double) * 6 * (size_t)N) != cudaSuccess ||
+      alloc(&ctx->blockmax, sizeof(double) * (size_t)sc.nblocksA) != cudaSuccess ||
+      cudaMalloc((void**)&ctx->clk, sizeof(DevClock)) != cudaSuccess) {
+    cudaGetLastError();
+    hyq_destroy(ctx);
+    return fail(nullptr, HYQ_ENOMEM, "device allocation failed");
+  }
+  if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    int r = cuda_fail(nullptr, e, "cudaStreamCreate");
+    hyq_destroy(ctx);
+    return r;
+  }
+  k_set_clock<<<1, 1, 0, ctx->stream>>>(ctx->clk, 0.0, 0);
+  // capture one step as a graph
+  if ((e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+    int r = cuda_fail(nullptr, e, "cudaStreamBeginCapture"); hyq_destroy(ctx); return r;
+  }
+  enqueue_step(ctx, ctx->stream);
+  if ((e = cudaStreamEndCapture(ctx->stream, &ctx->graph)) != cudaSuccess) {
+    int r = cuda_fail(nullptr, e, "cudaStreamEndCapture"); hyq_destroy(ctx); return r;
+  }
+  if ((e = cudaGraphInstantiate(&ctx->exec, ctx->graph, 0)) != cudaSuccess) {
+    int r = cuda_fail(nullptr, e, "cudaGraphInstantiate"); hyq_destroy(ctx); return r;
+  }
+  if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) {
+    int r = cuda_fail(nullptr, e, "create sync"); hyq_destroy(ctx); return r;
+  }
+  *out = ctx;
+  return HYQ_OK;
+}
+
+void hyq_destroy(hyq_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->exec) cudaGraphExecDestroy(ctx->exec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  double* bufs[] = {ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax};
+  for (double* b : bufs) if (b) cudaFree(b);
+  if (ctx->clk) cudaFree(ctx->clk);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+void* hyq_stream(hyq_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int hyq_set_clock(hyq_ctx* ctx, double t, int64_t nn) {
+  if (!ctx) return fail(nullptr, HYQ_EINVAL, "null ctx");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  k_set_clock<<<1, 1, 0, ctx->stream>>>(ctx->clk, t, (long long)nn);
+  HQ_CHECK(ctx, cudaGetLastError());
+  return HYQ_OK;
+}
+
+int hyq_set_state(hyq_ctx* ctx, const double* M) {
+  if (!ctx || !M) return fail(ctx, HYQ_EINVAL, "null argument");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  HQ_CHECK(ctx, cudaMemcpyAsync(ctx->M, M, sizeof(double) * 35 * ctx->N, cudaMemcpyHostToDevice, ctx->stream));
+  k_set_clock<<<1, 1, 0, ctx->stream>>>(ctx->clk, 0.0, 0);
+  HQ_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  return HYQ_OK;
+}
+
+int hyq_set_state_device(hyq_ctx* ctx, const double* dM) {
+  if (!ctx || !dM) return fail(ctx, HYQ_EINVAL, "null argument");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  HQ_CHECK(ctx, cudaMemcpyAsync(ctx->M, dM, sizeof(double) * 35 * ctx->N, cudaMemcpyDeviceToDevice, ctx->stream));
+  k_set_clock<<<1, 1, 0, ctx->stream>>>(ctx->clk, 0.0, 0);
+  HQ_CHECK(ctx, cudaGetLastError());
+  return HYQ_OK;
+}
+
+int hyq_get_state(hyq_ctx* ctx, double* M) {
+  if (!ctx || !M) return fail(ctx, HYQ_EINVAL, "null argument");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  HQ_CHECK(ctx, cudaMemcpyAsync(M, ctx->M, sizeof(double) * 35 * ctx->N, cudaMemcpyDeviceToHost, ctx->stream));
+  HQ_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  return HYQ_OK;
+}
+
+int hyq_get_state_device(hyq_ctx* ctx, double* dM) {
+  if (!ctx || !dM) return fail(ctx, HYQ_EINVAL, "null argument");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  HQ_CHECK(ctx, cudaMemcpyAsync(dM, ctx->M, sizeof(double) * 35 * ctx->N, cudaMemcpyDeviceToDevice, ctx->stream));
+  return HYQ_OK;
+}
+
+int hyq_advance_async(hyq_ctx* ctx, int64_t max_steps) {
+  if (!ctx || max_steps < 0) return fail(ctx, HYQ_EINVAL, "bad argument");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  for (int64_t s = 0; s < max_steps; ++s) HQ_CHECK(ctx, cudaGraphLaunch(ctx->exec, ctx->stream));
+  return HYQ_OK;
+}
+
+int hyq_advance_timed(hyq_ctx* ctx, int64_t steps, float* ms) {
+  if (!ctx || !ms || steps < 0) return fail(ctx, HYQ_EINVAL, "bad argument");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  cudaEvent_t ev[5];
+  for (int q = 0; q < 5; ++q) HQ_CHECK(ctx, cudaEventCreate(&ev[q]));
+  for (int q = 0; q < 4; ++q) ms[q] = 0.0f;
+  const long long N = ctx->N;
+  cudaStream_t s = ctx->stream;
+  for (int64_t it = 0; it < steps; ++it) {
+    cudaEventRecord(ev[0], s);
+    launch_phase_A(ctx->sc, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s);
+    cudaEventRecord(ev[1], s);
+    k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
+    cudaEventRecord(ev[2], s);
+    k_hll<<<dim3(grid_of(N, BS_HLL), 35), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
+    cudaEventRecord(ev[3], s);
+    launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->clk, s);
+    cudaEventRecord(ev[4], s);
+    HQ_CHECK(ctx, cudaEventSynchronize(ev[4]));
+    for (int q = 0; q < 4; ++q) {
+      float t = 0.0f;
+      cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
+      ms[q] += t;
+    }
+  }
+  for (int q = 0; q < 5; ++q) cudaEventDestroy(ev[q]);
+  HQ_CHECK(ctx, cudaGetLastError());
+  return HYQ_OK;
+}
+
+int hyq_synchronize(hyq_ctx* ctx) {
+  if (!ctx) return fail(nullptr, HYQ_EINVAL, "null ctx");
+  HQ_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  return HYQ_OK;
+}
+
+int hyq_stats_get(hyq_ctx* ctx, hyq_stats* out) {
+  if (!ctx || !out) return fail(ctx, HYQ_EINVAL, "null argument");
+  DevClock h;
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  HQ_CHECK(ctx, cudaMemcpyAsync(&h, ctx->clk, sizeof(DevClock), cudaMemcpyDeviceToHost, ctx->stream));
+  HQ_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  out->t = h.t; out->dt = h.dt; out->vmax = h.vmax; out->nn = h.nn; out->status = h.status;
+  out->done = (h.t < ctx->p.tmax && h.nn < ctx->p.nnmax) ? 0 : 1;
+  return HYQ_OK;
+}
+
+int hyq_advance(hyq_ctx* ctx, int64_t max_steps, double* t, int64_t* nn, int32_t* done) {
+  int r = hyq_advance_async(ctx, max_steps);
+  if (r) return r;
+  hyq_stats st;
+  r = hyq_stats_get(ctx, &st);
+  if (r) return r;
+  if (t) *t = st.t;
+  if (nn) *nn = st.nn;
+  if (done) *done = st.done;
+  return HYQ_OK;
+}
+
+int hyq_get_SC(hyq_ctx* ctx, double* S, double* C) {
+  if (!ctx) return fail(nullptr, HYQ_EINVAL, "null ctx");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  const size_t b = sizeof(double) * 35 * ctx->N;
+  // Fx/Fy are scratch between steps: reuse them for S and C
+  launch_std_central(ctx->M, ctx->N, ctx->Fx, ctx->Fy, ctx->stream);
+  HQ_CHECK(ctx, cudaGetLastError());
+  if (S) HQ_CHECK(ctx, cudaMemcpyAsync(S, ctx->Fx, b, cudaMemcpyDeviceToHost, ctx->stream));
+  if (C) HQ_CHECK(ctx, cudaMemcpyAsync(C, ctx->Fy, b, cudaMemcpyDeviceToHost, ctx->stream));
+  HQ_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  return HYQ_OK;
+}
+
+#define CELLS_LAUNCH_CHECK()                                    \
+  do {                                                          \
+    cudaError_t e_ = cudaGetLastError();                        \
+    if (e_ != cudaSuccess) return cuda_fail(nullptr, e_, "launch"); \
+  } while (0)
+
+int hyq_cells_flux_closure(const double* M, int64_t n, int32_t flag2D, double Ma, double* Fx, double* Fy, double* Fz, double* Mr, void* stream) {
+  if (!M || n <= 0) return fail(nullptr, HYQ_EINVAL, "bad argument");
+  launch_cells_flux(M, n, flag2D, Ma, Fx, Fy, Fz, Mr, (cudaStream_t)stream);
+  CELLS_LAUNCH_CHECK();
+  return HYQ_OK;
+}
+int hyq_cells_eigenvalues(const double* M, int64_t n, int32_t axis, int32_t flag2D, double Ma, int32_t positivity, double* v, double* Mr,
+                          void* stream) {
+  if (!M || !v || !Mr || n <= 0 || axis < 1 || axis > 3) return fail(nullptr, HYQ_EINVAL, "bad argument");
+  launch_cells_eig(M, n, axis, flag2D, Ma, positivity, v, Mr, (cudaStream_t)stream);
+  CELLS_LAUNCH_CHECK();
+  return HYQ_OK;
+}
+int hyq_cells_closure_eigs(const double* mom, int64_t n, double* v, void* stream) {
+  if (!mom || !v || n <= 0) return fail(nullptr, HYQ_EINVAL, "bad argument");
+  launch_cells_closure_eigs(mom, n, v, (cudaStream_t)stream);
+  CELLS_LAUNCH_CHECK();
+  return HYQ_OK;
+}
+int hyq_cells_collision(const double* M, int64_t n, double dt, double Kn, int32_t positivity, double* out, void* stream) {
+  if (!M || !out || n <= 0) return fail(nullptr, HYQ_EINVAL, "bad argument");
+  launch_cells_collision(M, n, dt, Kn, positivity, out, (cudaStream_t)stream);
+  CELLS_LAUNCH_CHECK();
+  return HYQ_OK;
+}
+int hyq_cells_phase_A(const double* M, int64_t n, int32_t flag2D, double Ma, int32_t positivity, double* Fx, double* Fy, double* Fz, double* Mr,
+                      double* vp, void* stream) {
+  if (!M || !Fx || !Fy || !Fz || !Mr || !vp || n <= 0) return fail(nullptr, HYQ_EINVAL, "bad argument");
+  launch_cells_phase_A(M, n, flag2D, Ma, positivity, Fx, Fy, Fz, Mr, vp, (cudaStream_t)stream);
+  CELLS_LAUNCH_CHECK();
+  return HYQ_OK;
+}
+
+}  // extern "C"

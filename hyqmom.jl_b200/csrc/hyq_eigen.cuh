@@ -1,0 +1,653 @@
+// Wave speeds and BGK relaxation (device code): jacobian6, the LAPACK-path
+// nonsymmetric eigenvalue solve, eigenvalues6_hyperbolic_3D (x, y),
+// eigenvalues6z_hyperbolic_3D, closure_and_eigenvalues and collision35.
+// Restates src/numerics/{eigenvalues6_hyperbolic_3D.jl:22-252,
+// eigenvalues6z_hyperbolic_3D.jl:23-365, compute_jacobian_eigenvalues.jl:18-50,
+// closure_and_eigenvalues.jl:76-137, collision35.jl:154-182},
+// src/utils/axis_moment_slice.jl:31-54 and src/autogen/jacobian6.jl:14-59.
+#pragma once
+#include "hyq_closure.cuh"
+
+namespace hyq {
+
+// ------------------------------------------------------------ jacobian6
+// Dual number with 6 derivative components (forward differentiation with
+// respect to W = (m02, m12, m22, m03, m13, m04)).
+struct Dual {
+  double v, d[6];
+};
+HQD Dual dconst(double x) { Dual r; r.v = x;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) r.d[i] = 0.0; return r; }
+HQD Dual operator+(const Dual& a, const Dual& b) { Dual r; r.v = a.v + b.v;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) r.d[i] = a.d[i] + b.d[i]; return r; }
+HQD Dual operator-(const Dual& a, const Dual& b) { Dual r; r.v = a.v - b.v;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) r.d[i] = a.d[i] - b.d[i]; return r; }
+HQD Dual operator-(const Dual& a) { Dual r; r.v = -a.v;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) r.d[i] = -a.d[i]; return r; }
+HQD Dual operator*(const Dual& a, const Dual& b) { Dual r; r.v = a.v * b.v;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i]; return r; }
+HQD Dual operator/(const Dual& a, const Dual& b) { Dual r; r.v = a.v / b.v;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) / b.v; return r; }
+HQD Dual dsqrt(const Dual& a) { Dual r; r.v = sqrt(a.v);
+#pragma unroll
+  for (int i = 0; i < 6; ++i) r.d[i] = a.d[i] / (2.0 * r.v); return r; }
+
+// m[15] in jacobian6 argument order (m00,m01,m02,m03,m04,m10,m11,m12,m13,
+// m20,m21,m22,m30,m31,m40); m_ab = E[x^a y^b], x = flux direction.
+// Output: rows 3, 5, 6 of the Jacobian (rows 1, 2, 4 are unit rows e2, e3, e5).
+HQN void jacobian6_rows(const double* m, double* r3, double* r5, double* r6) {
+  // index of m_ab in the argument list
+  const int AB[5][5] = {{0, 1, 2, 3, 4}, {5, 6, 7, 8, -1}, {9, 10, 11, -1, -1}, {12, 13, -1, -1, -1}, {14, -1, -1, -1, -1}};
+  const int SEED[15] = {-1, -1, 0, 3, 5, -1, -1, 1, 4, -1, -1, 2, -1, -1, -1};
+  Dual R[15];
+#pragma unroll
+  for (int n = 0; n < 15; ++n) { R[n] = dconst(m[n]); if (SEED[n] >= 0) R[n].d[SEED[n]] = 1.0; }
+  const Dual m00 = R[0];
+  const Dual u = R[5] / m00, vv = R[1] / m00;
+  Dual pu[5], pv[5];
+  pu[0] = dconst(1.0); pv[0] = dconst(1.0);
+#pragma unroll
+  for (int i = 1; i < 5; ++i) { pu[i] = pu[i - 1] * (-u); pv[i] = pv[i - 1] * (-vv); }
+  Dual Cc[15];
+#pragma unroll
+  for (int a = 0; a < 5; ++a)
+#pragma unroll
+    for (int b = 0; a + b < 5; ++b) {
+      Dual s = dconst(0.0);
+#pragma unroll
+      for (int p = 0; p <= a; ++p)
+#pragma unroll
+        for (int q = 0; q <= b; ++q)
+          s = s + dconst(double(binom(a, p) * binom(b, q))) * (R[AB[p][q]] / m00) * (pu[a - p] * pv[b - q]);
+      Cc[AB[a][b]] = s;
+    }
+  const Dual sx = dsqrt(Cc[AB[2][0]]), sy = dsqrt(Cc[AB[0][2]]);
+  auto S = [&](int a, int b) {
+    Dual d = dconst(1.0);
+    for (int i = 0; i < a; ++i) d = d * sx;
+    for (int i = 0; i < b; ++i) d = d * sy;
+    return Cc[AB[a][b]] / d;
+  };
+  const Dual S30 = S(3, 0), S40 = S(4, 0), S03 = S(0, 3), S04 = S(0, 4), S11 = S(1, 1), S21 = S(2, 1), S12 = S(1, 2), S31 = S(3, 1),
+             S13 = S(1, 3), S22 = S(2, 2);
+  const Dual one = dconst(1.0), two = dconst(2.0), three = dconst(3.0);
+  auto c32 = [&](const Dual& Sj3, const Dual& Si3, const Dual& Si4, const Dual& Sij, const Dual& Sijj, const Dual& Siij, const Dual& Siijj,
+                 const Dual& Siiij) {
+    return ((Sj3 * Si3 * Si3) / two - Sj3 + Sj3 * (Si3 * Si3 - Si4 + one)) * Sij + (Si4 - (three * Si3 * Si3) / two) * Sijj +
+           (-(three * Sj3 * Si3) / two) * Siij + ((three * Si3) / two) * Siijj + Sj3 * Siiij - Si3 / two;
+  };
+  const Dual S32 = c32(S03, S30, S40, S11, S12, S21, S22, S31);
+  const Dual S23 = c32(S30, S03, S04, S11, S21, S12, S22, S13);
+  const Dual S14 = (S03 - two * S03 * S04 + (dconst(9.0) * S03 * S03 * S03) / dconst(4.0)) * S11 +
+                   ((dconst(5.0) * S04) / two - (dconst(15.0) * S03 * S03) / dconst(4.0) - dconst(1.5)) * S12 + (two * S03) * S13;
+  auto scl = [&](Dual s, int a, int b) { for (int i = 0; i < a; ++i) s = s * sx; for (int i = 0; i < b; ++i) s = s * sy; return s; };
+  const Dual C32 = scl(S32, 3, 2), C23 = scl(S23, 2, 3), C14 = scl(S14, 1, 4);
+  Dual qu[6], qv[6];
+  qu[0] = dconst(1.0); qv[0] = dconst(1.0);
+#pragma unroll
+  for (int i = 1; i < 6; ++i) { qu[i] = qu[i - 1] * u; qv[i] = qv[i - 1] * vv; }
+  auto Ct = [&](int a, int b) -> Dual {
+    if (a + b == 0) return dconst(1.0);
+    if (a + b == 1) return dconst(0.0);
+    if (a == 3 && b == 2) return C32;
+    if (a == 2 && b == 3) return C23;
+    if (a == 1 && b == 4) return C14;
+    return Cc[AB[a][b]];
+  };
+  auto raw = [&](int a, int b) {
+    Dual s = dconst(0.0);
+#pragma unroll
+    for (int p = 0; p <= 5; ++p)
+#pragma unroll
+      for (int q = 0; q <= 5; ++q) {
+        if (p > a || q > b || p + q == 1) continue;
+        s = s + dconst(double(binom(a, p) * binom(b, q))) * Ct(p, q) * (qu[a - p] * qv[b - q]);
+      }
+    return m00 * s;
+  };
+  const Dual m32 = raw(3, 2), m23 = raw(2, 3), m14 = raw(1, 4);
+#pragma unroll
+  for (int j = 0; j < 6; ++j) { r3[j] = m32.d[j]; r5[j] = m23.d[j]; r6[j] = m14.d[j]; }
+}
+
+// ------------------------------------------- LAPACK-path eigenvalues, N <= 6
+// Julia eigvals(::Matrix{Float64}) -> geevx('B'): dgebal (permute + power-of-2
+// scaling), dgehd2 Householder Hessenberg reduction, dlahqr double-shift QR
+// (eigenvalues only) with dlanv2 standardization of 2x2 blocks.
+constexpr double ULP = 2.220446049250313e-16;
+constexpr double SAFMIN = 2.2250738585072014e-308;
+
+HQD double lsign(double a, double b) { return signbit(b) ? -fabs(a) : fabs(a); }
+HQD double dlapy2(double x, double y) {
+  const double xa = fabs(x), ya = fabs(y);
+  const double w = jmax(xa, ya), z = jmin(xa, ya);
+  if (z == 0.0 || w > 1.79769313486231571e308) return w;
+  const double r = z / w;
+  return w * sqrt(1.0 + r * r);
+}
+HQD double nrm2(const double* x, int n, int inc) {
+  double scale = 0.0, ssq = 1.0;
+  for (int i = 0; i < n; ++i) {
+    const double xi = x[i * inc];
+    if (xi != 0.0) {
+      const double a = fabs(xi);
+      if (scale < a) { const double r = scale / a; ssq = 1.0 + ssq * r * r; scale = a; }
+      else { const double r = a / scale; ssq = ssq + r * r; }
+    }
+  }
+  return scale * sqrt(ssq);
+}
+HQD double dlarfg(int n, double& alpha, double* x, int inc) {
+  if (n <= 1) return 0.0;
+  const double xnorm = nrm2(x, n - 1, inc);
+  if (xnorm == 0.0) return 0.0;
+  const double beta = -lsign(dlapy2(alpha, xnorm), alpha);
+  const double tau = (beta - alpha) / beta;
+  const double sc = 1.0 / (alpha - beta);
+  for (int i = 0; i < n - 1; ++i) x[i * inc] = x[i * inc] * sc;
+  alpha = beta;
+  return tau;
+}
+HQD void dlanv2(double a, double b, double c, double d, double& rt1r, double& rt1i, double& rt2r, double& rt2i) {
+  const double eps = ULP;
+  const double safmn2 = 1.0010415475915505e-146;  // 2^-485
+  const double safmx2 = 1.0 / safmn2;
+  if (c == 0.0) {
+  } else if (b == 0.0) {
+    const double t = d; d = a; a = t; b = -c; c = 0.0;
+  } else if ((a - d) == 0.0 && lsign(1.0, b) != lsign(1.0, c)) {
+  } else {
+    double temp = a - d;
+    double p = 0.5 * temp;
+    const double bcmax = jmax(fabs(b), fabs(c));
+    const double bcmis = jmin(fabs(b), fabs(c)) * lsign(1.0, b) * lsign(1.0, c);
+    double scale = jmax(fabs(p), bcmax);
+    double z = (p / scale) * p + (bcmax / scale) * bcmis;
+    if (z >= 4.0 * eps) {
+      z = p + lsign(sqrt(scale) * sqrt(z), p);
+      a = d + z;
+      d = d - (bcmax / z) * bcmis;
+      b = b - c;
+      c = 0.0;
+    } else {
+      int count = 0;
+      double sigma = b + c;
+      for (;;) {
+        ++count;
+        scale = jmax(fabs(temp), fabs(sigma));
+        if (scale >= safmx2) { sigma = sigma * safmn2; temp = temp * safmn2; if (count <= 20) continue; }
+        if (scale <= safmn2) { sigma = sigma * safmx2; temp = temp * safmx2; if (count <= 20) continue; }
+        break;
+      }
+      p = 0.5 * temp;
+      const double tau = dlapy2(sigma, temp);
+      const double cs = sqrt(0.5 * (1.0 + fabs(sigma) / tau));
+      const double sn = -(p / (tau * cs)) * lsign(1.0, sigma);
+      const double aa = a * cs + b * sn, bb = -a * sn + b * cs, cc = c * cs + d * sn, dd = -c * sn + d * cs;
+      a = aa * cs + cc * sn; b = bb * cs + dd * sn; c = -aa * sn + cc * cs; d = -bb * sn + dd * cs;
+      temp = 0.5 * (a + d);
+      a = temp; d = temp;
+      if (c != 0.0) {
+        if (b != 0.0) {
+          if (lsign(1.0, b) == lsign(1.0, c)) {
+            const double sab = sqrt(fabs(b)), sac = sqrt(fabs(c));
+            p = lsign(sab * sac, c);
+            a = temp + p; d = temp - p;
+            b = b - c; c = 0.0;
+          }
+        } else {
+          b = -c; c = 0.0;
+        }
+      }
+    }
+  }
+  rt1r = a; rt2r = d;
+  if (c == 0.0) { rt1i = 0.0; rt2i = 0.0; }
+  else { rt1i = sqrt(fabs(b)) * sqrt(fabs(c)); rt2i = -rt1i; }
+}
+
+// Eigenvalues of the N x N row-major matrix A (overwritten).  Returns 0 on
+// success, > 0 when the QR iteration limit was reached.
+template <int N>
+HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
+  for (int i = 0; i < N; ++i) { wr[i] = 0.0; wi[i] = 0.0; }
+  int k = 0, l = N - 1;
+  auto swapij = [&](int j, int m) {
+    if (j == m) return;
+    for (int r = 0; r <= l; ++r) { const double t = A[r][j]; A[r][j] = A[r][m]; A[r][m] = t; }
+    for (int c = k; c < N; ++c) { const double t = A[j][c]; A[j][c] = A[m][c]; A[m][c] = t; }
+  };
+  bool found = true;
+  while (found && l >= 0) {
+    found = false;
+    if (l == 0) break;
+    for (int j = l; j >= 0; --j) {
+      bool zero = true;
+      for (int i = 0; i <= l; ++i) { if (i == j) continue; if (A[j][i] != 0.0) { zero = false; break; } }
+      if (zero) { swapij(j, l); --l; found = true; break; }
+    }
+  }
+  found = true;
+  while (found) {
+    found = false;
+    for (int j = k; j <= l; ++j) {
+      bool zero = true;
+      for (int i = k; i <= l; ++i) { if (i == j) continue; if (A[i][j] != 0.0) { zero = false; break; } }
+      if (zero) { swapij(j, k); ++k; found = true; break; }
+    }
+  }
+  {
+    const double radix = 2.0, factor = 0.95;
+    const double sfmin1 = SAFMIN / ULP, sfmax1 = 1.0 / sfmin1, sfmin2 = sfmin1 * radix, sfmax2 = 1.0 / sfmin2;
+    double scal[N];
+    for (int i = 0; i < N; ++i) scal[i] = 1.0;
+    bool noconv = true;
+    int guard = 0;
+    while (noconv && guard++ < 1000) {
+      noconv = false;
+      for (int i = k; i <= l; ++i) {
+        double col[N], row[N];
+        for (int r = k; r <= l; ++r) col[r - k] = A[r][i];
+        for (int c2 = k; c2 <= l; ++c2) row[c2 - k] = A[i][c2];
+        double c = nrm2(col, l - k + 1, 1), r = nrm2(row, l - k + 1, 1);
+        double ca = 0.0, ra = 0.0;
+        for (int rr = 0; rr <= l; ++rr) ca = jmax(ca, fabs(A[rr][i]));
+        for (int cc = k; cc < N; ++cc) ra = jmax(ra, fabs(A[i][cc]));
+        if (c == 0.0 || r == 0.0) continue;
+        if (!isfinite(c + ca + r + ra)) return -1;  // LAPACK dgebal: NaN -> error return
+        double g = r / radix, f = 1.0;
+        const double s = c + r;
+        for (int guard2 = 0; guard2 < 2200 && !(c >= g || jmax(jmax(f, c), ca) >= sfmax2 || jmin(jmin(r, g), ra) <= sfmin2); ++guard2) {
+          f = f * radix; c = c * radix; ca = ca * radix; r = r / radix; g = g / radix; ra = ra / radix;
+        }
+        g = c / radix;
+        for (int guard3 = 0; guard3 < 2200 && !(g < r || jmax(r, ra) >= sfmax2 || jmin(jmin(jmin(f, c), g), ca) <= sfmin2); ++guard3) {
+          f = f / radix; c = c / radix; g = g / radix; ca = ca / radix; r = r * radix; ra = ra * radix;
+        }
+        if ((c + r) >= factor * s) continue;
+        if (f < 1.0 && scal[i] < 1.0) if (f * scal[i] <= sfmin1) continue;
+        if (f > 1.0 && scal[i] > 1.0) if (scal[i] >= sfmax1 / f) continue;
+        g = 1.0 / f;
+        scal[i] = scal[i] * f;
+        noconv = true;
+        for (int cc = k; cc < N; ++cc) A[i][cc] = A[i][cc] * g;
+        for (int rr = 0; rr <= l; ++rr) A[rr][i] = A[rr][i] * f;
+      }
+    }
+  }
+  const int ilo = k, ihi = l;
+  for (int i = 0; i < ilo; ++i) { wr[i] = A[i][i]; wi[i] = 0.0; }
+  for (int i = ihi + 1; i < N; ++i) { wr[i] = A[i][i]; wi[i] = 0.0; }
+  if (ilo > ihi) return 0;
+  if (ilo == ihi) { wr[ilo] = A[ilo][ilo]; wi[ilo] = 0.0; return 0; }
+  for (int i = ilo; i < ihi; ++i) {
+    const int nr = ihi - i;
+    double v[N];
+    double alpha = A[i + 1][i];
+    for (int r = 0; r < nr - 1; ++r) v[r + 1] = A[i + 2 + r][i];
+    const double tau = dlarfg(nr, alpha, &v[1], 1);
+    v[0] = 1.0;
+    if (tau != 0.0) {
+      for (int r = 0; r <= ihi; ++r) {
+        double w = 0.0;
+        for (int c = 0; c < nr; ++c) w = w + A[r][i + 1 + c] * v[c];
+        for (int c = 0; c < nr; ++c) A[r][i + 1 + c] = A[r][i + 1 + c] - tau * w * v[c];
+      }
+      for (int c = i + 1; c < N; ++c) {
+        double w = 0.0;
+        for (int r = 0; r < nr; ++r) w = w + A[i + 1 + r][c] * v[r];
+        for (int r = 0; r < nr; ++r) A[i + 1 + r][c] = A[i + 1 + r][c] - tau * v[r] * w;
+      }
+    }
+    A[i + 1][i] = alpha;
+    for (int r = i + 2; r < N; ++r) A[r][i] = 0.0;
+  }
+  double (&H)[N][N] = A;
+  const int nh = ihi - ilo + 1;
+  const double smlnum = SAFMIN * (double(nh) / ULP);
+  const double ulp = ULP;
+  const int itmax = 30 * (nh > 10 ? nh : 10);
+  const double dat1 = 0.75, dat2 = -0.4375;
+  int kdefl = 0;
+  int i = ihi;
+  while (i >= ilo) {
+    int lq = ilo;
+    bool converged = false;
+    for (int its = 0; its <= itmax; ++its) {
+      int kk;
+      for (kk = i; kk > lq; --kk) {
+        if (fabs(H[kk][kk - 1]) <= smlnum) break;
+        double tst = fabs(H[kk - 1][kk - 1]) + fabs(H[kk][kk]);
+        if (tst == 0.0) {
+          if (kk - 2 >= ilo) tst = tst + fabs(H[kk - 1][kk - 2]);
+          if (kk + 1 <= ihi) tst = tst + fabs(H[kk + 1][kk]);
+        }
+        if (fabs(H[kk][kk - 1]) <= ulp * tst) {
+          const double ab = jmax(fabs(H[kk][kk - 1]), fabs(H[kk - 1][kk]));
+          const double ba = jmin(fabs(H[kk][kk - 1]), fabs(H[kk - 1][kk]));
+          const double aa = jmax(fabs(H[kk][kk]), fabs(H[kk - 1][kk - 1] - H[kk][kk]));
+          const double bb = jmin(fabs(H[kk][kk]), fabs(H[kk - 1][kk - 1] - H[kk][kk]));
+          const double s = aa + ab;
+          if (ba * (ab / s) <= jmax(smlnum, ulp * (bb * (aa / s)))) break;
+        }
+      }
+      lq = kk;
+      if (lq > ilo) H[lq][lq - 1] = 0.0;
+      if (lq >= i - 1) { converged = true; break; }
+      ++kdefl;
+      const int i1 = lq, i2 = i;
+      double h11, h12, h21, h22;
+      if (kdefl % 20 == 0) {
+        const double s = fabs(H[i][i - 1]) + fabs(H[i - 1][i - 2]);
+        h11 = dat1 * s + H[i][i]; h12 = dat2 * s; h21 = s; h22 = h11;
+      } else if (kdefl % 10 == 0) {
+        const double s = fabs(H[lq + 1][lq]) + fabs(H[lq + 2][lq + 1]);
+        h11 = dat1 * s + H[lq][lq]; h12 = dat2 * s; h21 = s; h22 = h11;
+      } else {
+        h11 = H[i - 1][i - 1]; h21 = H[i][i - 1]; h12 = H[i - 1][i]; h22 = H[i][i];
+      }
+      const double s = fabs(h11) + fabs(h12) + fabs(h21) + fabs(h22);
+      double rt1r, rt1i, rt2r, rt2i;
+      if (s == 0.0) { rt1r = rt1i = rt2r = rt2i = 0.0; }
+      else {
+        h11 = h11 / s; h21 = h21 / s; h12 = h12 / s; h22 = h22 / s;
+        const double tr = (h11 + h22) / 2.0;
+        const double det = (h11 - tr) * (h22 - tr) - h12 * h21;
+        const double rtdisc = sqrt(fabs(det));
+        if (det >= 0.0) { rt1r = tr * s; rt2r = rt1r; rt1i = rtdisc * s; rt2i = -rt1i; }
+        else {
+          rt1r = tr + rtdisc; rt2r = tr - rtdisc;
+          if (fabs(rt1r - h22) <= fabs(rt2r - h22)) { rt1r = rt1r * s; rt2r = rt1r; }
+          else { rt2r = rt2r * s; rt1r = rt2r; }
+          rt1i = rt2i = 0.0;
+        }
+      }
+      int m;
+      double v[3];
+      for (m = i - 2; m >= lq; --m) {
+        double h21s = H[m + 1][m];
+        double s2 = fabs(H[m][m] - rt2r) + fabs(rt2i) + fabs(h21s);
+        h21s = H[m + 1][m] / s2;
+        v[0] = h21s * H[m][m + 1] + (H[m][m] - rt1r) * ((H[m][m] - rt2r) / s2) - rt1i * (rt2i / s2);
+        v[1] = h21s * (H[m][m] + H[m + 1][m + 1] - rt1r - rt2r);
+        v[2] = h21s * H[m + 2][m + 1];
+        s2 = fabs(v[0]) + fabs(v[1]) + fabs(v[2]);
+        v[0] = v[0] / s2; v[1] = v[1] / s2; v[2] = v[2] / s2;
+        if (m == lq) break;
+        const double h00 = fabs(H[m][m - 1]) * (fabs(v[1]) + fabs(v[2]));
+        const double h11b = fabs(v[0]) * (fabs(H[m - 1][m - 1]) + fabs(H[m][m]) + fabs(H[m + 1][m + 1]));
+        if (h00 <= ulp * h11b) break;
+      }
+      for (int kq = m; kq <= i - 1; ++kq) {
+        const int nr = (i - kq + 1) < 3 ? (i - kq + 1) : 3;
+        if (kq > m) for (int r = 0; r < nr; ++r) v[r] = H[kq + r][kq - 1];
+        const double t1 = dlarfg(nr, v[0], &v[1], 1);
+        if (kq > m) {
+          H[kq][kq - 1] = v[0];
+          H[kq + 1][kq - 1] = 0.0;
+          if (kq < i - 1) H[kq + 2][kq - 1] = 0.0;
+        } else if (m > lq) {
+          H[kq][kq - 1] = H[kq][kq - 1] * (1.0 - t1);
+        }
+        const double v2 = v[1], t2 = t1 * v2;
+        if (nr == 3) {
+          const double v3 = v[2], t3v = t1 * v3;
+          for (int j = kq; j <= i2; ++j) {
+            const double sum = H[kq][j] + v2 * H[kq + 1][j] + v3 * H[kq + 2][j];
+            H[kq][j] = H[kq][j] - sum * t1; H[kq + 1][j] = H[kq + 1][j] - sum * t2; H[kq + 2][j] = H[kq + 2][j] - sum * t3v;
+          }
+          const int jm = (kq + 3 < i) ? kq + 3 : i;
+          for (int j = i1; j <= jm; ++j) {
+            const double sum = H[j][kq] + v2 * H[j][kq + 1] + v3 * H[j][kq + 2];
+            H[j][kq] = H[j][kq] - sum * t1; H[j][kq + 1] = H[j][kq + 1] - sum * t2; H[j][kq + 2] = H[j][kq + 2] - sum * t3v;
+          }
+        } else if (nr == 2) {
+          for (int j = kq; j <= i2; ++j) {
+            const double sum = H[kq][j] + v2 * H[kq + 1][j];
+            H[kq][j] = H[kq][j] - sum * t1; H[kq + 1][j] = H[kq + 1][j] - sum * t2;
+          }
+          for (int j = i1; j <= i; ++j) {
+            const double sum = H[j][kq] + v2 * H[j][kq + 1];
+            H[j][kq] = H[j][kq] - sum * t1; H[j][kq + 1] = H[j][kq + 1] - sum * t2;
+          }
+        }
+      }
+    }
+    if (!converged) return i + 1;
+    if (lq == i) { wr[i] = H[i][i]; wi[i] = 0.0; }
+    else if (lq == i - 1) dlanv2(H[i - 1][i - 1], H[i - 1][i], H[i][i - 1], H[i][i], wr[i - 1], wi[i - 1], wr[i], wi[i]);
+    kdefl = 0;
+    i = lq - 1;
+  }
+  return 0;
+}
+
+// compute_jacobian_eigenvalues for one 15-moment slice: extreme real parts
+// and max |imag|.  A non-finite Jacobian gives NaN (the reference's guard).
+struct EigOut { double vmin, vmax, imax; };
+HQN EigOut jac_eigs(const double* ma) {
+  double r3[6], r5[6], r6[6];
+  jacobian6_rows(ma, r3, r5, r6);
+  double J[6][6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+#pragma unroll
+    for (int j = 0; j < 6; ++j) J[i][j] = 0.0;
+  J[0][1] = 1.0; J[1][2] = 1.0; J[3][4] = 1.0;
+  bool fin = true;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    J[2][j] = r3[j]; J[4][j] = r5[j]; J[5][j] = r6[j];
+    fin = fin && isfinite(r3[j]) && isfinite(r5[j]) && isfinite(r6[j]);
+  }
+  EigOut o;
+  if (!fin) { o.vmin = qnan(); o.vmax = qnan(); o.imax = qnan(); return o; }
+  double wr[6], wi[6];
+  eig_real<6>(J, wr, wi);
+  // sort(real) with NaN last, first and last
+  double mn = wr[0], mx = wr[0];
+  bool anynan = (wr[0] != wr[0]);
+  for (int q = 1; q < 6; ++q) {
+    if (wr[q] != wr[q]) { anynan = true; continue; }
+    if (mn != mn || wr[q] < mn) mn = wr[q];
+    if (mx != mx || wr[q] > mx) mx = wr[q];
+  }
+  o.vmin = mn;
+  o.vmax = anynan ? qnan() : mx;
+  double im = fabs(wi[0]);
+  for (int q = 1; q < 6; ++q) im = jmax(im, fabs(wi[q]));
+  o.imax = im;
+  return o;
+}
+
+// axis_moment_slice (src/utils/axis_moment_slice.jl:31-54), 0-based
+__device__ constexpr int SLICE[4][15] = {{0, 5, 9, 12, 14, 1, 6, 10, 13, 2, 7, 11, 3, 8, 4},
+                                         {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14},
+                                         {0, 15, 19, 22, 24, 1, 16, 20, 23, 2, 17, 21, 3, 18, 4},
+                                         {0, 15, 19, 22, 24, 5, 25, 31, 33, 9, 28, 34, 12, 30, 14}};
+// eigenvalues6z planes: WU and WV argument orders
+__device__ constexpr int WUI[15] = {0, 1, 2, 3, 4, 15, 16, 17, 18, 19, 20, 21, 22, 23, 24};
+
+// Reference correct_{uv,uw,vw}_plane on central moments C (35-order) for the
+// coordinate pair (i, j) in {0,1,2}.
+HQD void correct_plane(double* C, int i, int j, double Sij, double Si3, double Sj3, double Si4, double Sj4, double Sii_jj, double Cii, double Cjj) {
+  const double Sijj = Sij * Sj3, Siij = Sij * Si3, Sijjj = Sij * Sj4, Siiij = Sij * Si4;
+  const double s22min = (2.0 + 5.0 * Sj3 * Sij * Si3) / 6.0;
+  if (Sii_jj < s22min) Sii_jj = s22min;
+  const double si = sqrt(jmax(EPS, Cii)), sj = sqrt(jmax(EPS, Cjj));
+  auto at = [&](int a, int b) {
+    int e[3] = {0, 0, 0};
+    e[i] += a; e[j] += b;
+    return idx35(e[0], e[1], e[2]);
+  };
+  C[at(2, 1)] = Siij * (si * si) * sj;
+  C[at(1, 2)] = Sijj * si * (sj * sj);
+  C[at(3, 1)] = Siiij * (si * si * si) * sj;
+  C[at(1, 3)] = Sijjj * si * (sj * sj * sj);
+  C[at(2, 2)] = Sii_jj * (si * si) * (sj * sj);
+}
+
+// Moments whose flux-Jacobian eigenvalues are complex are corrected, rebuilt
+// and re-realized (correct_moments_for_real_eigenvalues and the eigenvalues6z
+// branch).  planes: bit0 = first slice (pair a), bit1 = second slice.
+HQN void correct_for_real(const double* M, int pa_i, int pa_j, int pb_i, int pb_j, int planes, int flag2D, double Ma, double* Mout) {
+  const double M000 = M[0];
+  const double u = M[1] / M000, v = M[5] / M000, w = M[15] / M000;
+  double C[35], S[35];
+  raw_to_central(M, C);
+  central_to_std(C, S);
+  const double Cd[3] = {C[2], C[9], C[19]};
+  const double S3[3] = {S[3], S[12], S[22]}, S4v[3] = {S[4], S[14], S[24]};
+  auto corr = [&](int i, int j) {
+    const int ij = (i == 0 && j == 1) ? 6 : (i == 0 && j == 2) ? 16 : 25;   // S110, S101, S011
+    const int iijj = (i == 0 && j == 1) ? 11 : (i == 0 && j == 2) ? 21 : 34; // S220, S202, S022
+    correct_plane(C, i, j, S[ij], S3[i], S3[j], S4v[i], S4v[j], S[iijj], Cd[i], Cd[j]);
+  };
+  if (planes & 1) corr(pa_i, pa_j);
+  if (planes & 2) corr(pb_i, pb_j);
+  double Mh[35];
+  C[0] = 1.0;
+  central_to_raw4(M000, u, v, w, C, Mh);
+  flux_closure35(Mh, flag2D, Ma, nullptr, nullptr, nullptr, Mout);
+}
+
+// eigenvalues6_hyperbolic_3D for axis 1 (x) or 2 (y).
+HQN void eigenvalues6(const double* M, int axis, int flag2D, double Ma, double& vmin, double& vmax, double* Mr) {
+  const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
+  double a[15], b[15];
+  for (int n = 0; n < 15; ++n) { a[n] = M[SLICE[sa][n]]; b[n] = M[SLICE[sb][n]]; }
+  EigOut ea = jac_eigs(a), eb = jac_eigs(b);
+  auto combine = [&]() {
+    vmin = ea.vmin; vmax = ea.vmax;
+    if (eb.vmin == eb.vmin || eb.vmax == eb.vmax) { vmin = jmin(vmin, eb.vmin); vmax = jmax(vmax, eb.vmax); }
+  };
+  combine();
+#pragma unroll
+  for (int n = 0; n < 35; ++n) Mr[n] = M[n];
+  const double thr = 1000.0 * EPS;
+  const bool ca = ea.imax > thr, cb = eb.imax > thr;
+  if (ca || cb) {
+    double Mc[35];
+    // pair a is always the UV plane; pair b is UW (x) or VW (y)
+    correct_for_real(M, 0, 1, axis == 1 ? 0 : 1, 2, (ca ? 1 : 0) | (cb ? 2 : 0), flag2D, Ma, Mc);
+    for (int n = 0; n < 15; ++n) { a[n] = Mc[SLICE[sa][n]]; b[n] = Mc[SLICE[sb][n]]; }
+    ea = jac_eigs(a); eb = jac_eigs(b);
+    combine();
+#pragma unroll
+    for (int n = 0; n < 35; ++n) Mr[n] = Mc[n];
+  }
+}
+
+// eigenvalues6z_hyperbolic_3D
+HQN void eigenvalues6z(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr) {
+#pragma unroll
+  for (int n = 0; n < 35; ++n) Mr[n] = M[n];
+  if (positivity && M[0] <= 0.0) Mr[0] = jmax(M[0], 1e-14);
+  double Mw[35];
+#pragma unroll
+  for (int n = 0; n < 35; ++n) Mw[n] = M[n];
+  Mw[0] = Mr[0];
+  if (positivity && Mw[0] > 1e-15) {
+    const double m000 = Mw[0];
+    const double vx = M[2] / m000 - sq(M[1] / m000), vy = M[9] / m000 - sq(M[5] / m000), vz = M[19] / m000 - sq(M[15] / m000);
+    if (vx < 0.0 || vy < 0.0 || vz < 0.0) {
+      flux_closure35(M, flag2D, Ma, nullptr, nullptr, nullptr, Mr);
+#pragma unroll
+      for (int n = 0; n < 35; ++n) Mw[n] = Mr[n];
+    }
+  }
+  double a[15], b[15];
+  for (int n = 0; n < 15; ++n) { a[n] = Mw[WUI[n]]; b[n] = Mw[SLICE[3][n]]; }
+  EigOut ea = jac_eigs(a), eb = jac_eigs(b);
+  vmin = jmin(ea.vmin, eb.vmin);
+  vmax = jmax(ea.vmax, eb.vmax);
+  const double thr = 1000.0 * EPS;
+  const bool ca = ea.imax > thr, cb = eb.imax > thr;
+  if (ca || cb) {
+    correct_for_real(M, 0, 2, 1, 2, (ca ? 1 : 0) | (cb ? 2 : 0), flag2D, Ma, Mr);
+    for (int n = 0; n < 15; ++n) { a[n] = Mr[WUI[n]]; b[n] = Mr[SLICE[3][n]]; }
+    ea = jac_eigs(a); eb = jac_eigs(b);
+    vmin = jmin(ea.vmin, eb.vmin);
+    vmax = jmax(ea.vmax, eb.vmax);
+  }
+}
+
+// closure_and_eigenvalues with N = 2: extreme eigenvalues of the 3x3 Jacobi
+// matrix (symmetric tridiagonal when both b >= 0; otherwise through the real
+// matrix with the same characteristic polynomial).
+HQN void closure_eigs(double m0, double m1, double m2, double m3, double m4, double& vmin, double& vmax) {
+  // Chebyshev recurrence
+  const double a0 = m1 / m0;
+  const double s21 = m0, s22 = m1, s23 = m2, s24 = m3, s25 = m4;
+  const double r32 = s23 - a0 * s22, r33 = s24 - a0 * s23, r34 = s25 - a0 * s24;
+  const double a1 = r33 / r32 - s22 / s21;
+  const double b1 = r32 / s21;
+  const double r43 = r34 - a1 * r33 - b1 * s23;
+  double b2 = r43 / r32;
+  const double a2 = (a0 + a1) / 2.0;
+  b2 = b2 * 5.0 / 2.0;
+  if (!(isfinite(a0) && isfinite(a1) && isfinite(a2) && isfinite(b1) && isfinite(b2))) { vmin = qnan(); vmax = qnan(); return; }
+  if (b1 >= 0.0 && b2 >= 0.0) {
+    double A[3][3] = {{a0, sqrt(b1), 0.0}, {sqrt(b1), a1, sqrt(b2)}, {0.0, sqrt(b2), a2}};
+    for (int sweep = 0; sweep < 60; ++sweep) {
+      const double off = fabs(A[0][1]) + fabs(A[0][2]) + fabs(A[1][2]);
+      if (off == 0.0) break;
+      for (int p = 0; p < 2; ++p)
+        for (int q = p + 1; q < 3; ++q) {
+          if (A[p][q] == 0.0) continue;
+          const double theta = (A[q][q] - A[p][p]) / (2.0 * A[p][q]);
+          double t = jsign(theta) / (fabs(theta) + sqrt(theta * theta + 1.0));
+          if (theta == 0.0) t = 1.0;
+          const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+          for (int kk = 0; kk < 3; ++kk) { const double akp = A[kk][p], akq = A[kk][q]; A[kk][p] = c * akp - s * akq; A[kk][q] = s * akp + c * akq; }
+          for (int kk = 0; kk < 3; ++kk) { const double apk = A[p][kk], aqk = A[q][kk]; A[p][kk] = c * apk - s * aqk; A[q][kk] = s * apk + c * aqk; }
+        }
+    }
+    vmin = jmin(jmin(A[0][0], A[1][1]), A[2][2]);
+    vmax = jmax(jmax(A[0][0], A[1][1]), A[2][2]);
+    return;
+  }
+  double R[3][3] = {{a0, b1, 0.0}, {1.0, a1, b2}, {0.0, 1.0, a2}};
+  double wr[3], wi[3];
+  eig_real<3>(R, wr, wi);
+  vmin = jmin(jmin(wr[0], wr[1]), wr[2]);
+  vmax = jmax(jmax(wr[0], wr[1]), wr[2]);
+}
+
+// collision35: BGK relaxation toward the isotropic Gaussian.
+HQD void collision35(double* M, double dt, double Kn, int positivity) {
+  const double rho = M[0];
+  const double u = M[1] / rho, v = M[5] / rho, w = M[15] / rho;
+  const double C200 = M[2] / rho - u * u, C020 = M[9] / rho - v * v, C002 = M[19] / rho - w * w;
+  double Th = (C200 + C020 + C002) / 3.0;
+  if (positivity) Th = jmax(Th, 1e-14);
+  const double tc = Kn / (rho * sqrt(Th) * 2.0);
+  // central moments of the isotropic Gaussian: A = sqrt(Th) I,
+  // C_ijk = S_ijk a^i a^j a^k with S the standard-normal moments.
+  const double a = sqrt(Th);
+  const double p2 = a * a, p3 = a * a * a, p4 = p2 * p2;
+  const double pw[5] = {1.0, a, p2, p3, p4};
+  double C[35];
+#pragma unroll
+  for (int n = 0; n < 35; ++n) {
+    const int i = ex_i(n), j = ex_j(n), k = ex_k(n);
+    const double zi = (i == 0) ? 1.0 : (i == 2) ? 1.0 : (i == 4) ? 3.0 : 0.0;
+    const double zj = (j == 0) ? 1.0 : (j == 2) ? 1.0 : (j == 4) ? 3.0 : 0.0;
+    const double zk = (k == 0) ? 1.0 : (k == 2) ? 1.0 : (k == 4) ? 3.0 : 0.0;
+    C[n] = zi * zj * zk * pw[i] * pw[j] * pw[k];
+  }
+  C[0] = 1.0;
+  double MG[35];
+  central_to_raw4(rho, u, v, w, C, MG);
+  const double e = exp(-dt / tc);
+#pragma unroll
+  for (int n = 0; n < 35; ++n) M[n] = MG[n] - e * (MG[n] - M[n]);
+}
+
+}  // namespace hyq

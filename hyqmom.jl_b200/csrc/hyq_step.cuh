@@ -1,0 +1,71 @@
+// Shared definitions of the step kernels, split over several translation
+// units so that ptxas compiles the large per-cell kernels in parallel.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace hyqk {
+
+// Device-side loop clock of one simulation (t, dt, nn live on the GPU).
+struct DevClock {
+  double t, dt, vmax;
+  long long nn;
+  int active;  // 1 while the current step runs
+  int status;
+};
+
+// Per-context constants of the step.
+struct StepConst {
+  long long N;
+  int Nx, Ny, Nz, flag2D, positivity;
+  long long nnmax;
+  double tmax, Kn, Ma, CFL, dtmax, dx, dy, dz;
+  int nblocksA;
+};
+
+constexpr int BS_A = 128;
+constexpr int BS_EF = 128;
+constexpr int BS_HLL = 256;
+constexpr int BS_CELLS = 128;
+
+inline int grid_of(long long n, int bs) { return int((n + bs - 1) / bs); }
+
+// launch wrappers (defined in k_phase_A.cu, k_phase_EF.cu, k_cells.cu)
+void launch_phase_A(const StepConst& sc, double* M, double* Fx, double* Fy, double* Fz, double* vp, double* blockmax, DevClock* clk,
+                    cudaStream_t s);
+void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, const DevClock* clk, cudaStream_t s);
+void launch_cells_phase_A(const double* M, long long n, int flag2D, double Ma, int positivity, double* Fx, double* Fy, double* Fz,
+                          double* Mr, double* vp, cudaStream_t s);
+void launch_cells_flux(const double* M, long long n, int flag2D, double Ma, double* Fx, double* Fy, double* Fz, double* Mr, cudaStream_t s);
+void launch_cells_eig(const double* M, long long n, int axis, int flag2D, double Ma, int positivity, double* v, double* Mr, cudaStream_t s);
+void launch_cells_closure_eigs(const double* mom, long long n, double* v, cudaStream_t s);
+void launch_cells_collision(const double* M, long long n, double dt, double Kn, int positivity, double* out, cudaStream_t s);
+void launch_std_central(const double* M, long long n, double* S, double* C, cudaStream_t s);
+
+}  // namespace hyqk
+
+#ifdef __CUDACC__
+namespace hyqk {
+__device__ __forceinline__ double nanmax(double a, double b) { return (a != a) ? a : ((b != b) ? b : fmax(a, b)); }
+
+__device__ __forceinline__ double warp_nanmax(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// NaN-propagating block max (Julia `maximum` semantics).
+template <int BS> __device__ double block_nanmax(double v) {
+  __shared__ double red[BS / 32];
+  v = warp_nanmax(v);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double w = (threadIdx.x < BS / 32) ? red[threadIdx.x] : 0.0;
+    w = warp_nanmax(w);
+    if (threadIdx.x == 0) red[0] = w;
+  }
+  __syncthreads();
+  return red[0];
+}
+}  // namespace hyqk
+#endif

@@ -1,0 +1,82 @@
+"""ctypes binding of libhyqmom_b200.so (declared in include/hyqmom.h).
+
+The library is the only compute path: if it is missing or fails to load the
+import raises; there is no CPU fallback.
+"""
+import ctypes
+import os
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_NAME = "libhyqmom_b200.so"
+LIB_PATH = os.path.join(PKG_DIR, LIB_NAME)
+
+HYQ_OK = 0
+ERRORS = {-1: "HYQ_EINVAL", -2: "HYQ_ECUDA", -3: "HYQ_ENONFINITE", -4: "HYQ_ETIMEOUT", -5: "HYQ_ENOMEM"}
+
+
+class HyqParams(ctypes.Structure):
+    _fields_ = [("Nx", ctypes.c_int32), ("Ny", ctypes.c_int32), ("Nz", ctypes.c_int32), ("flag2D", ctypes.c_int32),
+                ("positivity", ctypes.c_int32), ("device", ctypes.c_int32), ("nnmax", ctypes.c_int64),
+                ("tmax", ctypes.c_double), ("Kn", ctypes.c_double), ("Ma", ctypes.c_double), ("CFL", ctypes.c_double),
+                ("dtmax", ctypes.c_double), ("xmin", ctypes.c_double), ("xmax", ctypes.c_double),
+                ("ymin", ctypes.c_double), ("ymax", ctypes.c_double), ("zmin", ctypes.c_double), ("zmax", ctypes.c_double)]
+
+
+class HyqStats(ctypes.Structure):
+    _fields_ = [("t", ctypes.c_double), ("dt", ctypes.c_double), ("vmax", ctypes.c_double), ("nn", ctypes.c_int64),
+                ("done", ctypes.c_int32), ("status", ctypes.c_int32)]
+
+
+class HyqError(RuntimeError):
+    pass
+
+
+_lib = None
+
+# exported symbols (include/hyqmom.h)
+SYMBOLS = ["hyq_abi_version", "hyq_create", "hyq_destroy", "hyq_last_error", "hyq_set_state", "hyq_get_state",
+           "hyq_set_state_device", "hyq_get_state_device", "hyq_set_clock", "hyq_advance", "hyq_advance_async",
+           "hyq_synchronize", "hyq_stats_get", "hyq_advance_timed", "hyq_get_SC", "hyq_stream", "hyq_cells_flux_closure",
+           "hyq_cells_eigenvalues", "hyq_cells_closure_eigs", "hyq_cells_collision", "hyq_cells_phase_A"]
+
+
+def load(path=None):
+    """Load the library (raises if the CUDA build is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise HyqError(f"{LIB_NAME} not built (expected at {path}); run __graft_entry__.build()")
+    lib = ctypes.CDLL(path)
+    vp, dp, i64, i32, dbl = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int64, ctypes.c_int32, ctypes.c_double
+    lib.hyq_abi_version.restype = ctypes.c_int
+    lib.hyq_create.argtypes = [ctypes.POINTER(HyqParams), ctypes.POINTER(vp)]
+    lib.hyq_destroy.argtypes = [vp]
+    lib.hyq_destroy.restype = None
+    lib.hyq_last_error.argtypes = [vp]
+    lib.hyq_last_error.restype = ctypes.c_char_p
+    for nm in ("hyq_set_state", "hyq_get_state", "hyq_set_state_device", "hyq_get_state_device"):
+        getattr(lib, nm).argtypes = [vp, vp]
+    lib.hyq_set_clock.argtypes = [vp, dbl, i64]
+    lib.hyq_advance.argtypes = [vp, i64, dp, ctypes.POINTER(i64), ctypes.POINTER(i32)]
+    lib.hyq_advance_async.argtypes = [vp, i64]
+    lib.hyq_synchronize.argtypes = [vp]
+    lib.hyq_advance_timed.argtypes = [vp, i64, ctypes.POINTER(ctypes.c_float)]
+    lib.hyq_stats_get.argtypes = [vp, ctypes.POINTER(HyqStats)]
+    lib.hyq_get_SC.argtypes = [vp, vp, vp]
+    lib.hyq_stream.argtypes = [vp]
+    lib.hyq_stream.restype = vp
+    lib.hyq_cells_flux_closure.argtypes = [vp, i64, i32, dbl, vp, vp, vp, vp, vp]
+    lib.hyq_cells_eigenvalues.argtypes = [vp, i64, i32, i32, dbl, i32, vp, vp, vp]
+    lib.hyq_cells_closure_eigs.argtypes = [vp, i64, vp, vp]
+    lib.hyq_cells_collision.argtypes = [vp, i64, dbl, dbl, i32, vp, vp]
+    lib.hyq_cells_phase_A.argtypes = [vp, i64, i32, dbl, i32, vp, vp, vp, vp, vp, vp]
+    _lib = lib
+    return lib
+
+
+def check(rc, ctx=None):
+    if rc != HYQ_OK:
+        msg = load().hyq_last_error(ctx).decode() if load() else ""
+        raise HyqError(f"{ERRORS.get(rc, rc)}: {msg}")

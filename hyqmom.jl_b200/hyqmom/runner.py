@@ -1,0 +1,171 @@
+"""Host mirror of the reference's entry points over the CUDA step.
+
+    simulation_runner(params)                      src/simulation_runner.jl:63-759
+    run_simulation(; Nx, Ny, Nz, tmax, ...)        src/simulation_runner.jl:816-944
+    run_simulation_with_snapshots(params; interval) src/simulation_runner.jl:994-1011
+
+Same parameter names, same return tuples.  The IC is built on the host (as in
+the reference), every time step runs on the GPU through libhyqmom_b200.so.
+"""
+import ctypes
+import time
+
+import numpy as np
+
+from . import _lib
+from . import ic as _ic
+from .snapshots import SnapshotWriter
+
+
+class Solver:
+    """One simulation domain on one GPU (a hyq_ctx)."""
+
+    def __init__(self, params, device=0):
+        lib = _lib.load()
+        p = params
+        xmin, xmax, ymin, ymax, zmin, zmax = _ic.extents(p)
+        hp = _lib.HyqParams(Nx=p["Nx"], Ny=p["Ny"], Nz=p["Nz"], flag2D=int(p["flag2D"]),
+                            positivity=int(bool(p.get("positivity", True))), device=device, nnmax=int(p["nnmax"]),
+                            tmax=float(p["tmax"]), Kn=float(p["Kn"]), Ma=float(p["Ma"]), CFL=float(p["CFL"]),
+                            dtmax=float(p["dtmax"]), xmin=xmin, xmax=xmax, ymin=ymin, ymax=ymax, zmin=zmin, zmax=zmax)
+        h = ctypes.c_void_p()
+        rc = lib.hyq_create(ctypes.byref(hp), ctypes.byref(h))
+        if rc != 0:
+            raise _lib.HyqError(f"{_lib.ERRORS.get(rc, rc)}: {lib.hyq_last_error(None).decode()}")
+        self._lib, self._h, self.params = lib, h, dict(p)
+        self.shape = (p["Nx"], p["Ny"], p["Nz"], 35)
+
+    def close(self):
+        if self._h:
+            self._lib.hyq_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, rc):
+        if rc != 0:
+            raise _lib.HyqError(f"{_lib.ERRORS.get(rc, rc)}: {self._lib.hyq_last_error(self._h).decode()}")
+
+    # state ----------------------------------------------------------------
+    def set_state(self, M):
+        M = np.asfortranarray(M, dtype=np.float64)
+        assert M.shape == self.shape
+        self._chk(self._lib.hyq_set_state(self._h, M.ctypes.data))
+
+    def get_state(self):
+        M = np.empty(self.shape, dtype=np.float64, order="F")
+        self._chk(self._lib.hyq_get_state(self._h, M.ctypes.data))
+        return M
+
+    def set_state_device(self, ptr):
+        self._chk(self._lib.hyq_set_state_device(self._h, ctypes.c_void_p(ptr)))
+
+    def get_state_device(self, ptr):
+        self._chk(self._lib.hyq_get_state_device(self._h, ctypes.c_void_p(ptr)))
+
+    def get_SC(self):
+        S = np.empty(self.shape, dtype=np.float64, order="F")
+        C = np.empty(self.shape, dtype=np.float64, order="F")
+        self._chk(self._lib.hyq_get_SC(self._h, S.ctypes.data, C.ctypes.data))
+        return S, C
+
+    def set_clock(self, t, nn):
+        self._chk(self._lib.hyq_set_clock(self._h, float(t), int(nn)))
+
+    # stepping --------------------------------------------------------------
+    def advance(self, max_steps):
+        t = ctypes.c_double()
+        nn = ctypes.c_int64()
+        done = ctypes.c_int32()
+        self._chk(self._lib.hyq_advance(self._h, int(max_steps), ctypes.byref(t), ctypes.byref(nn), ctypes.byref(done)))
+        return t.value, nn.value, bool(done.value)
+
+    def advance_async(self, max_steps):
+        self._chk(self._lib.hyq_advance_async(self._h, int(max_steps)))
+
+    def synchronize(self):
+        self._chk(self._lib.hyq_synchronize(self._h))
+
+    def stats(self):
+        st = _lib.HyqStats()
+        self._chk(self._lib.hyq_stats_get(self._h, ctypes.byref(st)))
+        return dict(t=st.t, dt=st.dt, vmax=st.vmax, nn=st.nn, done=bool(st.done), status=st.status)
+
+    @property
+    def stream(self):
+        return self._lib.hyq_stream(self._h)
+
+
+def _runner_params(params):
+    p = dict(params)
+    p.setdefault("positivity", True)
+    p.setdefault("nnmax", 20000000)
+    return p
+
+
+def simulation_runner(params, device=0, verbose=False, chunk=64):
+    """Reference ``simulation_runner(params)`` for one rank.
+
+    Returns ``(M_final, final_time, time_steps, grid)`` or, when
+    ``params['snapshot_interval'] > 0``, ``(snapshot_filename, grid)``.
+    """
+    p = _runner_params(params)
+    interval = int(p.get("snapshot_interval", 0) or 0)
+    grid_out = _ic.grid(p)
+    M0 = _ic.initial_state(p)
+    solver = Solver(p, device=device)
+    try:
+        solver.set_state(M0)
+        writer = None
+        if interval > 0:
+            fname = p.get("snapshot_filename") or "snapshots_Nx%d_Ny%d_Nz%d_Kn%.2f_Ma%.2f_tmax%.4f.jld2" % (
+                p["Nx"], p["Ny"], p["Nz"], p["Kn"], p["Ma"], p["tmax"])
+            writer = SnapshotWriter(fname, p, interval)
+            S, C = solver.get_SC()
+            writer.write(M0, 0.0, 0, S, C)
+        t0 = time.time()
+        done = False
+        t, nn = 0.0, 0
+        step_block = interval if interval > 0 else chunk
+        while not done:
+            t, nn, done = solver.advance(step_block)
+            if verbose:
+                st = solver.stats()
+                print("Step %4d: t = %.4f, dt = %.4e, wall = %.4f s" % (nn, t, st["dt"], time.time() - t0))
+            if writer is not None and (nn % interval == 0 or done):
+                S, C = solver.get_SC()
+                writer.write(solver.get_state(), t, nn, S, C)
+        if writer is not None:
+            writer.close(grid_out)
+            return writer.filename, grid_out
+        return solver.get_state(), t, nn, grid_out
+    finally:
+        solver.close()
+
+
+def run_simulation(Np=None, Nx=20, Ny=20, Nz=1, tmax=0.1, num_workers=1, verbose=True, Kn=1.0, Ma=0.0, flag2D=0, CFL=0.5,
+                   homogeneous_z=True, debug_output=False, device=0, **_unused):
+    """Reference ``run_simulation`` (src/simulation_runner.jl:816-944); returns the result dict."""
+    if Np is not None:
+        Nx = Ny = Np
+    p = _ic.run_simulation_params(Nx=Nx, Ny=Ny, Nz=Nz, tmax=tmax, Kn=Kn, Ma=Ma, flag2D=flag2D, CFL=CFL,
+                                  homogeneous_z=homogeneous_z, debug_output=debug_output)
+    M, t, nn, g = simulation_runner(p, device=device, verbose=False)
+    if verbose:
+        print("Simulation complete! Final time: %s Time steps: %d" % (t, nn))
+    return {"M": M, "final_time": t, "time_steps": nn, "xm": g["xm"], "ym": g["ym"], "zm": g["zm"], "Nx": Nx, "Ny": Ny,
+            "Nz": Nz, "tmax": tmax}
+
+
+def run_simulation_with_snapshots(params, snapshot_interval=2, device=0):
+    """Reference ``run_simulation_with_snapshots`` (src/simulation_runner.jl:994-1011)."""
+    p = dict(params)
+    p["snapshot_interval"] = snapshot_interval
+    result = simulation_runner(p, device=device)
+    if snapshot_interval > 0:
+        return result
+    return None, result[3]

@@ -1,0 +1,118 @@
+/* C-ABI of libhyqmom_b200.so: the HyQMOM explicit time step on one B200.
+ *
+ * Drop-in boundary for the reference's time loop.  The reference
+ * (HyQMOM.jl) has no FFI; these entry points replace the body of
+ * simulation_runner (src/simulation_runner.jl:346-560, one rank):
+ *   hyq_create        <- parameter unpacking + allocation (:63-185)
+ *   hyq_set_state     <- IC fill of M (:187-271), done by the caller's IC code
+ *   hyq_advance       <- `while t < tmax && nn < nnmax` step loop (:346-560)
+ *   hyq_get_state     <- gather_M of the interior (:745-752)
+ *   hyq_get_SC        <- compute_standardized_field / compute_central_field
+ *                        (src/utils/compute_standardized_field.jl:16-66)
+ *   hyq_stats         <- vmax / dt diagnostics printed by the loop (:402-433)
+ * State buffers are Julia column-major (Nx, Ny, Nz, 35) Float64 arrays
+ * (moment-major SoA), passed as plain pointers.
+ *
+ * Conventions: every call returns 0 on success or a negative HYQ_E* code;
+ * hyq_last_error(ctx) describes the last failure.  The library owns device
+ * memory; the caller owns host buffers.  A context is not thread-safe.
+ */
+#ifndef HYQMOM_B200_H
+#define HYQMOM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HYQ_ABI_VERSION 1
+
+#define HYQ_OK 0
+#define HYQ_EINVAL -1      /* invalid argument or parameter */
+#define HYQ_ECUDA -2       /* CUDA runtime error */
+#define HYQ_ENONFINITE -3  /* non-finite state found (opt-in check) */
+#define HYQ_ETIMEOUT -4    /* a bounded device wait ran out */
+#define HYQ_ENOMEM -5      /* device allocation failed */
+
+/* Fields read by simulation_runner (src/simulation_runner.jl:74-129). */
+typedef struct hyq_params {
+  int32_t Nx, Ny, Nz;
+  int32_t flag2D;      /* params.flag2D */
+  int32_t positivity;  /* params.positivity (default true, :87-91) */
+  int32_t device;      /* CUDA device ordinal */
+  int64_t nnmax;       /* params.nnmax */
+  double tmax, Kn, Ma, CFL, dtmax;
+  double xmin, xmax, ymin, ymax, zmin, zmax; /* domain extents (:123-129) */
+} hyq_params;
+
+typedef struct hyq_stats {
+  double t, dt, vmax;  /* time, last dt, last CFL wave speed (:402-433) */
+  int64_t nn;          /* steps taken */
+  int32_t done;        /* 1 once t >= tmax or nn >= nnmax */
+  int32_t status;      /* device-side status word (0 = ok) */
+} hyq_stats;
+
+typedef struct hyq_ctx hyq_ctx;
+
+int hyq_abi_version(void);
+int hyq_create(const hyq_params* p, hyq_ctx** out);
+void hyq_destroy(hyq_ctx* ctx);
+const char* hyq_last_error(const hyq_ctx* ctx);
+
+/* Host (Nx,Ny,Nz,35) column-major buffers; time and step count reset to 0
+ * by hyq_set_state (simulation_runner's t = 0.0; nn = 0, :333-334). */
+int hyq_set_state(hyq_ctx* ctx, const double* M);
+int hyq_get_state(hyq_ctx* ctx, double* M);
+/* Device-pointer variants (same layout, device memory of ctx's device). */
+int hyq_set_state_device(hyq_ctx* ctx, const double* dM);
+int hyq_get_state_device(hyq_ctx* ctx, double* dM);
+/* Set the loop clock (t, nn) without touching the state. */
+int hyq_set_clock(hyq_ctx* ctx, double t, int64_t nn);
+
+/* Run up to max_steps steps of the reference loop, stopping on the device
+ * once t >= tmax or nn >= nnmax.  Outputs may be NULL. */
+int hyq_advance(hyq_ctx* ctx, int64_t max_steps, double* t, int64_t* nn, int32_t* done);
+/* Same, asynchronous on the context's stream (no host synchronization). */
+int hyq_advance_async(hyq_ctx* ctx, int64_t max_steps);
+int hyq_synchronize(hyq_ctx* ctx);
+int hyq_stats_get(hyq_ctx* ctx, hyq_stats* out);
+
+/* Standardized and central moment fields of the current state, host
+ * (Nx,Ny,Nz,35) buffers (either may be NULL). */
+int hyq_get_SC(hyq_ctx* ctx, double* S, double* C);
+
+/* cudaStream_t of the context, for callers that order their own work. */
+void* hyq_stream(hyq_ctx* ctx);
+
+/* Run `steps` steps launching the four step kernels individually (not the
+ * graph) with CUDA events around each on the context stream; ms[4] receives
+ * the summed device time of phase A, the CFL reduction, the HLL sweep and
+ * phase E+F.  For profiling; results equal hyq_advance. */
+int hyq_advance_timed(hyq_ctx* ctx, int64_t steps, float* ms);
+
+/* ---- per-cell entry points on device arrays (SoA, stride n) ------------
+ * Used by parity tests and by callers composing their own loops.  `stream`
+ * is a cudaStream_t (NULL = default stream).  Arrays are device pointers. */
+/* Flux_closure35_and_realizable_3D (src/numerics/Flux_closure35_and_realizable_3D.jl:33). */
+int hyq_cells_flux_closure(const double* M, int64_t n, int32_t flag2D, double Ma, double* Fx, double* Fy, double* Fz,
+                           double* Mr, void* stream);
+/* eigenvalues6_hyperbolic_3D (axis 1, 2) and eigenvalues6z_hyperbolic_3D (axis 3):
+ * v[2n] = (vmin, vmax) pairs, Mr the corrected moments
+ * (src/numerics/eigenvalues6_hyperbolic_3D.jl:22, eigenvalues6z_hyperbolic_3D.jl:23). */
+int hyq_cells_eigenvalues(const double* M, int64_t n, int32_t axis, int32_t flag2D, double Ma, int32_t positivity,
+                          double* v, double* Mr, void* stream);
+/* closure_and_eigenvalues on 5 moments per cell (src/numerics/closure_and_eigenvalues.jl:76):
+ * mom[5n] SoA, v[2n] = (vmin, vmax). */
+int hyq_cells_closure_eigs(const double* mom, int64_t n, double* v, void* stream);
+/* collision35 (src/numerics/collision35.jl:154). */
+int hyq_cells_collision(const double* M, int64_t n, double dt, double Kn, int32_t positivity, double* out, void* stream);
+/* Phase [A] of the step (src/simulation_runner.jl:357-379): fluxes, realizable
+ * moments and the six wave-speed arrays vp[6n] = (xmin,xmax,ymin,ymax,zmin,zmax). */
+int hyq_cells_phase_A(const double* M, int64_t n, int32_t flag2D, double Ma, int32_t positivity, double* Fx, double* Fy,
+                      double* Fz, double* Mr, double* vp, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HYQMOM_B200_H */

@@ -258,12 +258,13 @@ template <class T, int N> int eig_real(const T (&Ain)[N][N], T (&wr)[N], T (&wi)
         for (int rr = 0; rr <= l; ++rr) ca = jmax(ca, T(fabs(A[rr][i])));
         for (int cc = k; cc < N; ++cc) ra = jmax(ra, T(fabs(A[i][cc])));
         if (c == T(0) || r == T(0)) continue;
+        if (!std::isfinite(double(c + ca + r + ra))) return -1;  // LAPACK dgebal: NaN -> error return
         T g = r / radix, f = T(1), s = c + r;
-        while (!(c >= g || jmax(jmax(f, c), ca) >= sfmax2 || jmin(jmin(r, g), ra) <= sfmin2)) {
+        for (int guard2 = 0; guard2 < 2200 && !(c >= g || jmax(jmax(f, c), ca) >= sfmax2 || jmin(jmin(r, g), ra) <= sfmin2); ++guard2) {
           f = f * radix; c = c * radix; ca = ca * radix; r = r / radix; g = g / radix; ra = ra / radix;
         }
         g = c / radix;
-        while (!(g < r || jmax(r, ra) >= sfmax2 || jmin(jmin(jmin(f, c), g), ca) <= sfmin2)) {
+        for (int guard3 = 0; guard3 < 2200 && !(g < r || jmax(r, ra) >= sfmax2 || jmin(jmin(jmin(f, c), g), ca) <= sfmin2); ++guard3) {
           f = f / radix; c = c / radix; g = g / radix; ca = ca / radix; r = r * radix; ra = ra * radix;
         }
         if ((c + r) >= factor * s) continue;

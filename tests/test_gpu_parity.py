@@ -1,0 +1,216 @@
+"""CUDA path vs the CPU oracle (FP64 throughout).
+
+Tolerances: <= 1e-12 relative for one step and per-cell
+functions, <= 1e-8 relative on all 35 moments after 100 steps.  "Relative" is
+max |gpu - oracle| / max |oracle| over each moment field (a per-field scale:
+the 35 moments span many orders of magnitude, and near-zero odd moments of a
+symmetric state have no meaningful pointwise relative error).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from hyqmom import ic
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hyqmom import _lib
+    return _lib.load()
+
+
+def field_rel(a, b, axis=-1):
+    a, b = np.asarray(a), np.asarray(b)
+    a = np.moveaxis(a, axis, 0).reshape(a.shape[axis], -1)
+    b = np.moveaxis(b, axis, 0).reshape(b.shape[axis], -1)
+    scale = np.maximum(np.max(np.abs(b), axis=1), 1e-300)
+    return float(np.max(np.max(np.abs(a - b), axis=1) / scale))
+
+
+def sample_states(n=384, seed=7):
+    """Cell states from the crossing-jets IC after a few oracle steps plus
+    random Gaussian-mixture moments (realizable, varied velocity/temperature)."""
+    rng = np.random.default_rng(seed)
+    p = ic.with_jets(ic.default_params(Nx=8, Ny=8, Nz=8, Ma=1.0, Kn=1.0, CFL=0.7, tmax=10.0), "crossing")
+    M = ic.initial_state(p)
+    g = ic.grid_spacing(p)
+    pp = dict(p, **g)
+    t = 0.0
+    for _ in range(3):
+        _, t, _ = ol.step(M, pp, t)
+    cells = M.reshape(-1, 35)
+    out = [cells]
+    E35 = ic.E35
+    for _ in range(n - cells.shape[0]):
+        k = rng.integers(2, 5)
+        w = rng.dirichlet(np.ones(k)) * (0.01 + rng.random())
+        mu = rng.normal(0, 1.0, size=(k, 3))
+        X = []
+        for q in range(k):
+            A = rng.normal(size=(3, 3))
+            C = A @ A.T / 3 + 0.2 * np.eye(3)
+            X.append((w[q], mu[q], C))
+        # exact Gaussian-mixture raw moments
+        m = np.zeros(35)
+        for (wq, muq, Cq) in X:
+            r = np.sqrt(np.diag(Cq))
+            corr = Cq / np.outer(r, r)
+            m += ic.gaussian_moments(wq, muq[0], muq[1], muq[2], Cq[0, 0], Cq[0, 1], Cq[0, 2], Cq[1, 1], Cq[1, 2], Cq[2, 2]) \
+                if abs(corr[0, 1]) < 1 else 0
+        out.append(m[None, :])
+    return np.concatenate(out, axis=0)[:n]
+
+
+def to_dev(cells):
+    """(n,35) -> device SoA (35, n) contiguous."""
+    return torch.tensor(np.ascontiguousarray(cells.T), dtype=torch.float64, device="cuda")
+
+
+@pytest.fixture(scope="module")
+def states():
+    return sample_states()
+
+
+def test_flux_closure_cells(states):
+    lib = cuda()
+    n = states.shape[0]
+    dM = to_dev(states)
+    outs = [torch.empty_like(dM) for _ in range(4)]
+    assert lib.hyq_cells_flux_closure(dM.data_ptr(), n, 0, 1.0, *[o.data_ptr() for o in outs], None) == 0
+    torch.cuda.synchronize()
+    got = [o.cpu().numpy().T for o in outs]
+    ref = [np.array(x) for x in zip(*[ol.flux_closure35(s, 0, 1.0) for s in states])]
+    for g, r in zip(got, ref):
+        assert field_rel(g, r) < 1e-12
+
+
+@pytest.mark.parametrize("axis", [1, 2, 3])
+def test_eigenvalues_cells(states, axis):
+    lib = cuda()
+    n = states.shape[0]
+    dM = to_dev(states)
+    v = torch.empty(2, n, dtype=torch.float64, device="cuda")
+    Mr = torch.empty_like(dM)
+    assert lib.hyq_cells_eigenvalues(dM.data_ptr(), n, axis, 0, 1.0, 1, v.data_ptr(), Mr.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    gv, gM = v.cpu().numpy().T, Mr.cpu().numpy().T
+    for c in range(n):
+        if axis == 3:
+            a, b, r = ol.eigenvalues6z(states[c], 0, 1.0, True)
+        else:
+            a, b, r = ol.eigenvalues6(states[c], axis, 0, 1.0)
+        scale = max(abs(a), abs(b), 1e-300)
+        assert abs(gv[c, 0] - a) <= 1e-12 * scale and abs(gv[c, 1] - b) <= 1e-12 * scale, (c, gv[c], a, b)
+    ref = np.array([ol.eigenvalues6z(s, 0, 1.0, True)[2] if axis == 3 else ol.eigenvalues6(s, axis, 0, 1.0)[2] for s in states])
+    assert field_rel(gM, ref) < 1e-12
+
+
+def test_closure_eigs_and_collision(states):
+    lib = cuda()
+    n = states.shape[0]
+    mom = np.ascontiguousarray(states[:, [0, 1, 2, 3, 4]])
+    dmom = to_dev(mom)
+    v = torch.empty(2, n, dtype=torch.float64, device="cuda")
+    assert lib.hyq_cells_closure_eigs(dmom.data_ptr(), n, v.data_ptr(), None) == 0
+    dM = to_dev(states)
+    out = torch.empty_like(dM)
+    assert lib.hyq_cells_collision(dM.data_ptr(), n, 1e-3, 0.1, 1, out.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    gv = v.cpu().numpy().T
+    for c in range(n):
+        _, a, b = ol.closure_and_eigenvalues(mom[c])
+        scale = max(abs(a), abs(b), 1e-300)
+        assert abs(gv[c, 0] - a) <= 1e-12 * scale and abs(gv[c, 1] - b) <= 1e-12 * scale
+    ref = np.array([ol.collision35(s, 1e-3, 0.1) for s in states])
+    assert field_rel(out.cpu().numpy().T, ref) < 1e-12
+
+
+def run_gpu(p, nsteps):
+    from hyqmom.runner import Solver
+    s = Solver(p)
+    try:
+        s.set_state(ic.initial_state(p))
+        t, nn, done = s.advance(nsteps)
+        return s.get_state(), t, nn
+    finally:
+        s.close()
+
+
+def run_oracle(p, nsteps):
+    M = ic.initial_state(p)
+    pp = dict(p, **ic.grid_spacing(p))
+    t, nn = 0.0, 0
+    while t < p["tmax"] and nn < min(nsteps, p["nnmax"]):
+        _, t, _ = ol.step(M, pp, t)
+        nn += 1
+    return M, t, nn
+
+
+@pytest.mark.parametrize("name", ["small", "medium"])
+def test_gpu_end_to_end_nz1_golden(name):
+    """The CUDA path against the reference's own end-to-end goldens."""
+    cuda()
+    g = np.load(os.path.join(GOLD, f"mpi_1rank_{name}.npz"))
+    Np, tmax = int(g["Np"]), float(g["tmax"])
+    p = ic.run_simulation_params(Nx=Np, Ny=Np, Nz=1, tmax=tmax, Kn=1.0, Ma=0.0, flag2D=0, CFL=0.5)
+    M, t, nn = run_gpu(p, 1000)
+    assert nn == int(g["steps"]) and t == float(g["tfinal"])
+    np.testing.assert_allclose(M[:, :, 0, :], g["M"], atol=1e-12, rtol=0)
+
+
+def crossing_c1(**kw):
+    """Crossing jets, 20^3, Ma=0, Kn=1, CFL=0.7, dtmax=1e-2, 100 steps."""
+    base = dict(Nx=20, Ny=20, Nz=20, Ma=0.0, Kn=1.0, CFL=0.7, dtmax=1e-2, tmax=10.0, nnmax=100, flag2D=0)
+    base.update(kw)
+    return ic.with_jets(ic.default_params(**base), "crossing")
+
+
+def test_one_step_matches_oracle():
+    cuda()
+    p = crossing_c1(Ma=1.0, nnmax=1)
+    Mg, tg, _ = run_gpu(p, 1)
+    Mo, to, _ = run_oracle(p, 1)
+    assert abs(tg - to) <= 1e-14 * to
+    assert field_rel(Mg, Mo) < 1e-12
+
+
+def test_hardcoded_ic_steps_match_oracle():
+    cuda()
+    p = ic.run_simulation_params(Nx=16, Ny=16, Nz=6, tmax=10.0, Kn=1.0, Ma=1.0, CFL=0.5)
+    p["nnmax"] = 10
+    Mg, tg, _ = run_gpu(p, 10)
+    Mo, to, _ = run_oracle(p, 10)
+    assert abs(tg - to) <= 1e-12 * to
+    assert field_rel(Mg, Mo) < 1e-10
+
+
+@pytest.mark.slow
+def test_hundred_steps_crossing_c1():
+    cuda()
+    p = crossing_c1()
+    Mg, tg, ng = run_gpu(p, 100)
+    Mo, to, no = run_oracle(p, 100)
+    assert ng == no == 100
+    assert abs(tg - to) <= 1e-10 * to
+    assert field_rel(Mg, Mo) < 1e-8
+
+
+def test_conservation_of_mass_and_momentum():
+    """Interior HLL is conservative and BGK conserves rho, rho*u: with the jets
+    away from the walls, total mass and momentum are constant to round-off."""
+    cuda()
+    p = crossing_c1(Ma=1.0, nnmax=20)
+    M0 = ic.initial_state(p)
+    Mg, _, nn = run_gpu(p, 20)
+    for n in (0, 1, 5, 15):
+        a, b = M0[..., n].sum(), Mg[..., n].sum()
+        scale = np.abs(M0[..., n]).sum()
+        assert abs(a - b) <= 1e-12 * scale * max(1, nn), (n, a, b)
