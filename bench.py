@@ -39,11 +39,17 @@ B_ALG = 2 * 35 * 8  # bytes per cell-step: state read once, written once
 def workload(name="c2"):
     from hyqmom import ic
     if name == "c2":
-        p = ic.default_params(Nx=160, Ny=160, Nz=80, Ma=1.0, Kn=1.0, CFL=0.7, tmax=1e9, nnmax=200)
+        # CFL 0.5: at the named CFL 0.7 the reference scheme empties a jet-corner
+        # cell in step 1 and its flux Jacobian is NaN in step 2 (the reference's
+        # eigvals throws there); 0.5 is the largest of {0.3, 0.5, 0.7} that runs
+        p = ic.default_params(Nx=160, Ny=160, Nz=80, Ma=1.0, Kn=1.0, CFL=0.5, tmax=1e9, nnmax=1000000)
     elif name == "c5":
-        p = ic.default_params(Nx=256, Ny=256, Nz=128, Ma=1.0, Kn=0.01, CFL=0.7, tmax=1e9, nnmax=500)
+        p = ic.default_params(Nx=256, Ny=256, Nz=128, Ma=1.0, Kn=0.01, CFL=0.5, tmax=1e9, nnmax=1000000)
+    elif name == "c2s":
+        # the same case on 96 x 96 x 48 cells: profiling captures (ncu)
+        p = ic.default_params(Nx=96, Ny=96, Nz=48, Ma=1.0, Kn=1.0, CFL=0.5, tmax=1e9, nnmax=1000000)
     elif name == "c1":
-        p = ic.default_params(Nx=20, Ny=20, Nz=20, Ma=0.0, Kn=1.0, CFL=0.7, tmax=1e9, nnmax=100)
+        p = ic.default_params(Nx=20, Ny=20, Nz=20, Ma=0.0, Kn=1.0, CFL=0.7, tmax=1e9, nnmax=1000000)
     else:
         raise ValueError(name)
     return ic.with_jets(p, "crossing")
@@ -93,7 +99,7 @@ class ClockSampler:
         sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
         mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[q] for r in self.rows for q in range(4) if len(r) > 3 + q and "Active" in r[3 + q]})
+        reasons = sorted({names[q] for r in self.rows for q in range(4) if len(r) > 3 + q and r[3 + q].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
                 "samples": len(self.rows)}
 
@@ -189,6 +195,7 @@ def run_gpu(args, rank, world, local_rank):
         barrier()
     ms = e0.elapsed_time(e1)
     st = s.stats()
+    assert st["status"] == 0 and st["nn"] == args.warmup + args.steps, f"steps did not all run: {st}"
     if dist is not None:
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -270,7 +277,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c5"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c2s", "c5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--count-ops", action="store_true")
     args = ap.parse_args()

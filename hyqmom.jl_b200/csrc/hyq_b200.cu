@@ -45,6 +45,11 @@ __global__ void __launch_bounds__(1024) k_cfl(const double* __restrict__ blockma
   for (int b = threadIdx.x; b < sc.nblocksA; b += 1024) v = nanmax(v, blockmax[b]);
   const double vmax = block_nanmax<1024>(v);
   if (threadIdx.x == 0) {
+    // A non-finite wave speed: the reference's eigvals would throw here
+    // (src/numerics/eigenvalues6z_hyperbolic_3D.jl:108); the step still runs
+    // with the NaN dt exactly as the Julia arithmetic would, and the status
+    // word records the step at which it happened.
+    if (!(vmax == vmax) || isinf(vmax)) { if (clk->status == 0) clk->status = (int)(clk->nn + 1); }
     double dt = jmin(sc.CFL * jmin(jmin(sc.dx, sc.dy), sc.dz) / vmax, jmin(sc.dtmax, sc.Kn));
     dt = jmin(dt, sc.tmax - clk->t);
     clk->vmax = vmax;
@@ -340,6 +345,10 @@ int hyq_advance(hyq_ctx* ctx, int64_t max_steps, double* t, int64_t* nn, int32_t
   if (t) *t = st.t;
   if (nn) *nn = st.nn;
   if (done) *done = st.done;
+  if (st.status > 0)
+    return fail(ctx, HYQ_ENONFINITE,
+                "non-finite CFL wave speed at step " + std::to_string(st.status) +
+                    " (a flux Jacobian with Inf/NaN entries; the reference's eigvals throws there)");
   return HYQ_OK;
 }
 

@@ -50,7 +50,7 @@ typedef struct hyq_stats {
   double t, dt, vmax;  /* time, last dt, last CFL wave speed (:402-433) */
   int64_t nn;          /* steps taken */
   int32_t done;        /* 1 once t >= tmax or nn >= nnmax */
-  int32_t status;      /* device-side status word (0 = ok) */
+  int32_t status;      /* 0 = ok; k > 0: step k met a non-finite wave speed */
 } hyq_stats;
 
 typedef struct hyq_ctx hyq_ctx;
@@ -71,7 +71,10 @@ int hyq_get_state_device(hyq_ctx* ctx, double* dM);
 int hyq_set_clock(hyq_ctx* ctx, double t, int64_t nn);
 
 /* Run up to max_steps steps of the reference loop, stopping on the device
- * once t >= tmax or nn >= nnmax.  Outputs may be NULL. */
+ * once t >= tmax or nn >= nnmax.  Outputs may be NULL.  Returns
+ * HYQ_ENONFINITE (outputs still filled) once a step met a non-finite CFL wave
+ * speed: the reference's eigvals throws at that point; here t becomes NaN
+ * and the loop predicate stops further steps. */
 int hyq_advance(hyq_ctx* ctx, int64_t max_steps, double* t, int64_t* nn, int32_t* done);
 /* Same, asynchronous on the context's stream (no host synchronization). */
 int hyq_advance_async(hyq_ctx* ctx, int64_t max_steps);

@@ -39,7 +39,7 @@ def sample_states(n=384, seed=7):
     """Cell states from the crossing-jets IC after a few oracle steps plus
     random Gaussian-mixture moments (realizable, varied velocity/temperature)."""
     rng = np.random.default_rng(seed)
-    p = ic.with_jets(ic.default_params(Nx=8, Ny=8, Nz=8, Ma=1.0, Kn=1.0, CFL=0.7, tmax=10.0), "crossing")
+    p = ic.with_jets(ic.default_params(Nx=8, Ny=8, Nz=8, Ma=1.0, Kn=1.0, CFL=0.5, tmax=10.0), "crossing")
     M = ic.initial_state(p)
     g = ic.grid_spacing(p)
     pp = dict(p, **g)
@@ -175,7 +175,7 @@ def crossing_c1(**kw):
 
 def test_one_step_matches_oracle():
     cuda()
-    p = crossing_c1(Ma=1.0, nnmax=1)
+    p = crossing_c1(Ma=1.0, CFL=0.5, nnmax=1)
     Mg, tg, _ = run_gpu(p, 1)
     Mo, to, _ = run_oracle(p, 1)
     assert abs(tg - to) <= 1e-14 * to
@@ -207,10 +207,33 @@ def test_conservation_of_mass_and_momentum():
     """Interior HLL is conservative and BGK conserves rho, rho*u: with the jets
     away from the walls, total mass and momentum are constant to round-off."""
     cuda()
-    p = crossing_c1(Ma=1.0, nnmax=20)
+    p = crossing_c1(Ma=1.0, CFL=0.5, nnmax=5)
     M0 = ic.initial_state(p)
-    Mg, _, nn = run_gpu(p, 20)
+    Mg, _, nn = run_gpu(p, 5)
+    assert nn == 5
     for n in (0, 1, 5, 15):
         a, b = M0[..., n].sum(), Mg[..., n].sum()
         scale = np.abs(M0[..., n]).sum()
         assert abs(a - b) <= 1e-12 * scale * max(1, nn), (n, a, b)
+
+
+def test_nonfinite_wave_speed_is_reported():
+    """Crossing jets Ma=1 at CFL 0.7: the scheme's x+y+z-2M combination leaves a
+    non-realizable jet-corner cell after step 1 and its flux Jacobian is NaN in
+    step 2 (the reference's eigvals throws there).  The oracle and the GPU agree
+    on that, and the library reports it as HYQ_ENONFINITE with t = NaN."""
+    cuda()
+    from hyqmom import _lib
+    from hyqmom.runner import Solver
+    p = crossing_c1(Ma=1.0, CFL=0.7, nnmax=5)
+    s = Solver(p)
+    try:
+        s.set_state(ic.initial_state(p))
+        with pytest.raises(_lib.HyqError, match="HYQ_ENONFINITE"):
+            s.advance(5)
+        st = s.stats()
+        assert st["status"] == 2 and st["nn"] == 2 and st["t"] != st["t"]
+    finally:
+        s.close()
+    Mo, to, no = run_oracle(p, 5)
+    assert no == 2 and to != to
