@@ -45,6 +45,49 @@ HQD double pow4(double x) { double y = x * x; return y * y; }
 HQD double pow5(double x) { double y = x * x; return y * y * x; }
 HQD double qnan() { return __longlong_as_double(0x7ff8000000000000LL); }
 
+// exp(x) written here (Cody-Waite reduction x = k ln2 + r, |r| <= ln2/2, the
+// Taylor series of exp(r) to degree 14 by Horner, scaling by 2^k), so that
+// the device code and the CPU oracle round identically; accuracy ~1 ulp.
+HQD double hexp(double x) {
+  if (x != x) return x;
+  if (x > 709.782712893384) return __longlong_as_double(0x7ff0000000000000LL);
+  if (x < -745.1332191019412) return 0.0;
+  const double k = rint(x * 1.4426950408889634);
+  const double r = (x - k * 0.6931471803691238) - k * 1.9082149292705877e-10;
+  double p = 1.1470745597729725e-11;
+  p = p * r + 1.6059043836821613e-10;
+  p = p * r + 2.08767569878681e-09;
+  p = p * r + 2.505210838544172e-08;
+  p = p * r + 2.755731922398589e-07;
+  p = p * r + 2.7557319223985893e-06;
+  p = p * r + 2.48015873015873e-05;
+  p = p * r + 0.0001984126984126984;
+  p = p * r + 0.001388888888888889;
+  p = p * r + 0.008333333333333333;
+  p = p * r + 0.041666666666666664;
+  p = p * r + 0.16666666666666666;
+  p = p * r + 0.5;
+  p = p * r + 1.0;
+  p = p * r + 1.0;
+  return ldexp(p, (int)k);
+}
+
+// Real cube root written here (exponent split into a multiple of 3, Newton
+// iterations on the mantissa), identical on device and in the oracle.
+HQD double hcbrt(double x) {
+  if (x == 0.0 || x != x || isinf(x)) return x;
+  int e;
+  double m = frexp(fabs(x), &e);
+  int rr = e % 3;
+  if (rr < 0) rr += 3;
+  m = ldexp(m, rr);
+  e -= rr;
+  double y = 0.7 + 0.25 * m;
+  for (int it = 0; it < 7; ++it) y = y - (y * y * y - m) / (3.0 * y * y);
+  y = ldexp(y, e / 3);
+  return x < 0.0 ? -y : y;
+}
+
 // 35-moment order (src/utils/moment_idx.jl:73-76) as exponent tables.
 __device__ constexpr int T_EXI[35] = {0,1,2,3,4,0,1,2,3,0,1,2,0,1,0,0,1,2,3,0,1,2,0,1,0,0,1,2,0,1,0,0,1,0,0};
 __device__ constexpr int T_EXJ[35] = {0,0,0,0,0,1,1,1,1,2,2,2,3,3,4,0,0,0,0,0,0,0,0,0,0,1,1,1,2,2,3,1,1,1,2};
@@ -62,61 +105,68 @@ HQD int idx35(int i, int j, int k) { return T_IDX35[i * 36 + j * 6 + k]; }
 HQD int binom(int n, int k) { return T_BIN[n * 7 + k]; }
 
 // ------------------------------------------------------------ conversions
+// 56-entry moment storage (order <= 5): the 35 moments of order <= 4 in the
+// reference order, then the 21 fifth-order moments in the closure order.
+__device__ constexpr unsigned char T_EX56I[56] = {0,1,2,3,4,0,1,2,3,0,1,2,0,1,0,0,1,2,3,0,1,2,0,1,0,0,1,2,0,1,0,0,1,0,0,5,4,3,2,1,4,3,2,1,3,2,1,2,1,1,0,0,0,0,0,0};
+__device__ constexpr unsigned char T_EX56J[56] = {0,0,0,0,0,1,1,1,1,2,2,2,3,3,4,0,0,0,0,0,0,0,0,0,0,1,1,1,2,2,3,1,1,1,2,0,1,2,3,4,0,0,0,0,1,2,3,1,1,2,5,4,3,2,1,0};
+__device__ constexpr unsigned char T_EX56K[56] = {0,0,0,0,0,0,0,0,0,0,0,0,0,0,0,1,1,1,1,2,2,2,3,3,4,1,1,1,1,1,1,2,2,3,2,0,0,0,0,0,1,2,3,4,1,1,1,2,3,2,0,1,2,3,4,5};
+__device__ constexpr signed char T_IDX56[216] = {0,15,19,22,24,55,5,25,31,33,54,-1,9,28,34,53,-1,-1,12,30,52,-1,-1,-1,14,51,-1,-1,-1,-1,50,-1,-1,-1,-1,-1,1,16,20,23,43,-1,6,26,32,48,-1,-1,10,29,49,-1,-1,-1,13,46,-1,-1,-1,-1,39,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,2,17,21,42,-1,-1,7,27,47,-1,-1,-1,11,45,-1,-1,-1,-1,38,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,3,18,41,-1,-1,-1,8,44,-1,-1,-1,-1,37,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,4,40,-1,-1,-1,-1,36,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,35,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1};
+// pass orders of the separable shift transforms (exponent of the axis descending)
+__device__ constexpr unsigned char T_L35X[35] = {4,3,8,18,2,7,11,17,21,27,1,6,10,13,16,20,23,26,29,32,0,5,9,12,14,15,19,22,24,25,28,30,31,33,34};
+__device__ constexpr unsigned char T_L35Y[35] = {14,12,13,30,9,10,11,28,29,34,5,6,7,8,25,26,27,31,32,33,0,1,2,3,4,15,16,17,18,19,20,21,22,23,24};
+__device__ constexpr unsigned char T_L35Z[35] = {24,22,23,33,19,20,21,31,32,34,15,16,17,18,25,26,27,28,29,30,0,1,2,3,4,5,6,7,8,9,10,11,12,13,14};
+__device__ constexpr unsigned char T_L56X[56] = {35,4,36,40,3,8,18,37,41,44,2,7,11,17,21,27,38,42,45,47,1,6,10,13,16,20,23,26,29,32,39,43,46,48,49,0,5,9,12,14,15,19,22,24,25,28,30,31,33,34,50,51,52,53,54,55};
+__device__ constexpr unsigned char T_L56Y[56] = {50,14,39,51,12,13,30,38,46,52,9,10,11,28,29,34,37,45,49,53,5,6,7,8,25,26,27,31,32,33,36,44,47,48,54,0,1,2,3,4,15,16,17,18,19,20,21,22,23,24,35,40,41,42,43,55};
+__device__ constexpr unsigned char T_L56Z[56] = {55,24,43,54,22,23,33,42,48,53,19,20,21,31,32,34,41,47,49,52,15,16,17,18,25,26,27,28,29,30,40,44,45,46,51,0,1,2,3,4,5,6,7,8,9,10,11,12,13,14,35,36,37,38,39,50};
+// 28-set index of each stored moment (-1: order 0, 1, diagonal 2, or 5)
+__device__ constexpr signed char T_S28OF56[56] = {-1,-1,-1,0,1,-1,2,3,4,-1,5,6,7,8,9,-1,10,11,12,-1,13,14,15,16,17,18,19,20,21,22,23,24,25,26,27,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1};
+// storage index of the x/y/z flux moment of each of the 35 moments
+__device__ constexpr unsigned char T_FX[35] = {1,2,3,4,35,6,7,8,36,10,11,37,13,38,39,16,17,18,40,20,21,41,23,42,43,26,27,44,29,45,46,32,47,48,49};
+__device__ constexpr unsigned char T_FY[35] = {5,6,7,8,36,9,10,11,37,12,13,38,14,39,50,25,26,27,44,31,32,47,33,48,54,28,29,45,30,46,51,34,49,53,52};
+__device__ constexpr unsigned char T_FZ[35] = {15,16,17,18,40,25,26,27,44,28,29,45,30,46,51,19,20,21,41,22,23,42,24,43,55,31,32,47,34,49,52,33,48,54,53};
+
+// Separable binomial shift of stored moments along one axis (n = 35: order
+// <= 4, n = 56: order <= 5):  A_ijk <- sum_{a <= i} C(i,a) s^(i-a) A_ajk
+// (x axis shown).  Entries are visited with the axis exponent descending, so
+// the update is in place.  Raw <-> central conversions are three such passes,
+// one per axis, instead of the full triple sums.
+HQN void shift_axis(double* A, int n, int axis, double sh) {
+  double pw[6];
+  pw[0] = 1.0;
+  for (int q = 1; q < 6; ++q) pw[q] = pw[q - 1] * sh;
+  const unsigned char* L = (n == 35) ? (axis == 0 ? T_L35X : axis == 1 ? T_L35Y : T_L35Z) : (axis == 0 ? T_L56X : axis == 1 ? T_L56Y : T_L56Z);
+  const int stride = axis == 0 ? 36 : axis == 1 ? 6 : 1;
+  for (int t = 0; t < n; ++t) {
+    const int q = L[t];
+    const int e = axis == 0 ? T_EX56I[q] : axis == 1 ? T_EX56J[q] : T_EX56K[q];
+    if (e == 0) continue;
+    const int base = T_EX56I[q] * 36 + T_EX56J[q] * 6 + T_EX56K[q] - e * stride;
+    double acc = 0.0;
+    for (int a = 0; a <= e; ++a) acc = acc + (double(T_BIN[e * 7 + a]) * pw[e - a]) * A[T_IDX56[base + a * stride]];
+    A[q] = acc;
+  }
+}
+
 // Central moments C (35-order, C000=1, first order 0) of raw M
 // (M4toC4_3D, src/autogen/M4toC4_3D.jl:42-55).
 HQD void raw_to_central(const double* M, double* C) {
   const double inv = 1.0 / M[0];
-  const double nu = -(M[1] * inv), nv = -(M[5] * inv), nw = -(M[15] * inv);
-  double pu[5], pv[5], pw[5];
-  pu[0] = pv[0] = pw[0] = 1.0;
-#pragma unroll
-  for (int q = 1; q < 5; ++q) { pu[q] = pu[q - 1] * nu; pv[q] = pv[q - 1] * nv; pw[q] = pw[q - 1] * nw; }
-  double Mn[35];
-#pragma unroll
-  for (int n = 0; n < 35; ++n) Mn[n] = M[n] * inv;
-#pragma unroll
-  for (int n = 0; n < 35; ++n) {
-    const int i = ex_i(n), j = ex_j(n), k = ex_k(n);
-    double s = 0.0;
-#pragma unroll
-    for (int a = 0; a <= 4; ++a)
-#pragma unroll
-      for (int b = 0; b <= 4; ++b)
-#pragma unroll
-        for (int c = 0; c <= 4; ++c) {
-          if (a > i || b > j || c > k) continue;
-          const double coef = double(binom(i, a) * binom(j, b) * binom(k, c));
-          s = s + coef * Mn[idx35(a, b, c)] * (pu[i - a] * pv[j - b] * pw[k - c]);
-        }
-    C[n] = s;
-  }
+  const double u = M[1] * inv, v = M[5] * inv, w = M[15] * inv;
+  for (int n = 0; n < 35; ++n) C[n] = M[n] * inv;
+  shift_axis(C, 35, 0, -u);
+  shift_axis(C, 35, 1, -v);
+  shift_axis(C, 35, 2, -w);
   C[0] = 1.0; C[1] = 0.0; C[5] = 0.0; C[15] = 0.0;
 }
 
-// Raw moments of order <= 4 from density, mean and central moments
-// (C4toM4_3D, src/autogen/C4toM4_3D.jl:64-118).  C uses the 35-order.
-HQD void central_to_raw4(double M000, double u, double v, double w, const double* C, double* M) {
-  double pu[5], pv[5], pw[5];
-  pu[0] = pv[0] = pw[0] = 1.0;
-#pragma unroll
-  for (int q = 1; q < 5; ++q) { pu[q] = pu[q - 1] * u; pv[q] = pv[q - 1] * v; pw[q] = pw[q - 1] * w; }
-#pragma unroll
-  for (int n = 0; n < 35; ++n) {
-    const int i = ex_i(n), j = ex_j(n), k = ex_k(n);
-    double s = 0.0;
-#pragma unroll
-    for (int a = 0; a <= 4; ++a)
-#pragma unroll
-      for (int b = 0; b <= 4; ++b)
-#pragma unroll
-        for (int c = 0; c <= 4; ++c) {
-          if (a > i || b > j || c > k || a + b + c == 1) continue;
-          const double coef = double(binom(i, a) * binom(j, b) * binom(k, c));
-          const double cm = (a + b + c == 0) ? 1.0 : C[idx35(a, b, c)];
-          s = s + coef * cm * (pu[i - a] * pv[j - b] * pw[k - c]);
-        }
-    M[n] = M000 * s;
-  }
+// Raw moments from density, mean and central moments, in place on the store
+// A (n = 35 or 56 entries; A[0] = 1 and first order 0 on entry)
+// (C4toM4_3D / C5toM5_3D, src/autogen/C4toM4_3D.jl:64-118, C5toM5_3D.jl:16-28).
+HQD void central_to_raw(double M000, double u, double v, double w, double* A, int n) {
+  shift_axis(A, n, 0, u);
+  shift_axis(A, n, 1, v);
+  shift_axis(A, n, 2, w);
+  for (int q = 0; q < n; ++q) A[q] = M000 * A[q];
 }
 
 // Standardized moments S (35-order) from central C (M2CS4_35,
@@ -336,14 +386,13 @@ struct Delta {
 __device__ constexpr int TRI[6][6] = {{0, 1, 2, 3, 4, 5}, {1, 6, 7, 8, 9, 10}, {2, 7, 11, 12, 13, 14},
                                       {3, 8, 12, 15, 16, 17}, {4, 9, 13, 16, 18, 19}, {5, 10, 14, 17, 19, 20}};
 
-template <int P> HQD void delta2star(const double* s, Delta& D, bool want_e = true) {
+HQN void delta2star_p(const double* s, int P, Delta& D) {
   // arguments of delta2star3D for permutation P (named by the argument slot)
-  const double g300 = s[PERM[P][0]], g400 = s[PERM[P][1]], g110 = s[PERM[P][2]], g210 = s[PERM[P][3]], g310 = s[PERM[P][4]],
-               g120 = s[PERM[P][5]], g220 = s[PERM[P][6]], g030 = s[PERM[P][7]], g130 = s[PERM[P][8]], g040 = s[PERM[P][9]],
-               g101 = s[PERM[P][10]], g201 = s[PERM[P][11]], g301 = s[PERM[P][12]], g102 = s[PERM[P][13]], g202 = s[PERM[P][14]],
-               g003 = s[PERM[P][15]], g103 = s[PERM[P][16]], g004 = s[PERM[P][17]], g011 = s[PERM[P][18]], g111 = s[PERM[P][19]],
-               g211 = s[PERM[P][20]], g021 = s[PERM[P][21]], g121 = s[PERM[P][22]], g031 = s[PERM[P][23]], g012 = s[PERM[P][24]],
-               g112 = s[PERM[P][25]], g013 = s[PERM[P][26]], g022 = s[PERM[P][27]];
+  const int* pm = PERM[P];
+  const double g300 = s[pm[0]], g400 = s[pm[1]], g110 = s[pm[2]], g210 = s[pm[3]], g310 = s[pm[4]], g120 = s[pm[5]], g220 = s[pm[6]],
+               g030 = s[pm[7]], g130 = s[pm[8]], g040 = s[pm[9]], g101 = s[pm[10]], g201 = s[pm[11]], g301 = s[pm[12]], g102 = s[pm[13]],
+               g202 = s[pm[14]], g003 = s[pm[15]], g103 = s[pm[16]], g004 = s[pm[17]], g011 = s[pm[18]], g111 = s[pm[19]], g211 = s[pm[20]],
+               g021 = s[pm[21]], g121 = s[pm[22]], g031 = s[pm[23]], g012 = s[pm[24]], g112 = s[pm[25]], g013 = s[pm[26]], g022 = s[pm[27]];
   // R^-1 (symmetric) of R = [1 g110 g101; g110 1 g011; g101 g011 1]
   const double c00 = 1.0 - g011 * g011, c01 = g101 * g011 - g110, c02 = g110 * g011 - g101;
   const double c11 = 1.0 - g101 * g101, c12 = g110 * g101 - g011, c22 = 1.0 - g110 * g110;
@@ -370,64 +419,48 @@ template <int P> HQD void delta2star(const double* s, Delta& D, bool want_e = tr
     for (int b = a; b < 6; ++b) {
       const double qv = mu[a] * mu[b] + (w[a][0] * z[b][0] + w[a][1] * z[b][1] + w[a][2] * z[b][2]);
       D.q[TRI[a][b]] = qv;
-      if (want_e) D.e[TRI[a][b]] = m22[TRI[a][b]] - qv;
+      D.e[TRI[a][b]] = m22[TRI[a][b]] - qv;
     }
 }
 
 HQD double E_(const Delta& D, int a, int b) { return D.e[TRI[a][b]]; }
 
-// Leading-minor determinants with Julia det semantics (LU, partial pivot;
-// triangular shortcut).
-template <int K> HQD double lead_det(const Delta& D) {
-  double A[K][K];
-#pragma unroll
+// Leading K x K minor determinant with Julia det semantics (triangular
+// shortcut, else LU with partial pivoting and reciprocal row scaling).
+HQN double lead_det(const Delta& D, int K) {
+  double A[4][4];
   for (int i = 0; i < K; ++i)
-#pragma unroll
     for (int j = 0; j < K; ++j) A[i][j] = E_(D, i, j);
   bool triu = true, tril = true;
-#pragma unroll
   for (int i = 0; i < K; ++i)
-#pragma unroll
     for (int j = 0; j < K; ++j) {
       if (i > j && A[i][j] != 0.0) triu = false;
       if (i < j && A[i][j] != 0.0) tril = false;
     }
   if (triu || tril) {
     double p = 1.0;
-#pragma unroll
     for (int i = 0; i < K; ++i) p = p * A[i][i];
     return p;
   }
   int swaps = 0;
   bool singular = false;
-#pragma unroll
   for (int k = 0; k < K; ++k) {
     int p = k;
     double amax = fabs(A[k][k]);
-#pragma unroll
     for (int i = k + 1; i < K; ++i)
       if (fabs(A[i][k]) > amax) { amax = fabs(A[i][k]); p = i; }
     if (p != k) {
-#pragma unroll
-      for (int i = k + 1; i < K; ++i)
-        if (i == p) {
-#pragma unroll
-          for (int j = 0; j < K; ++j) { const double t = A[k][j]; A[k][j] = A[i][j]; A[i][j] = t; }
-        }
+      for (int j = 0; j < K; ++j) { const double t = A[k][j]; A[k][j] = A[p][j]; A[p][j] = t; }
       ++swaps;
     }
     if (A[k][k] == 0.0) { singular = true; continue; }
     const double r = 1.0 / A[k][k];
-#pragma unroll
     for (int i = k + 1; i < K; ++i) A[i][k] = A[i][k] * r;
-#pragma unroll
     for (int i = k + 1; i < K; ++i)
-#pragma unroll
       for (int j = k + 1; j < K; ++j) A[i][j] = A[i][j] - A[i][k] * A[k][j];
   }
   if (singular) return 0.0;
   double P = 1.0;
-#pragma unroll
   for (int i = 0; i < K; ++i) P = P * A[i][i];
   return (swaps & 1) ? -P : P;
 }
@@ -449,7 +482,7 @@ HQD Roots3 cardano(double c3, double c2, double c1, double c0) {
     for (int i = 0; i < 3; ++i) { R.re[i] = sd; R.im[i] = i == 0 ? 0.0 : sd; }
     return R;
   }
-  const double C = cbrt(q + sd);
+  const double C = hcbrt(q + sd);
   const double pc = p / C;
   const double sh = B / 3.0;
   const double s3 = 1.7320508075688772;  // sqrt(3)

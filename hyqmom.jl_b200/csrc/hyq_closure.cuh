@@ -95,7 +95,7 @@ HQN int realizable_3D(double* s) {
 
   const double beta = 1.0;
   Delta D;
-  delta2star<0>(s, D);
+  delta2star_p(s, 0, D);
   int fE11 = 0, fE22 = 0, fE33 = 0, fE44 = 0, fE55 = 0, fE66 = 0;
   if (E_(D, 0, 0) < 0.0) { realizability_S210(s[s110], s[s101], s[s011], s[s300], s[s210], s[s201], H200, beta); fE11 = 1; }
   if (E_(D, 3, 3) < 0.0) { realizability_S210(s[s110], s[s011], s[s101], s[s030], s[s120], s[s021], H020, beta); fE44 = 1; }
@@ -107,7 +107,7 @@ HQN int realizable_3D(double* s) {
   const double S022_310 = realizability_S310_220(s[s011], s[s110], s[s101], s[s021], s[s012], s[s111], s[s022]);
   double S220_diag = s[s220], S202_diag = s[s202], S022_diag = s[s022];
   // lower_bound_S220: projection diagonal of the current moments
-  delta2star<0>(s, D);
+  delta2star_p(s, 0, D);
   const double lb0 = D.q[TRI[1][1]], lb1 = D.q[TRI[2][2]], lb2 = D.q[TRI[4][4]];
   if (s[s220] < lb0) { S220_diag = lb0; fE22 = 1; flag220 = 1; }
   if (s[s202] < lb1) { S202_diag = lb1; fE33 = 1; flag220 = 1; }
@@ -136,11 +136,8 @@ HQN int realizable_3D(double* s) {
   // 2x2 minors of the six permutations
   double S220a = s[s220], S220b = s[s220], S202a = s[s202], S202b = s[s202], S022a = s[s022], S022b = s[s022];
   double d2[6], d3[6];
-  Delta P0, P1, P2, P3, P4, P5;
-  delta2star<0>(s, P0); delta2star<1>(s, P1); delta2star<2>(s, P2);
-  delta2star<3>(s, P3); delta2star<4>(s, P4); delta2star<5>(s, P5);
-  d2[0] = lead_det<2>(P0); d2[1] = lead_det<2>(P1); d2[2] = lead_det<2>(P2);
-  d2[3] = lead_det<2>(P3); d2[4] = lead_det<2>(P4); d2[5] = lead_det<2>(P5);
+  Delta P[6];
+  for (int p = 0; p < 6; ++p) { delta2star_p(s, p, P[p]); d2[p] = lead_det(P[p], 2); }
   int flag310 = 0;
   if (!fE11 && !fE44 && d2[0] < h2min) {
     s[s310] = realizability_S310(s[s110], s[s101], s[s011], s[s300], s[s210], s[s120], s[s201], s[s111], s[s310], s[s220], H200, beta);
@@ -176,10 +173,12 @@ HQN int realizable_3D(double* s) {
   double S202_310r = S202_310;
   if (s[s202] < S202r) { S202_310r = S202r; flag220 = 1; }
   if (flag310) {
-    delta2star<0>(s, P0); delta2star<1>(s, P1); delta2star<2>(s, P2);
-    delta2star<3>(s, P3); delta2star<4>(s, P4); delta2star<5>(s, P5);
-    const double dm = jmin(jmin(jmin(jmin(jmin(lead_det<2>(P0), lead_det<2>(P1)), lead_det<2>(P2)), lead_det<2>(P3)), lead_det<2>(P4)),
-                           lead_det<2>(P5));
+    double dm = 0.0;
+    for (int p = 0; p < 6; ++p) {
+      delta2star_p(s, p, P[p]);
+      const double d = lead_det(P[p], 2);
+      dm = (p == 0) ? d : jmin(dm, d);
+    }
     if (dm < 0.0) flag220 = 1;
   }
 
@@ -189,9 +188,9 @@ HQN int realizable_3D(double* s) {
   S022b = s[s022];
   double S022c = s[s022];
   if (!fE11 && !fE22 && !fE33 && !fE55) {
-    d3[0] = lead_det<3>(P0); d3[1] = lead_det<3>(P1);
+    d3[0] = lead_det(P[0], 3); d3[1] = lead_det(P[1], 3);
     if (d3[0] <= h2min || d3[1] <= h2min) {
-      const double e11 = E_(P0, 0, 0), e12 = E_(P0, 0, 1), e13 = E_(P0, 0, 2), e22 = E_(P0, 1, 1), e23 = E_(P0, 1, 2), e33 = E_(P0, 2, 2);
+      const double e11 = E_(P[0], 0, 0), e12 = E_(P[0], 0, 1), e13 = E_(P[0], 0, 2), e22 = E_(P[0], 1, 1), e23 = E_(P[0], 1, 2), e33 = E_(P[0], 2, 2);
       const double d23 = s[s211] - e23, d22 = s[s220] - e22, d33 = s[s202] - e33;
       if (e11 > diagmin) { S220a = d22 + e13 * e13 / e11; S202a = d33 + e12 * e12 / e11; }
       s[s211] = realizability_S211(e11, e22, e33, e12, e13, d23, s[s211], beta);
@@ -199,9 +198,9 @@ HQN int realizable_3D(double* s) {
     }
   }
   if (!fE22 && !fE33 && !fE44 && !fE55) {
-    d3[2] = lead_det<3>(P2); d3[4] = lead_det<3>(P4);
+    d3[2] = lead_det(P[2], 3); d3[4] = lead_det(P[4], 3);
     if (d3[2] < h2min || d3[4] < h2min) {
-      const double e11 = E_(P2, 0, 0), e12 = E_(P2, 0, 1), e13 = E_(P2, 0, 2), e22 = E_(P2, 1, 1), e23 = E_(P2, 1, 2), e33 = E_(P2, 2, 2);
+      const double e11 = E_(P[2], 0, 0), e12 = E_(P[2], 0, 1), e13 = E_(P[2], 0, 2), e22 = E_(P[2], 1, 1), e23 = E_(P[2], 1, 2), e33 = E_(P[2], 2, 2);
       const double d23 = s[s121] - e23, d22 = s[s220] - e22, d33 = s[s022] - e33;
       if (e11 > diagmin) { S220b = d22 + e13 * e13 / e11; S022b = d33 + e12 * e12 / e11; }
       s[s121] = realizability_S211(e11, e22, e33, e12, e13, d23, s[s121], beta);
@@ -209,9 +208,9 @@ HQN int realizable_3D(double* s) {
     }
   }
   if (!fE22 && !fE33 && !fE55 && !fE66) {
-    d3[3] = lead_det<3>(P3); d3[5] = lead_det<3>(P5);
+    d3[3] = lead_det(P[3], 3); d3[5] = lead_det(P[5], 3);
     if (d3[3] < h2min || d3[5] < h2min) {
-      const double e11 = E_(P5, 0, 0), e12 = E_(P5, 0, 1), e13 = E_(P5, 0, 2), e22 = E_(P5, 1, 1), e23 = E_(P5, 1, 2), e33 = E_(P5, 2, 2);
+      const double e11 = E_(P[5], 0, 0), e12 = E_(P[5], 0, 1), e13 = E_(P[5], 0, 2), e22 = E_(P[5], 1, 1), e23 = E_(P[5], 1, 2), e33 = E_(P[5], 2, 2);
       const double d23 = s[s112] - e23, d22 = s[s022] - e22, d33 = s[s202] - e33;
       if (e11 > diagmin) { S202c = d22 + e13 * e13 / e11; S022c = d33 + e12 * e12 / e11; }
       s[s112] = realizability_S211(e11, e22, e33, e12, e13, d23, s[s112], beta);
@@ -223,21 +222,13 @@ HQN int realizable_3D(double* s) {
   // 4x4 minors: cubic roots bound the S220-type moments
   double lo[6], hi[6];
   const double cur[6] = {s[s220], s[s220], s[s202], s[s202], s[s022], s[s022]};
-#pragma unroll
   for (int q = 0; q < 6; ++q) {
     // order of the reference: E1, E3 (S220), E2, E4 (S202), E5, E6 (S022)
     const int p = (q == 0) ? 0 : (q == 1) ? 2 : (q == 2) ? 1 : (q == 3) ? 3 : (q == 4) ? 4 : 5;
     Delta E;
-    switch (p) {
-      case 0: delta2star<0>(s, E); break;
-      case 1: delta2star<1>(s, E); break;
-      case 2: delta2star<2>(s, E); break;
-      case 3: delta2star<3>(s, E); break;
-      case 4: delta2star<4>(s, E); break;
-      default: delta2star<5>(s, E); break;
-    }
+    delta2star_p(s, p, E);
     lo[q] = cur[q]; hi[q] = cur[q];
-    if (lead_det<4>(E) < 0.0) {
+    if (lead_det(E, 4) < 0.0) {
       flag220 = 1;
       const double ex = -E_(E, 1, 1) + E_(E, 0, 3);
       const double d22 = cur[q] - E_(E, 1, 1);
@@ -430,7 +421,7 @@ HQN void flux_closure35(const double* M4, int flag2D, double Ma, double* Fx, dou
   }
   double f[21];
   hyqmom_3D(s, f);
-  // S -> C (S_to_C_batch) and C -> raw (C5toM5_3D) for orders <= 5
+  // S -> C (S_to_C_batch) on the 56-entry store, then C -> raw (C5toM5_3D)
   const double sx = sqrt(jmax(EPS, C200)), sy = sqrt(jmax(EPS, C020)), sz = sqrt(jmax(EPS, C002));
   double px[6], py[6], pz[6];
   px[0] = py[0] = pz[0] = 1.0;
@@ -439,45 +430,31 @@ HQN void flux_closure35(const double* M4, int flag2D, double Ma, double* Fx, dou
   px[3] = sx * sx * sx; py[3] = sy * sy * sy; pz[3] = sz * sz * sz;
   px[4] = pow4(sx); py[4] = pow4(sy); pz[4] = pow4(sz);
   px[5] = pow5(sx); py[5] = pow5(sy); pz[5] = pow5(sz);
-  // central moments of order 2..5 on demand
-  auto cen = [&](int i, int j, int k) -> double {
+  double A[56];
+  for (int q = 0; q < 56; ++q) {
+    const int i = T_EX56I[q], j = T_EX56J[q], k = T_EX56K[q];
     const int o = i + j + k;
-    if (o == 0) return 1.0;
-    if (o == 1) return 0.0;
-    if (i == 2 && o == 2) return C200;
-    if (j == 2 && o == 2) return C020;
-    if (k == 2 && o == 2) return C002;
-    double sv = (o == 5) ? f[f5_of(i, j, k)] : s[s28_of(i, j, k)];
-    double d = sv;
-    if (i) d = d * px[i];
-    if (j) d = d * py[j];
-    if (k) d = d * pz[k];
-    return d;
-  };
-  double pu[6], pv[6], pw[6];
-  pu[0] = pv[0] = pw[0] = 1.0;
-#pragma unroll
-  for (int q = 1; q < 6; ++q) { pu[q] = pu[q - 1] * u; pv[q] = pv[q - 1] * v; pw[q] = pw[q - 1] * w; }
-  auto raw = [&](int i, int j, int k) -> double {
-    double acc = 0.0;
-#pragma unroll
-    for (int a = 0; a <= 5; ++a)
-#pragma unroll
-      for (int b = 0; b <= 5; ++b)
-#pragma unroll
-        for (int c = 0; c <= 5; ++c) {
-          if (a > i || b > j || c > k || a + b + c == 1) continue;
-          acc = acc + double(binom(i, a) * binom(j, b) * binom(k, c)) * cen(a, b, c) * (pu[i - a] * pv[j - b] * pw[k - c]);
-        }
-    return M000 * acc;
-  };
-#pragma unroll
+    double val;
+    if (o == 0) val = 1.0;
+    else if (o == 1) val = 0.0;
+    else if (o == 2 && i == 2) val = C200;
+    else if (o == 2 && j == 2) val = C020;
+    else if (o == 2 && k == 2) val = C002;
+    else {
+      double d = (q >= 35) ? f[q - 35] : s[T_S28OF56[q]];
+      if (i) d = d * px[i];
+      if (j) d = d * py[j];
+      if (k) d = d * pz[k];
+      val = d;
+    }
+    A[q] = val;
+  }
+  central_to_raw(M000, u, v, w, A, 56);
   for (int n = 0; n < 35; ++n) {
-    const int i = ex_i(n), j = ex_j(n), k = ex_k(n);
-    Mr[n] = raw(i, j, k);
-    if (Fx) Fx[n] = raw(i + 1, j, k);
-    if (Fy) Fy[n] = raw(i, j + 1, k);
-    if (Fz) Fz[n] = raw(i, j, k + 1);
+    Mr[n] = A[n];
+    if (Fx) Fx[n] = A[T_FX[n]];
+    if (Fy) Fy[n] = A[T_FY[n]];
+    if (Fz) Fz[n] = A[T_FZ[n]];
   }
 }
 

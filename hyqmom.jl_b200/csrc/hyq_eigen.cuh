@@ -38,35 +38,46 @@ HQD Dual dsqrt(const Dual& a) { Dual r; r.v = sqrt(a.v);
 #pragma unroll
   for (int i = 0; i < 6; ++i) r.d[i] = a.d[i] / (2.0 * r.v); return r; }
 
+// 2-D moment tables in jacobian6 argument order: exponents and shift-pass orders
+__device__ constexpr int A2[15] = {0, 0, 0, 0, 0, 1, 1, 1, 1, 2, 2, 2, 3, 3, 4};
+__device__ constexpr int B2[15] = {0, 1, 2, 3, 4, 0, 1, 2, 3, 0, 1, 2, 0, 1, 0};
+__device__ constexpr int PASS2X[15] = {14, 12, 13, 9, 10, 11, 5, 6, 7, 8, 0, 1, 2, 3, 4};
+__device__ constexpr int PASS2Y[15] = {4, 3, 8, 2, 7, 11, 1, 6, 10, 13, 0, 5, 9, 12, 14};
+__device__ constexpr int AB2[5][5] = {{0, 1, 2, 3, 4}, {5, 6, 7, 8, -1}, {9, 10, 11, -1, -1}, {12, 13, -1, -1, -1}, {14, -1, -1, -1, -1}};
+
 // m[15] in jacobian6 argument order (m00,m01,m02,m03,m04,m10,m11,m12,m13,
 // m20,m21,m22,m30,m31,m40); m_ab = E[x^a y^b], x = flux direction.
 // Output: rows 3, 5, 6 of the Jacobian (rows 1, 2, 4 are unit rows e2, e3, e5).
 HQN void jacobian6_rows(const double* m, double* r3, double* r5, double* r6) {
   // index of m_ab in the argument list
-  const int AB[5][5] = {{0, 1, 2, 3, 4}, {5, 6, 7, 8, -1}, {9, 10, 11, -1, -1}, {12, 13, -1, -1, -1}, {14, -1, -1, -1, -1}};
+  const int (&AB)[5][5] = AB2;
   const int SEED[15] = {-1, -1, 0, 3, 5, -1, -1, 1, 4, -1, -1, 2, -1, -1, -1};
   Dual R[15];
-#pragma unroll
   for (int n = 0; n < 15; ++n) { R[n] = dconst(m[n]); if (SEED[n] >= 0) R[n].d[SEED[n]] = 1.0; }
   const Dual m00 = R[0];
   const Dual u = R[5] / m00, vv = R[1] / m00;
-  Dual pu[5], pv[5];
-  pu[0] = dconst(1.0); pv[0] = dconst(1.0);
-#pragma unroll
-  for (int i = 1; i < 5; ++i) { pu[i] = pu[i - 1] * (-u); pv[i] = pv[i - 1] * (-vv); }
+  // central 2-D moments: x pass then y pass of the binomial shift
   Dual Cc[15];
-#pragma unroll
-  for (int a = 0; a < 5; ++a)
-#pragma unroll
-    for (int b = 0; a + b < 5; ++b) {
-      Dual s = dconst(0.0);
-#pragma unroll
-      for (int p = 0; p <= a; ++p)
-#pragma unroll
-        for (int q = 0; q <= b; ++q)
-          s = s + dconst(double(binom(a, p) * binom(b, q))) * (R[AB[p][q]] / m00) * (pu[a - p] * pv[b - q]);
-      Cc[AB[a][b]] = s;
-    }
+  for (int n = 0; n < 15; ++n) Cc[n] = R[n] / m00;
+  const Dual nu = -u, nv = -vv;
+  for (int t = 0; t < 15; ++t) {
+    const int n = PASS2X[t], a = A2[n], b = B2[n];
+    if (a == 0) continue;
+    Dual pw = dconst(1.0), acc = dconst(0.0);
+    Dual terms[5];
+    for (int q = 0; q <= a; ++q) { terms[q] = pw; pw = pw * nu; }  // terms[q] = (-u)^q
+    for (int p = 0; p <= a; ++p) acc = acc + (dconst(double(binom(a, p))) * terms[a - p]) * Cc[AB[p][b]];
+    Cc[n] = acc;
+  }
+  for (int t = 0; t < 15; ++t) {
+    const int n = PASS2Y[t], a = A2[n], b = B2[n];
+    if (b == 0) continue;
+    Dual pw = dconst(1.0), acc = dconst(0.0);
+    Dual terms[5];
+    for (int q = 0; q <= b; ++q) { terms[q] = pw; pw = pw * nv; }
+    for (int p = 0; p <= b; ++p) acc = acc + (dconst(double(binom(b, p))) * terms[b - p]) * Cc[AB[a][p]];
+    Cc[n] = acc;
+  }
   const Dual sx = dsqrt(Cc[AB[2][0]]), sy = dsqrt(Cc[AB[0][2]]);
   auto S = [&](int a, int b) {
     Dual d = dconst(1.0);
@@ -90,7 +101,6 @@ HQN void jacobian6_rows(const double* m, double* r3, double* r5, double* r6) {
   const Dual C32 = scl(S32, 3, 2), C23 = scl(S23, 2, 3), C14 = scl(S14, 1, 4);
   Dual qu[6], qv[6];
   qu[0] = dconst(1.0); qv[0] = dconst(1.0);
-#pragma unroll
   for (int i = 1; i < 6; ++i) { qu[i] = qu[i - 1] * u; qv[i] = qv[i - 1] * vv; }
   auto Ct = [&](int a, int b) -> Dual {
     if (a + b == 0) return dconst(1.0);
@@ -102,11 +112,9 @@ HQN void jacobian6_rows(const double* m, double* r3, double* r5, double* r6) {
   };
   auto raw = [&](int a, int b) {
     Dual s = dconst(0.0);
-#pragma unroll
-    for (int p = 0; p <= 5; ++p)
-#pragma unroll
-      for (int q = 0; q <= 5; ++q) {
-        if (p > a || q > b || p + q == 1) continue;
+    for (int p = 0; p <= a; ++p)
+      for (int q = 0; q <= b; ++q) {
+        if (p + q == 1) continue;
         s = s + dconst(double(binom(a, p) * binom(b, q))) * Ct(p, q) * (qu[a - p] * qv[b - q]);
       }
     return m00 * s;
@@ -511,10 +519,9 @@ HQN void correct_for_real(const double* M, int pa_i, int pa_j, int pb_i, int pb_
   };
   if (planes & 1) corr(pa_i, pa_j);
   if (planes & 2) corr(pb_i, pb_j);
-  double Mh[35];
   C[0] = 1.0;
-  central_to_raw4(M000, u, v, w, C, Mh);
-  flux_closure35(Mh, flag2D, Ma, nullptr, nullptr, nullptr, Mout);
+  central_to_raw(M000, u, v, w, C, 35);
+  flux_closure35(C, flag2D, Ma, nullptr, nullptr, nullptr, Mout);
 }
 
 // eigenvalues6_hyperbolic_3D for axis 1 (x) or 2 (y).
@@ -643,11 +650,9 @@ HQD void collision35(double* M, double dt, double Kn, int positivity) {
     C[n] = zi * zj * zk * pw[i] * pw[j] * pw[k];
   }
   C[0] = 1.0;
-  double MG[35];
-  central_to_raw4(rho, u, v, w, C, MG);
-  const double e = exp(-dt / tc);
-#pragma unroll
-  for (int n = 0; n < 35; ++n) M[n] = MG[n] - e * (MG[n] - M[n]);
+  central_to_raw(rho, u, v, w, C, 35);
+  const double e = hexp(-dt / tc);
+  for (int n = 0; n < 35; ++n) M[n] = C[n] - e * (C[n] - M[n]);
 }
 
 }  // namespace hyq

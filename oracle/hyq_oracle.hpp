@@ -68,6 +68,55 @@ template <class T> inline T cube(T x) { return x * x * x; }
 template <class T> inline T pow4(T x) { T y = x * x; return y * y; }
 template <class T> inline T pow5(T x) { T y = x * x; return y * y * x; }
 
+// exp(x) written here (Cody-Waite reduction x = k ln2 + r, |r| <= ln2/2, the
+// Taylor series of exp(r) to degree 14 by Horner, scaling by 2^k), so that
+// the device code and the CPU oracle round identically; accuracy ~1 ulp.
+inline double hexp(double x) {
+  if (x != x) return x;
+  if (x > 709.782712893384) return std::numeric_limits<double>::infinity();
+  if (x < -745.1332191019412) return 0.0;
+  const double k = std::rint(x * 1.4426950408889634);
+  const double r = (x - k * 0.6931471803691238) - k * 1.9082149292705877e-10;
+  double p = 1.1470745597729725e-11;
+  p = p * r + 1.6059043836821613e-10;
+  p = p * r + 2.08767569878681e-09;
+  p = p * r + 2.505210838544172e-08;
+  p = p * r + 2.755731922398589e-07;
+  p = p * r + 2.7557319223985893e-06;
+  p = p * r + 2.48015873015873e-05;
+  p = p * r + 0.0001984126984126984;
+  p = p * r + 0.001388888888888889;
+  p = p * r + 0.008333333333333333;
+  p = p * r + 0.041666666666666664;
+  p = p * r + 0.16666666666666666;
+  p = p * r + 0.5;
+  p = p * r + 1.0;
+  p = p * r + 1.0;
+  return std::ldexp(p, (int)k);
+}
+
+// Real cube root written here (exponent split into a multiple of 3, Newton
+// iterations on the mantissa), identical on device and in the oracle.
+inline double hcbrt(double x) {
+  if (x == 0.0 || x != x || std::isinf(x)) return x;
+  int e;
+  double m = std::frexp(std::fabs(x), &e);
+  int rr = e % 3;
+  if (rr < 0) rr += 3;
+  m = std::ldexp(m, rr);
+  e -= rr;
+  double y = 0.7 + 0.25 * m;
+  for (int it = 0; it < 7; ++it) y = y - (y * y * y - m) / (3.0 * y * y);
+  y = std::ldexp(y, e / 3);
+  return x < 0.0 ? -y : y;
+}
+
+// the real type may be an op counter: exp/cbrt of T go through these
+template <class T> inline T hexpT(T x) { using std::exp; return exp(x); }
+template <> inline double hexpT<double>(double x) { return hexp(x); }
+template <class T> inline T hcbrtT(T x) { using std::cbrt; return cbrt(x); }
+template <> inline double hcbrtT<double>(double x) { return hcbrt(x); }
+
 template <class T> inline T ipow(T x, int n) {
   T r = T(1);
   for (int i = 0; i < n; ++i) r = r * x;
@@ -79,6 +128,70 @@ inline int binom(int n, int k) {
                               {1, 2, 1, 0, 0, 0}, {1, 3, 3, 1, 0, 0},
                               {1, 4, 6, 4, 1, 0}, {1, 5, 10, 10, 5, 1}};
   return B[n][k];
+}
+
+// 56-entry moment storage (order <= 5): the 35 moments of order <= 4 in the
+// reference order, then the 21 fifth-order moments in the closure order.
+static const unsigned char T_EX56I[56] = {0,1,2,3,4,0,1,2,3,0,1,2,0,1,0,0,1,2,3,0,1,2,0,1,0,0,1,2,0,1,0,0,1,0,0,5,4,3,2,1,4,3,2,1,3,2,1,2,1,1,0,0,0,0,0,0};
+static const unsigned char T_EX56J[56] = {0,0,0,0,0,1,1,1,1,2,2,2,3,3,4,0,0,0,0,0,0,0,0,0,0,1,1,1,2,2,3,1,1,1,2,0,1,2,3,4,0,0,0,0,1,2,3,1,1,2,5,4,3,2,1,0};
+static const unsigned char T_EX56K[56] = {0,0,0,0,0,0,0,0,0,0,0,0,0,0,0,1,1,1,1,2,2,2,3,3,4,1,1,1,1,1,1,2,2,3,2,0,0,0,0,0,1,2,3,4,1,1,1,2,3,2,0,1,2,3,4,5};
+static const signed char T_IDX56[216] = {0,15,19,22,24,55,5,25,31,33,54,-1,9,28,34,53,-1,-1,12,30,52,-1,-1,-1,14,51,-1,-1,-1,-1,50,-1,-1,-1,-1,-1,1,16,20,23,43,-1,6,26,32,48,-1,-1,10,29,49,-1,-1,-1,13,46,-1,-1,-1,-1,39,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,2,17,21,42,-1,-1,7,27,47,-1,-1,-1,11,45,-1,-1,-1,-1,38,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,3,18,41,-1,-1,-1,8,44,-1,-1,-1,-1,37,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,4,40,-1,-1,-1,-1,36,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,35,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1};
+// pass orders of the separable shift transforms (exponent of the axis descending)
+static const unsigned char T_L35X[35] = {4,3,8,18,2,7,11,17,21,27,1,6,10,13,16,20,23,26,29,32,0,5,9,12,14,15,19,22,24,25,28,30,31,33,34};
+static const unsigned char T_L35Y[35] = {14,12,13,30,9,10,11,28,29,34,5,6,7,8,25,26,27,31,32,33,0,1,2,3,4,15,16,17,18,19,20,21,22,23,24};
+static const unsigned char T_L35Z[35] = {24,22,23,33,19,20,21,31,32,34,15,16,17,18,25,26,27,28,29,30,0,1,2,3,4,5,6,7,8,9,10,11,12,13,14};
+static const unsigned char T_L56X[56] = {35,4,36,40,3,8,18,37,41,44,2,7,11,17,21,27,38,42,45,47,1,6,10,13,16,20,23,26,29,32,39,43,46,48,49,0,5,9,12,14,15,19,22,24,25,28,30,31,33,34,50,51,52,53,54,55};
+static const unsigned char T_L56Y[56] = {50,14,39,51,12,13,30,38,46,52,9,10,11,28,29,34,37,45,49,53,5,6,7,8,25,26,27,31,32,33,36,44,47,48,54,0,1,2,3,4,15,16,17,18,19,20,21,22,23,24,35,40,41,42,43,55};
+static const unsigned char T_L56Z[56] = {55,24,43,54,22,23,33,42,48,53,19,20,21,31,32,34,41,47,49,52,15,16,17,18,25,26,27,28,29,30,40,44,45,46,51,0,1,2,3,4,5,6,7,8,9,10,11,12,13,14,35,36,37,38,39,50};
+// 28-set index of each stored moment (-1: order 0, 1, diagonal 2, or 5)
+static const signed char T_S28OF56[56] = {-1,-1,-1,0,1,-1,2,3,4,-1,5,6,7,8,9,-1,10,11,12,-1,13,14,15,16,17,18,19,20,21,22,23,24,25,26,27,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1,-1};
+// storage index of the x/y/z flux moment of each of the 35 moments
+static const unsigned char T_FX[35] = {1,2,3,4,35,6,7,8,36,10,11,37,13,38,39,16,17,18,40,20,21,41,23,42,43,26,27,44,29,45,46,32,47,48,49};
+static const unsigned char T_FY[35] = {5,6,7,8,36,9,10,11,37,12,13,38,14,39,50,25,26,27,44,31,32,47,33,48,54,28,29,45,30,46,51,34,49,53,52};
+static const unsigned char T_FZ[35] = {15,16,17,18,40,25,26,27,44,28,29,45,30,46,51,19,20,21,41,22,23,42,24,43,55,31,32,47,34,49,52,33,48,54,53};
+static const int BIN7[49] = {1,0,0,0,0,0,0, 1,1,0,0,0,0,0, 1,2,1,0,0,0,0, 1,3,3,1,0,0,0, 1,4,6,4,1,0,0, 1,5,10,10,5,1,0, 1,6,15,20,15,6,1};
+
+// Separable binomial shift along one axis on the 56-entry moment store
+// (first n entries; n = 35: order <= 4, 56: order <= 5):
+// A_ijk <- sum_{a<=i} C(i,a) sh^(i-a) A_ajk (x shown); raw <-> central
+// conversions are three passes, one per axis.
+template <class T> void shift_axis(T* A, int n, int axis, T sh) {
+  T pw[6];
+  pw[0] = T(1);
+  for (int q = 1; q < 6; ++q) pw[q] = pw[q - 1] * sh;
+  const unsigned char* L = (n == 35) ? (axis == 0 ? T_L35X : axis == 1 ? T_L35Y : T_L35Z) : (axis == 0 ? T_L56X : axis == 1 ? T_L56Y : T_L56Z);
+  const int stride = axis == 0 ? 36 : axis == 1 ? 6 : 1;
+  for (int t = 0; t < n; ++t) {
+    const int q = L[t];
+    const int e = axis == 0 ? T_EX56I[q] : axis == 1 ? T_EX56J[q] : T_EX56K[q];
+    if (e == 0) continue;
+    const int base = T_EX56I[q] * 36 + T_EX56J[q] * 6 + T_EX56K[q] - e * stride;
+    T acc = T(0);
+    for (int a = 0; a <= e; ++a) acc = acc + (T(double(BIN7[e * 7 + a])) * pw[e - a]) * A[T_IDX56[base + a * stride]];
+    A[q] = acc;
+  }
+}
+
+// Central moments (35-order, C000=1, first order 0) of raw M
+// (M4toC4_3D, src/autogen/M4toC4_3D.jl:42-55).
+template <class T> void raw_to_central35(const T* M, T* C) {
+  T inv = T(1) / M[0];
+  T u = M[1] * inv, v = M[5] * inv, w = M[15] * inv;
+  for (int n = 0; n < 35; ++n) C[n] = M[n] * inv;
+  shift_axis(C, 35, 0, T(-u));
+  shift_axis(C, 35, 1, T(-v));
+  shift_axis(C, 35, 2, T(-w));
+  C[0] = T(1); C[1] = T(0); C[5] = T(0); C[15] = T(0);
+}
+
+// Raw moments from density, mean and central moments, in place on the
+// store A (n = 35 or 56; A[0] = 1, first order 0)
+// (C4toM4_3D / C5toM5_3D, src/autogen/C4toM4_3D.jl:64-118, C5toM5_3D.jl:16-28).
+template <class T> void central_to_raw(T M000, T u, T v, T w, T* A, int n) {
+  shift_axis(A, n, 0, u);
+  shift_axis(A, n, 1, v);
+  shift_axis(A, n, 2, w);
+  for (int q = 0; q < n; ++q) A[q] = M000 * A[q];
 }
 
 // ------------------------------------------------------------ small dense LA
@@ -147,56 +260,24 @@ template <class T, int N> void solve_lu(const T (&Ain)[N][N], const T (&b)[N], T
 
 // ------------------------------------------------ raw <-> central moments
 // M4toC4_3D (src/autogen/M4toC4_3D.jl:42-55): central moments of order <= 4
-// from raw moments, by the binomial expansion about the mean.
+// as a 6x6x6 cube.
 template <class T> void m4_to_c4(const T* M, T* C /*216 cube*/) {
-  T Mc[216];
-  for (int i = 0; i < 216; ++i) { Mc[i] = T(0); C[i] = T(0); }
-  for (int n = 0; n < 35; ++n) Mc[t3(E35[n][0], E35[n][1], E35[n][2])] = M[n];
-  T inv = T(1) / M[0];
-  T u = M[1] * inv, v = M[5] * inv, w = M[15] * inv;
-  T pu[5], pv[5], pw[5];
-  pu[0] = pv[0] = pw[0] = T(1);
-  for (int i = 1; i < 5; ++i) { pu[i] = pu[i - 1] * (-u); pv[i] = pv[i - 1] * (-v); pw[i] = pw[i - 1] * (-w); }
-  for (int n = 0; n < 35; ++n) {
-    int i = E35[n][0], j = E35[n][1], k = E35[n][2];
-    T s = T(0);
-    for (int a = 0; a <= i; ++a)
-      for (int b = 0; b <= j; ++b)
-        for (int c = 0; c <= k; ++c) {
-          T term = T(double(binom(i, a) * binom(j, b) * binom(k, c))) * (Mc[t3(a, b, c)] * inv) *
-                   (pu[i - a] * pv[j - b] * pw[k - c]);
-          s = s + term;
-        }
-    C[t3(i, j, k)] = s;
-  }
-  C[t3(0, 0, 0)] = T(1);
-  C[t3(1, 0, 0)] = T(0);
-  C[t3(0, 1, 0)] = T(0);
-  C[t3(0, 0, 1)] = T(0);
+  T C35[35];
+  raw_to_central35(M, C35);
+  for (int i = 0; i < 216; ++i) C[i] = T(0);
+  for (int n = 0; n < 35; ++n) C[t3(E35[n][0], E35[n][1], E35[n][2])] = C35[n];
 }
 
-// C4toM4_3D / C5toM5_3D (src/autogen/C4toM4_3D.jl:64-118,
-// src/autogen/C5toM5_3D.jl:16-28): raw moments from density, mean velocity
-// and central moments (C000=1, first order zero), for all i+j+k <= order.
+// C4toM4_3D / C5toM5_3D on 6x6x6 cubes (C000=1, first order zero), for all
+// i+j+k <= order (4 or 5), through the 56-entry store.
 template <class T> void c_to_m(T M000, T u, T v, T w, const T* C /*216*/, T* Mout /*216*/, int order) {
-  T pu[6], pv[6], pw[6];
-  pu[0] = pv[0] = pw[0] = T(1);
-  for (int i = 1; i < 6; ++i) { pu[i] = pu[i - 1] * u; pv[i] = pv[i - 1] * v; pw[i] = pw[i - 1] * w; }
+  const int n = order == 4 ? 35 : 56;
+  T A[56];
+  for (int q = 0; q < n; ++q) A[q] = C[t3(T_EX56I[q], T_EX56J[q], T_EX56K[q])];
+  A[0] = T(1); A[1] = T(0); A[5] = T(0); A[15] = T(0);
+  central_to_raw(M000, u, v, w, A, n);
   for (int i = 0; i < 216; ++i) Mout[i] = T(0);
-  for (int i = 0; i <= order; ++i)
-    for (int j = 0; i + j <= order; ++j)
-      for (int k = 0; i + j + k <= order; ++k) {
-        T s = T(0);
-        for (int a = 0; a <= i; ++a)
-          for (int b = 0; b <= j; ++b)
-            for (int c = 0; c <= k; ++c) {
-              int ord = a + b + c;
-              if (ord == 1) continue;
-              T cm = ord == 0 ? T(1) : C[t3(a, b, c)];
-              s = s + T(double(binom(i, a) * binom(j, b) * binom(k, c))) * cm * (pu[i - a] * pv[j - b] * pw[k - c]);
-            }
-        Mout[t3(i, j, k)] = M000 * s;
-      }
+  for (int q = 0; q < n; ++q) Mout[t3(T_EX56I[q], T_EX56J[q], T_EX56K[q])] = A[q];
 }
 
 // Symmetric 3x3 principal square root (Julia sqrt(::Matrix) on symmetric
@@ -545,26 +626,29 @@ template <class T> inline T sget(const S28<T>& s, int i, int j, int k) {
 static const int B1[4][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
 static const int B2[6][3] = {{2, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 2, 0}, {0, 1, 1}, {0, 0, 2}};
 
-// Q = M21 M11^{-1} M12 (6x6), the projection part of the Schur complement.
+// Q = M21 M11^{-1} M12 (6x6 symmetric), the projection part of the Schur
+// complement.  M11 = 1 (+) R with R the correlation matrix; R^{-1} by
+// cofactors; Q(a,b) = mu_a mu_b + w_a . R^{-1} w_b for a <= b, mirrored.
 template <class T> void delta_projection(const S28<T>& s, T (&Q)[6][6]) {
-  T M11[4][4], M12[4][6];
-  for (int a = 0; a < 4; ++a) {
-    for (int b = 0; b < 4; ++b)
-      M11[a][b] = sget(s, B1[a][0] + B1[b][0], B1[a][1] + B1[b][1], B1[a][2] + B1[b][2]);
-    for (int b = 0; b < 6; ++b)
-      M12[a][b] = sget(s, B1[a][0] + B2[b][0], B1[a][1] + B2[b][1], B1[a][2] + B2[b][2]);
-  }
-  T X[4][6];
-  for (int b = 0; b < 6; ++b) {
-    T rhs[4] = {M12[0][b], M12[1][b], M12[2][b], M12[3][b]}, x[4];
-    solve_lu<T, 4>(M11, rhs, x);
-    for (int a = 0; a < 4; ++a) X[a][b] = x[a];
+  const T c00 = T(1) - s.s011 * s.s011, c01 = s.s101 * s.s011 - s.s110, c02 = s.s110 * s.s011 - s.s101;
+  const T c11 = T(1) - s.s101 * s.s101, c12 = s.s110 * s.s101 - s.s011, c22 = T(1) - s.s110 * s.s110;
+  const T det = c00 + s.s110 * c01 + s.s101 * c02;
+  const T id = T(1) / det;
+  const T r00 = c00 * id, r01 = c01 * id, r02 = c02 * id, r11 = c11 * id, r12 = c12 * id, r22 = c22 * id;
+  const T mu[6] = {T(1), s.s110, s.s101, T(1), s.s011, T(1)};
+  const T w[6][3] = {{s.s300, s.s210, s.s201}, {s.s210, s.s120, s.s111}, {s.s201, s.s111, s.s102},
+                     {s.s120, s.s030, s.s021}, {s.s111, s.s021, s.s012}, {s.s102, s.s012, s.s003}};
+  T z[6][3];
+  for (int a = 0; a < 6; ++a) {
+    z[a][0] = r00 * w[a][0] + r01 * w[a][1] + r02 * w[a][2];
+    z[a][1] = r01 * w[a][0] + r11 * w[a][1] + r12 * w[a][2];
+    z[a][2] = r02 * w[a][0] + r12 * w[a][1] + r22 * w[a][2];
   }
   for (int a = 0; a < 6; ++a)
-    for (int b = 0; b < 6; ++b) {
-      T q = T(0);
-      for (int r = 0; r < 4; ++r) q = q + M12[r][a] * X[r][b];
-      Q[a][b] = q;
+    for (int b = a; b < 6; ++b) {
+      const T qv = mu[a] * mu[b] + (w[a][0] * z[b][0] + w[a][1] * z[b][1] + w[a][2] * z[b][2]);
+      Q[a][b] = qv;
+      Q[b][a] = qv;
     }
 }
 
@@ -573,8 +657,11 @@ template <class T> void delta2star3D(const S28<T>& s, T (&E)[6][6]) {
   T Q[6][6];
   delta_projection(s, Q);
   for (int a = 0; a < 6; ++a)
-    for (int b = 0; b < 6; ++b)
-      E[a][b] = sget(s, B2[a][0] + B2[b][0], B2[a][1] + B2[b][1], B2[a][2] + B2[b][2]) - Q[a][b];
+    for (int b = a; b < 6; ++b) {
+      const T e = sget(s, B2[a][0] + B2[b][0], B2[a][1] + B2[b][1], B2[a][2] + B2[b][2]) - Q[a][b];
+      E[a][b] = e;
+      E[b][a] = e;
+    }
 }
 
 // lower_bound_S220 (src/autogen/lower_bound_S220.jl:14-37): {Q(xy,xy), Q(xz,xz), Q(yz,yz)}.
@@ -594,36 +681,18 @@ template <class T> void bound_minor1(const S28<T>& s, T (&out)[12]) {
 }
 
 // ------------------------------------------------------------ 2-D pieces
-// 2-D Delta2* (basis {1,x,y} | {x2,xy,y2}) as a 3x3 matrix.
+// 2-D Delta2* (basis {1,x,y} | {x2,xy,y2}) as a 3x3 matrix; M11 =
+// [1 0 0; 0 1 s11; 0 s11 1] inverted in closed form.
 template <class T> void delta2star2D(T s30, T s40, T s11, T s21, T s31, T s12, T s22, T s03, T s13, T s04, T (&D)[3][3]) {
-  // standardized 2-D moments m(i,j)
-  auto m = [&](int i, int j) -> T {
-    int key = 10 * i + j;
-    switch (key) {
-      case 0: return T(1); case 10: case 1: return T(0); case 20: case 2: return T(1);
-      case 11: return s11; case 30: return s30; case 21: return s21; case 12: return s12; case 3: return s03;
-      case 40: return s40; case 31: return s31; case 22: return s22; case 13: return s13; case 4: return s04;
-    }
-    return T(0);
-  };
-  static const int b1[3][2] = {{0, 0}, {1, 0}, {0, 1}};
-  static const int b2[3][2] = {{2, 0}, {1, 1}, {0, 2}};
-  T A[3][3], Bm[3][3];
-  for (int a = 0; a < 3; ++a) {
-    for (int b = 0; b < 3; ++b) A[a][b] = m(b1[a][0] + b1[b][0], b1[a][1] + b1[b][1]);
-    for (int b = 0; b < 3; ++b) Bm[a][b] = m(b1[a][0] + b2[b][0], b1[a][1] + b2[b][1]);
-  }
-  T X[3][3];
-  for (int b = 0; b < 3; ++b) {
-    T rhs[3] = {Bm[0][b], Bm[1][b], Bm[2][b]}, x[3];
-    solve_lu<T, 3>(A, rhs, x);
-    for (int a = 0; a < 3; ++a) X[a][b] = x[a];
-  }
+  const T dt = T(1) - s11 * s11;
+  const T i00 = T(1) / dt, i01 = -s11 / dt;
+  const T mu[3] = {T(1), s11, T(1)};
+  const T w[3][2] = {{s30, s21}, {s21, s12}, {s12, s03}};
+  const T m22[3][3] = {{s40, s31, s22}, {s31, s22, s13}, {s22, s13, s04}};
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b) {
-      T q = T(0);
-      for (int r = 0; r < 3; ++r) q = q + Bm[r][a] * X[r][b];
-      D[a][b] = m(b2[a][0] + b2[b][0], b2[a][1] + b2[b][1]) - q;
+      const T z0 = i00 * w[b][0] + i01 * w[b][1], z1 = i01 * w[b][0] + i00 * w[b][1];
+      D[a][b] = m22[a][b] - (mu[a] * mu[b] + (w[a][0] * z0 + w[a][1] * z1));
     }
 }
 
@@ -684,8 +753,8 @@ template <class T> void cardano(const P3<T>& P, T (&re)[3], T (&im)[3]) {
   T q = B * B * B / T(27) - B * C / T(6) + D / T(2);
   T disc = q * q - p * p * p;
   T sd = fm_sqrt(disc);
-  using std::cbrt; using std::sqrt;
-  T Cc = cbrt(q + sd);
+  using std::sqrt;
+  T Cc = hcbrtT(T(q + sd));
   T pc = p / Cc;
   T sh = B / T(3);
   T s3 = sqrt(T(3));
@@ -696,19 +765,19 @@ template <class T> void cardano(const P3<T>& P, T (&re)[3], T (&im)[3]) {
 }
 
 // rootsR (src/autogen/rootsR.jl:7-292): roots in S22 of det(2-D Delta2*(S22)).
+// The Schur complement is affine in S22 with slope 1 at (x2,y2), (y2,x2),
+// (xy,xy): det [a b c+X; b d+X e; c+X e f] expanded as a cubic in X.
 template <class T> void rootsR(T Del1, T H02, T H20, T s03, T s11, T s12, T s13, T s21, T s30, T s31, T (&re)[3], T (&im)[3]) {
   (void)Del1;
   T s40 = H20 + s30 * s30 + T(1), s04 = H02 + s03 * s03 + T(1);
-  // entries of the 2-D Schur complement are affine in S22: evaluate at 0 and 1
-  T D0[3][3], D1m[3][3];
+  T D0[3][3];
   delta2star2D(s30, s40, s11, s21, s31, s12, T(0), s03, s13, s04, D0);
-  delta2star2D(s30, s40, s11, s21, s31, s12, T(1), s03, s13, s04, D1m);
-  P3<T> A[3][3];
-  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) A[i][j] = pconst(D0[i][j], D1m[i][j] - D0[i][j]);
-  // exact affine structure: only (xy,xy) and (x2,y2) depend on S22 with slope 1
-  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) A[i][j].c[1] = T(0);
-  A[1][1].c[1] = T(1); A[0][2].c[1] = T(1); A[2][0].c[1] = T(1);
-  P3<T> P = pdet3(A);
+  const T a = D0[0][0], b = D0[0][1], c = D0[0][2], d = D0[1][1], e = D0[1][2], f = D0[2][2];
+  const T k0 = a * (d * f - e * e) - b * (b * f - e * c) + c * (b * e - d * c);
+  const T k1 = a * f + b * e + (b * e - d * c) - c * (d + c);
+  const T k2 = -(d + c) - c;
+  P3<T> P;
+  P.c[0] = k0; P.c[1] = k1; P.c[2] = k2; P.c[3] = T(-1);
   cardano(P, re, im);
 }
 

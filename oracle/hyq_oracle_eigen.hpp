@@ -46,19 +46,28 @@ template <class T> void jacobian6(const T (&m)[15], T (&J)[6][6]) {
   }
   D6<T> m00 = R[0][0];
   D6<T> u = R[1][0] / m00, v = R[0][1] / m00;
-  // central moments C_ab (a+b <= 4)
+  // central moments C_ab (a+b <= 4): binomial shift along x, then along y
   D6<T> Cc[5][5];
-  D6<T> pu[5], pv[5];
-  pu[0] = pv[0] = dc<T>(1);
-  for (int i = 1; i < 5; ++i) { pu[i] = pu[i - 1] * (-u); pv[i] = pv[i - 1] * (-v); }
-  for (int a = 0; a < 5; ++a)
-    for (int b = 0; a + b < 5; ++b) {
-      D6<T> s = dc<T>(0);
-      for (int p = 0; p <= a; ++p)
-        for (int q = 0; q <= b; ++q)
-          s = s + dc<T>(double(binom(a, p) * binom(b, q))) * (R[p][q] / m00) * (pu[a - p] * pv[b - q]);
-      Cc[a][b] = s;
-    }
+  for (int a = 0; a < 5; ++a) for (int b = 0; a + b < 5; ++b) Cc[a][b] = R[a][b] / m00;
+  D6<T> nu = -u, nv = -v;
+  static const int PX[15][2] = {{4, 0}, {3, 0}, {3, 1}, {2, 0}, {2, 1}, {2, 2}, {1, 0}, {1, 1}, {1, 2}, {1, 3}, {0, 0}, {0, 1}, {0, 2}, {0, 3}, {0, 4}};
+  static const int PY[15][2] = {{0, 4}, {0, 3}, {1, 3}, {0, 2}, {1, 2}, {2, 2}, {0, 1}, {1, 1}, {2, 1}, {3, 1}, {0, 0}, {1, 0}, {2, 0}, {3, 0}, {4, 0}};
+  for (int t = 0; t < 15; ++t) {
+    const int a = PX[t][0], b = PX[t][1];
+    if (a == 0) continue;
+    D6<T> pw = dc<T>(1), acc = dc<T>(0), terms[5];
+    for (int q = 0; q <= a; ++q) { terms[q] = pw; pw = pw * nu; }
+    for (int p = 0; p <= a; ++p) acc = acc + (dc<T>(double(binom(a, p))) * terms[a - p]) * Cc[p][b];
+    Cc[a][b] = acc;
+  }
+  for (int t = 0; t < 15; ++t) {
+    const int a = PY[t][0], b = PY[t][1];
+    if (b == 0) continue;
+    D6<T> pw = dc<T>(1), acc = dc<T>(0), terms[5];
+    for (int q = 0; q <= b; ++q) { terms[q] = pw; pw = pw * nv; }
+    for (int p = 0; p <= b; ++p) acc = acc + (dc<T>(double(binom(b, p))) * terms[b - p]) * Cc[a][p];
+    Cc[a][b] = acc;
+  }
   D6<T> sx = dsqrt(Cc[2][0]), sy = dsqrt(Cc[0][2]);
   auto S = [&](int a, int b) {
     D6<T> d = dc<T>(1);
@@ -669,7 +678,7 @@ template <class T> void collision35(const T* M, T dt, T Kn, bool positivity, T* 
   T tc = Kn / (rho * sqrt(Theta) * T(2));
   T MG[35];
   initialize_m4_35(rho, u, v, w, Theta, T(0), T(0), Theta, T(0), Theta, MG);
-  T e = exp(-dt / tc);
+  T e = hexpT(T(-dt / tc));
   for (int n = 0; n < 35; ++n) Mout[n] = MG[n] - e * (MG[n] - M[n]);
 }
 

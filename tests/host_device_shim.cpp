@@ -1,0 +1,22 @@
+// Host (g++) build of the device per-cell code: the CPU tests compare it bit
+// for bit with the oracle, so arithmetic divergence between the CUDA path and
+// the checker is caught without a GPU.  Test infrastructure only.
+#include <cmath>
+#include <cstring>
+#include <limits>
+using std::sqrt; using std::fabs; using std::isfinite; using std::isinf; using std::signbit; using std::rint; using std::ldexp; using std::frexp; using std::fmax;
+static inline double __longlong_as_double(long long x) { double d; std::memcpy(&d, &x, 8); return d; }
+#define __device__
+#define __forceinline__ inline
+#define __noinline__
+#define __host__
+#include "hyq_eigen.cuh"
+using namespace hyq;
+extern "C" {
+void sh_flux(const double* m, int flag2D, double Ma, double* Fx, double* Fy, double* Fz, double* Mr) { flux_closure35(m, flag2D, Ma, Fx, Fy, Fz, Mr); }
+void sh_eig(const double* m, int axis, int flag2D, double Ma, int pos, double* v, double* Mr) {
+  if (axis == 3) eigenvalues6z(m, flag2D, Ma, pos, v[0], v[1], Mr); else eigenvalues6(m, axis, flag2D, Ma, v[0], v[1], Mr);
+}
+void sh_closure(const double* mom, double* v) { closure_eigs(mom[0], mom[1], mom[2], mom[3], mom[4], v[0], v[1]); }
+void sh_coll(double* m, double dt, double Kn, int pos) { collision35(m, dt, Kn, pos); }
+}

@@ -1,0 +1,64 @@
+"""The device per-cell code, compiled for the host with g++ (strict IEEE, no
+contraction), is bit-identical to the oracle on evolved crossing-jet states.
+
+The CUDA build uses the same source with -fmad=false and IEEE division and
+square root, so this pins GPU-vs-oracle agreement without a GPU; the GPU
+parity tests then check the CUDA build itself."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from hyqmom import ic
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(os.path.dirname(HERE), "hyqmom.jl_b200", "csrc")
+
+
+@pytest.fixture(scope="module")
+def shim(tmp_path_factory):
+    out = tmp_path_factory.mktemp("shim") / "libshim.so"
+    subprocess.check_call(["/usr/bin/g++", "-O2", "-std=c++17", "-fno-fast-math", "-ffp-contract=off", "-fPIC", "-shared",
+                           "-I", CSRC, "-o", str(out), os.path.join(HERE, "host_device_shim.cpp")])
+    return ctypes.CDLL(str(out))
+
+
+@pytest.fixture(scope="module")
+def states():
+    p = ic.with_jets(ic.default_params(Nx=12, Ny=12, Nz=12, Ma=0.0, Kn=1.0, CFL=0.7, dtmax=1e-2, tmax=10.0, nnmax=100), "crossing")
+    M = ic.initial_state(p)
+    pp = dict(p, **ic.grid_spacing(p))
+    t, out = 0.0, []
+    for s in range(24):
+        _, t, _ = ol.step(M, pp, t)
+        if s % 6 == 5:
+            out.append(np.array(M).reshape(-1, 35, order="F"))
+    return np.concatenate(out)
+
+
+def P(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def test_per_cell_functions_bitwise(shim, states):
+    for c in range(states.shape[0]):
+        m = np.ascontiguousarray(states[c])
+        o = [np.zeros(35) for _ in range(4)]
+        shim.sh_flux(P(m), 0, ctypes.c_double(0.0), *[P(x) for x in o])
+        for a, b in zip(o, ol.flux_closure35(m, 0, 0.0)):
+            assert np.array_equal(a, b, equal_nan=True), c
+        for ax in (1, 2, 3):
+            v, Mr = np.zeros(2), np.zeros(35)
+            shim.sh_eig(P(m), ax, 0, ctypes.c_double(0.0), 1, P(v), P(Mr))
+            rv = ol.eigenvalues6z(m, 0, 0.0, True) if ax == 3 else ol.eigenvalues6(m, ax, 0, 0.0)
+            assert np.array_equal(v, np.array(rv[:2]), equal_nan=True) and np.array_equal(Mr, rv[2], equal_nan=True), (c, ax)
+        mom = np.ascontiguousarray(m[[0, 1, 2, 3, 4]])
+        v = np.zeros(2)
+        shim.sh_closure(P(mom), P(v))
+        assert np.array_equal(v, np.array(ol.closure_and_eigenvalues(mom)[1:]), equal_nan=True)
+        mm = m.copy()
+        shim.sh_coll(P(mm), ctypes.c_double(3e-3), ctypes.c_double(1.0), 1)
+        assert np.array_equal(mm, ol.collision35(m, 3e-3, 1.0), equal_nan=True)
