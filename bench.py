@@ -39,9 +39,11 @@ B_ALG = 2 * 35 * 8  # bytes per cell-step: state read once, written once
 def workload(name="c2"):
     from hyqmom import ic
     if name == "c2":
-        # CFL 0.5: at the named CFL 0.7 the reference scheme empties a jet-corner
-        # cell in step 1 and its flux Jacobian is NaN in step 2 (the reference's
-        # eigvals throws there); 0.5 is the largest of {0.3, 0.5, 0.7} that runs
+        # CFL 0.5: at the named CFL 0.7 the reference scheme's x+y+z-2M update
+        # empties a jet-corner cell in step 1 (density 0.004, negative
+        # variance), the CFL speed jumps 20x and a flux Jacobian turns NaN a
+        # few steps later (the reference's eigvals throws there); 0.5 is the
+        # largest of {0.3, 0.5, 0.7} that runs
         p = ic.default_params(Nx=160, Ny=160, Nz=80, Ma=1.0, Kn=1.0, CFL=0.5, tmax=1e9, nnmax=1000000)
     elif name == "c5":
         p = ic.default_params(Nx=256, Ny=256, Nz=128, Ma=1.0, Kn=0.01, CFL=0.5, tmax=1e9, nnmax=1000000)
