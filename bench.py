@@ -32,7 +32,7 @@ UNIT = "cell-steps/s"
 # and sqrt/cbrt/exp counted 1 each), crossing jets 160x160x80 Ma=1 Kn=1, first
 # step, averaged over a 160x160x8 slab through the jets; recomputed by
 # `python bench.py --count-ops`.
-F_ALG = 201144.5
+F_ALG = 68589.2
 B_ALG = 2 * 35 * 8  # bytes per cell-step: state read once, written once
 
 

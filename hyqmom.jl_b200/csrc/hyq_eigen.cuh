@@ -11,117 +11,15 @@
 namespace hyq {
 
 // ------------------------------------------------------------ jacobian6
-// Dual number with 6 derivative components (forward differentiation with
-// respect to W = (m02, m12, m22, m03, m13, m04)).
-struct Dual {
-  double v, d[6];
-};
-HQD Dual dconst(double x) { Dual r; r.v = x;
-#pragma unroll
-  for (int i = 0; i < 6; ++i) r.d[i] = 0.0; return r; }
-HQD Dual operator+(const Dual& a, const Dual& b) { Dual r; r.v = a.v + b.v;
-#pragma unroll
-  for (int i = 0; i < 6; ++i) r.d[i] = a.d[i] + b.d[i]; return r; }
-HQD Dual operator-(const Dual& a, const Dual& b) { Dual r; r.v = a.v - b.v;
-#pragma unroll
-  for (int i = 0; i < 6; ++i) r.d[i] = a.d[i] - b.d[i]; return r; }
-HQD Dual operator-(const Dual& a) { Dual r; r.v = -a.v;
-#pragma unroll
-  for (int i = 0; i < 6; ++i) r.d[i] = -a.d[i]; return r; }
-HQD Dual operator*(const Dual& a, const Dual& b) { Dual r; r.v = a.v * b.v;
-#pragma unroll
-  for (int i = 0; i < 6; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i]; return r; }
-HQD Dual operator/(const Dual& a, const Dual& b) { Dual r; r.v = a.v / b.v;
-#pragma unroll
-  for (int i = 0; i < 6; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) / b.v; return r; }
-HQD Dual dsqrt(const Dual& a) { Dual r; r.v = sqrt(a.v);
-#pragma unroll
-  for (int i = 0; i < 6; ++i) r.d[i] = a.d[i] / (2.0 * r.v); return r; }
-
-// 2-D moment tables in jacobian6 argument order: exponents and shift-pass orders
-__device__ constexpr int A2[15] = {0, 0, 0, 0, 0, 1, 1, 1, 1, 2, 2, 2, 3, 3, 4};
-__device__ constexpr int B2[15] = {0, 1, 2, 3, 4, 0, 1, 2, 3, 0, 1, 2, 0, 1, 0};
-__device__ constexpr int PASS2X[15] = {14, 12, 13, 9, 10, 11, 5, 6, 7, 8, 0, 1, 2, 3, 4};
-__device__ constexpr int PASS2Y[15] = {4, 3, 8, 2, 7, 11, 1, 6, 10, 13, 0, 5, 9, 12, 14};
-__device__ constexpr int AB2[5][5] = {{0, 1, 2, 3, 4}, {5, 6, 7, 8, -1}, {9, 10, 11, -1, -1}, {12, 13, -1, -1, -1}, {14, -1, -1, -1, -1}};
-
 // m[15] in jacobian6 argument order (m00,m01,m02,m03,m04,m10,m11,m12,m13,
 // m20,m21,m22,m30,m31,m40); m_ab = E[x^a y^b], x = flux direction.
 // Output: rows 3, 5, 6 of the Jacobian (rows 1, 2, 4 are unit rows e2, e3, e5).
+// The body is the closed form d(m32,m23,m14)/dC chained with dC/dW, derived
+// symbolically from the 2-D HyQMOM closure by codegen/gen_jacobian6.py; the
+// CPU oracle includes the same generated body.
 HQN void jacobian6_rows(const double* m, double* r3, double* r5, double* r6) {
-  // index of m_ab in the argument list
-  const int (&AB)[5][5] = AB2;
-  const int SEED[15] = {-1, -1, 0, 3, 5, -1, -1, 1, 4, -1, -1, 2, -1, -1, -1};
-  Dual R[15];
-  for (int n = 0; n < 15; ++n) { R[n] = dconst(m[n]); if (SEED[n] >= 0) R[n].d[SEED[n]] = 1.0; }
-  const Dual m00 = R[0];
-  const Dual u = R[5] / m00, vv = R[1] / m00;
-  // central 2-D moments: x pass then y pass of the binomial shift
-  Dual Cc[15];
-  for (int n = 0; n < 15; ++n) Cc[n] = R[n] / m00;
-  const Dual nu = -u, nv = -vv;
-  for (int t = 0; t < 15; ++t) {
-    const int n = PASS2X[t], a = A2[n], b = B2[n];
-    if (a == 0) continue;
-    Dual pw = dconst(1.0), acc = dconst(0.0);
-    Dual terms[5];
-    for (int q = 0; q <= a; ++q) { terms[q] = pw; pw = pw * nu; }  // terms[q] = (-u)^q
-    for (int p = 0; p <= a; ++p) acc = acc + (dconst(double(binom(a, p))) * terms[a - p]) * Cc[AB[p][b]];
-    Cc[n] = acc;
-  }
-  for (int t = 0; t < 15; ++t) {
-    const int n = PASS2Y[t], a = A2[n], b = B2[n];
-    if (b == 0) continue;
-    Dual pw = dconst(1.0), acc = dconst(0.0);
-    Dual terms[5];
-    for (int q = 0; q <= b; ++q) { terms[q] = pw; pw = pw * nv; }
-    for (int p = 0; p <= b; ++p) acc = acc + (dconst(double(binom(b, p))) * terms[b - p]) * Cc[AB[a][p]];
-    Cc[n] = acc;
-  }
-  const Dual sx = dsqrt(Cc[AB[2][0]]), sy = dsqrt(Cc[AB[0][2]]);
-  auto S = [&](int a, int b) {
-    Dual d = dconst(1.0);
-    for (int i = 0; i < a; ++i) d = d * sx;
-    for (int i = 0; i < b; ++i) d = d * sy;
-    return Cc[AB[a][b]] / d;
-  };
-  const Dual S30 = S(3, 0), S40 = S(4, 0), S03 = S(0, 3), S04 = S(0, 4), S11 = S(1, 1), S21 = S(2, 1), S12 = S(1, 2), S31 = S(3, 1),
-             S13 = S(1, 3), S22 = S(2, 2);
-  const Dual one = dconst(1.0), two = dconst(2.0), three = dconst(3.0);
-  auto c32 = [&](const Dual& Sj3, const Dual& Si3, const Dual& Si4, const Dual& Sij, const Dual& Sijj, const Dual& Siij, const Dual& Siijj,
-                 const Dual& Siiij) {
-    return ((Sj3 * Si3 * Si3) / two - Sj3 + Sj3 * (Si3 * Si3 - Si4 + one)) * Sij + (Si4 - (three * Si3 * Si3) / two) * Sijj +
-           (-(three * Sj3 * Si3) / two) * Siij + ((three * Si3) / two) * Siijj + Sj3 * Siiij - Si3 / two;
-  };
-  const Dual S32 = c32(S03, S30, S40, S11, S12, S21, S22, S31);
-  const Dual S23 = c32(S30, S03, S04, S11, S21, S12, S22, S13);
-  const Dual S14 = (S03 - two * S03 * S04 + (dconst(9.0) * S03 * S03 * S03) / dconst(4.0)) * S11 +
-                   ((dconst(5.0) * S04) / two - (dconst(15.0) * S03 * S03) / dconst(4.0) - dconst(1.5)) * S12 + (two * S03) * S13;
-  auto scl = [&](Dual s, int a, int b) { for (int i = 0; i < a; ++i) s = s * sx; for (int i = 0; i < b; ++i) s = s * sy; return s; };
-  const Dual C32 = scl(S32, 3, 2), C23 = scl(S23, 2, 3), C14 = scl(S14, 1, 4);
-  Dual qu[6], qv[6];
-  qu[0] = dconst(1.0); qv[0] = dconst(1.0);
-  for (int i = 1; i < 6; ++i) { qu[i] = qu[i - 1] * u; qv[i] = qv[i - 1] * vv; }
-  auto Ct = [&](int a, int b) -> Dual {
-    if (a + b == 0) return dconst(1.0);
-    if (a + b == 1) return dconst(0.0);
-    if (a == 3 && b == 2) return C32;
-    if (a == 2 && b == 3) return C23;
-    if (a == 1 && b == 4) return C14;
-    return Cc[AB[a][b]];
-  };
-  auto raw = [&](int a, int b) {
-    Dual s = dconst(0.0);
-    for (int p = 0; p <= a; ++p)
-      for (int q = 0; q <= b; ++q) {
-        if (p + q == 1) continue;
-        s = s + dconst(double(binom(a, p) * binom(b, q))) * Ct(p, q) * (qu[a - p] * qv[b - q]);
-      }
-    return m00 * s;
-  };
-  const Dual m32 = raw(3, 2), m23 = raw(2, 3), m14 = raw(1, 4);
-#pragma unroll
-  for (int j = 0; j < 6; ++j) { r3[j] = m32.d[j]; r5[j] = m23.d[j]; r6[j] = m14.d[j]; }
+  typedef double R;
+#include "gen_jacobian6.inc"
 }
 
 // ------------------------------------------- LAPACK-path eigenvalues, N <= 6

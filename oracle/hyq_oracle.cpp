@@ -195,6 +195,12 @@ void hyqo_jacobian6(const double* m, double* J) {
   jacobian6<double>(mm, JJ);
   for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) J[i * 6 + j] = JJ[i][j];
 }
+void hyqo_jacobian6_ad(const double* m, double* J) {
+  double mm[15], JJ[6][6];
+  for (int i = 0; i < 15; ++i) mm[i] = m[i];
+  jacobian6_ad<double>(mm, JJ);
+  for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) J[i * 6 + j] = JJ[i][j];
+}
 int hyqo_eig6(const double* A, double* wr, double* wi) {
   double AA[6][6], r[6], im[6];
   for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) AA[i][j] = A[i * 6 + j];

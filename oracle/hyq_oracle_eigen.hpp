@@ -10,7 +10,8 @@ namespace hyqo {
 // jacobian6 (src/autogen/jacobian6.jl:14-59) is the Jacobian of the x-fluxes
 // (m12, m22, m32, m13, m23, m14) of W = (m02, m12, m22, m03, m13, m04) for
 // the 2-D HyQMOM closure of (m32, m23, m14); m_ab = E[x^a y^b], x the flux
-// direction.  Here it is evaluated with 6-component dual numbers.
+// direction.  jacobian6_ad evaluates it with 6-component dual numbers and
+// is kept as an independent check of the closed form below.
 template <class T> struct D6 {
   T v, d[6];
   D6() {}
@@ -33,7 +34,7 @@ template <class T> D6<T> dsqrt(const D6<T>& a) {
 }
 template <class T> D6<T> dc(double x) { return D6<T>(T(x)); }
 
-template <class T> void jacobian6(const T (&m)[15], T (&J)[6][6]) {
+template <class T> void jacobian6_ad(const T (&m)[15], T (&J)[6][6]) {
   // argument order (m00,m01,m02,m03,m04,m10,m11,m12,m13,m20,m21,m22,m30,m31,m40)
   static const int ab[15][2] = {{0, 0}, {0, 1}, {0, 2}, {0, 3}, {0, 4}, {1, 0}, {1, 1}, {1, 2}, {1, 3}, {2, 0}, {2, 1}, {2, 2}, {3, 0}, {3, 1}, {4, 0}};
   static const int seed[15] = {-1, -1, 0, 3, 5, -1, -1, 1, 4, -1, -1, 2, -1, -1, -1};
@@ -108,6 +109,17 @@ template <class T> void jacobian6(const T (&m)[15], T (&J)[6][6]) {
   for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) J[i][j] = T(0);
   J[0][1] = T(1); J[1][2] = T(1); J[3][4] = T(1);
   for (int j = 0; j < 6; ++j) { J[2][j] = m32.d[j]; J[4][j] = m23.d[j]; J[5][j] = m14.d[j]; }
+}
+
+// jacobian6 in closed form: d(m32,m23,m14)/dC derived symbolically from the
+// same closure (hyqmom.jl_b200/codegen/gen_jacobian6.py), chained with dC/dW.
+template <class T> void jacobian6(const T (&m)[15], T (&J)[6][6]) {
+  typedef T R;
+  T r3[6], r5[6], r6[6];
+#include "gen_jacobian6.inc"
+  for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) J[i][j] = T(0);
+  J[0][1] = T(1); J[1][2] = T(1); J[3][4] = T(1);
+  for (int j = 0; j < 6; ++j) { J[2][j] = r3[j]; J[4][j] = r5[j]; J[5][j] = r6[j]; }
 }
 
 // ------------------------------------- LAPACK-path nonsymmetric eigenvalues
