@@ -166,6 +166,20 @@ void enqueue_step(hyq_ctx* ctx, cudaStream_t s) {
 }
 }  // namespace
 
+// Launch helpers for other translation units (same kernels and shapes as
+// enqueue_step).
+namespace hyqk {
+void launch_cfl(const double* blockmax, const StepConst& sc, DevClock* clk, cudaStream_t s) {
+  k_cfl<<<1, 1024, 0, s>>>(blockmax, sc, clk);
+}
+void launch_hll(const double* M, const double* Fx, const double* Fy, const double* Fz, const double* vp, double* Mout, const StepConst& sc,
+                const DevClock* clk, cudaStream_t s) {
+  k_hll<<<dim3(grid_of(sc.N, BS_HLL), 35), BS_HLL, 0, s>>>(M, Fx, Fy, Fz, vp, Mout, sc, clk);
+}
+void launch_set_clock(DevClock* clk, double t, long long nn, cudaStream_t s) { k_set_clock<<<1, 1, 0, s>>>(clk, t, nn); }
+int report_error(int code, const char* msg) { return fail(nullptr, code, msg); }
+}  // namespace hyqk
+
 extern "C" {
 
 int hyq_abi_version(void) { return HYQ_ABI_VERSION; }

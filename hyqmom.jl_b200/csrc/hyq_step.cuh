@@ -40,6 +40,13 @@ void launch_cells_eig(const double* M, long long n, int axis, int flag2D, double
 void launch_cells_closure_eigs(const double* mom, long long n, double* v, cudaStream_t s);
 void launch_cells_collision(const double* M, long long n, double dt, double Kn, int positivity, double* out, cudaStream_t s);
 void launch_std_central(const double* M, long long n, double* S, double* C, cudaStream_t s);
+// (defined in hyq_b200.cu) the CFL, HLL and clock-reset launches of one step,
+// and the thread-local error text read by hyq_last_error(NULL)
+void launch_cfl(const double* blockmax, const StepConst& sc, DevClock* clk, cudaStream_t s);
+void launch_hll(const double* M, const double* Fx, const double* Fy, const double* Fz, const double* vp, double* Mout, const StepConst& sc,
+                const DevClock* clk, cudaStream_t s);
+void launch_set_clock(DevClock* clk, double t, long long nn, cudaStream_t s);
+int report_error(int code, const char* msg);
 
 }  // namespace hyqk
 

@@ -94,6 +94,27 @@ void* hyq_stream(hyq_ctx* ctx);
  * phase E+F.  For profiling; results equal hyq_advance. */
 int hyq_advance_timed(hyq_ctx* ctx, int64_t steps, float* ms);
 
+/* ---- allocation-free step ------------------------------------------------
+ * No counterpart in the reference (its Julia loop allocates freely); added
+ * for callers that must not allocate device memory while they step: a host
+ * program that passes in a buffer from its own pool under a fixed memory
+ * budget, or a loop that cannot take the device-wide synchronisation that
+ * cudaMalloc/cudaFree may cause.  hyq_step_noalloc runs one step of the same
+ * kernels as hyq_advance on M (device pointer, 35*N doubles, the moment-major
+ * layout of hyq_set_state_device), updated in place.  stats: in, t and nn of
+ * the state; out, t, dt, vmax, nn, done and status after the step (no step is
+ * taken once t >= tmax or nn >= nnmax).  It returns after the step finished
+ * on `stream` (a cudaStream_t, NULL = default stream).
+ * Its work arrays live in one fixed scratch array in the library's device
+ * image (about 19 MB), sized for at most HYQ_NOALLOC_MAX_CELLS cells; larger
+ * grids get HYQ_EINVAL.  All calls on a device share that scratch, so calls
+ * that overlap on one device (other host threads, unordered streams) race
+ * and corrupt each other's step.  The first call on each device looks up the
+ * scratch address (and may load the module); make it before any stream
+ * capture on that device. */
+#define HYQ_NOALLOC_MAX_CELLS 16384
+int hyq_step_noalloc(const hyq_params* p, double* M, hyq_stats* stats, void* stream);
+
 /* ---- per-cell entry points on device arrays (SoA, stride n) ------------
  * Used by parity tests and by callers composing their own loops.  `stream`
  * is a cudaStream_t (NULL = default stream).  Arrays are device pointers. */
