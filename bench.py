@@ -32,8 +32,16 @@ UNIT = "cell-steps/s"
 # and sqrt/cbrt/exp counted 1 each), crossing jets 160x160x80 Ma=1 Kn=1, first
 # step, averaged over a 160x160x8 slab through the jets; recomputed by
 # `python bench.py --count-ops`.
-F_ALG = 68589.2
+F_ALG = 43772.6
 B_ALG = 2 * 35 * 8  # bytes per cell-step: state read once, written once
+
+# The step's kernels in launch order (hyq_advance_timed slots) and their FP64
+# operations per cell from the same count (CFL: one max per cell; HLL: three
+# sweeps of 18 ops per moment plus the 4-op combination).
+KERNELS = ["A1_closure", "A2_eig_x", "A3_eig_y", "A4_eig_z", "A5_flux_speeds", "cfl", "hll",
+           "E1_closure", "E2_eig_x", "E3_eig_y", "E4_closure_bgk"]
+F_KERNEL = {"A1_closure": 7583.0, "A2_eig_x": 1696.2, "A3_eig_y": 1696.2, "A4_eig_z": 1708.2, "A5_flux_speeds": 9709.4,
+            "cfl": 1.0, "hll": 2030.0, "E1_closure": 7583.0, "E2_eig_x": 1696.3, "E3_eig_y": 1696.3, "E4_closure_bgk": 8374.0}
 
 
 def workload(name="c2"):
@@ -208,10 +216,10 @@ def run_gpu(args, rank, world, local_rank):
     s.set_state(M0)
     s.advance(args.warmup)
     import ctypes
-    kms = (ctypes.c_float * 4)()
+    kms = (ctypes.c_float * len(KERNELS))()
     ksteps = max(1, min(args.steps, 3))
     s._chk(s._lib.hyq_advance_timed(s._h, ksteps, kms))
-    kern = {"phase_A": kms[0] / ksteps, "cfl": kms[1] / ksteps, "hll": kms[2] / ksteps, "phase_EF": kms[3] / ksteps}
+    kern = {k: kms[i] / ksteps for i, k in enumerate(KERNELS)}
 
     # end to end through the public API: each step copies the host (pinned)
     # state in, advances one step and reads the state back, on the same steps
@@ -238,21 +246,27 @@ def run_gpu(args, rank, world, local_rank):
             dist.destroy_process_group()
         return
     fp64 = fp64_peak_tflops(torch)
-    falg = F_ALG
-    a_ms = kern["phase_A"] + kern["phase_EF"]
-    achieved = (falg * cells / (ms / args.steps * 1e-3) / 1e12) if falg else None
-    roof = {"bound": "fp64", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
-            "frac": (achieved / fp64) if (achieved and fp64) else None, "traffic": None,
+    # roofline of the dominant kernel: its algorithmic FP64 ops per launch over
+    # its mean launch time; the FP64 peak is a measured DGEMM (an FMA counts 2)
+    dom = max((k for k in KERNELS if k not in ("cfl", "hll")), key=lambda k: kern[k])
+    ach = F_KERNEL[dom] * cells / (kern[dom] * 1e-3) / 1e12
+    per_kernel = {k: {"ms": round(kern[k], 3), "tflops": round(F_KERNEL[k] * cells / (kern[k] * 1e-3) / 1e12, 3)}
+                  for k in KERNELS if k not in ("cfl",)}
+    step_tflops = F_ALG * cells / (ms / args.steps * 1e-3) / 1e12
+    roof = {"bound": "fp64", "achieved": ach, "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64, "traffic": None,
             "peak_source": "measured in this run: FP64 DGEMM 8192^3 (cuBLAS via torch), best of 3",
-            "dominant_kernel": "k_phase_A", "kernel_ms": kern,
-            "hbm_achieved_gbs": B_ALG * cells / (ms / args.steps * 1e-3) / 1e9}
+            "dominant_kernel": "k_" + dom, "f_alg_per_cell": F_KERNEL[dom],
+            "note": "built with -fmad=false: every counted op is one FP64 pipe instruction, so an FMA-free kernel tops out at peak/2",
+            "step": {"f_alg_per_cell": F_ALG, "achieved": step_tflops, "frac": step_tflops / fp64,
+                     "hbm_achieved_gbs": B_ALG * cells / (ms / args.steps * 1e-3) / 1e9},
+            "kernels": per_kernel}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (reference crossing-jets IC generator)",
             "config": {"workload": f"crossing jets {p['Nx']}x{p['Ny']}x{p['Nz']} Ma={p['Ma']} Kn={p['Kn']} CFL={p['CFL']}, plain eig",
                        "cells": cells, "parallelism": f"replicas x{world}", "l2": "state 573 MB > L2, no flush needed",
                        "steps_done": st["nn"]},
-            "gpu_launches": 4 * args.steps, "e2e": e2e, "roofline": roof, "clocks": sampler.summary()}
+            "gpu_launches": len(KERNELS) * args.steps, "e2e": e2e, "roofline": roof, "clocks": sampler.summary()}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, seconds=15.0)
     print(json.dumps(line), flush=True)
@@ -270,9 +284,12 @@ def count_ops():
     cells = M.shape[0] * M.shape[1] * M.shape[2]
     dt = 1e-3
     out = ol.count_ops(M, q, dt)
+    st = ol.count_ops_stages(M, q, dt) / cells
     per = (out[0] + out[1]) / cells + out[2]
+    names = [k for k in KERNELS if k not in ("cfl", "hll")]
     print(json.dumps({"cells": cells, "phase_A_ops_per_cell": out[0] / cells, "phase_EF_ops_per_cell": out[1] / cells,
-                      "hll_ops_per_cell": out[2], "F_alg": per}))
+                      "hll_ops_per_cell": out[2], "F_alg": per,
+                      "per_kernel": {k: round(float(v), 1) for k, v in zip(names, st)}}))
 
 
 def main():

@@ -1,21 +1,22 @@
 // libhyqmom_b200.so: kernels and C-ABI of the HyQMOM explicit step on B200.
 //
-// One step = four launches on the context stream, captured once in a CUDA
+// One step = eleven launches on the context stream, captured once in a CUDA
 // graph and replayed:
-//   k_phase_A    per cell: closure + realizability, x/y/z flux-Jacobian
-//                eigenvalues, closure of the realized moments, 1-D closure
-//                speeds; writes Fx, Fy, Fz, the realized state and 6 speeds,
-//                and a NaN-propagating per-block max |speed|
-//                (src/simulation_runner.jl:352-383)
+//   phase A      five per-cell kernels (k_phase_A.cu): closure +
+//                realizability, x, y and z flux-Jacobian eigenvalues with
+//                their corrections, closure of the realized moments with
+//                fluxes and the 1-D closure speeds; writes Fx, Fy, Fz, the
+//                realized state and 6 speeds, and a NaN-propagating
+//                per-block max |speed| (src/simulation_runner.jl:352-383)
 //   k_cfl        one block: global max -> dt, t += dt, nn += 1 on the device
 //                (src/simulation_runner.jl:402-433, 496)
-//   k_hll        per (cell, moment): x, y, z HLL updates with pas_HLL's copy
+//   k_hll        per cell, all 35 moments: x, y, z HLL updates with pas_HLL's copy
 //                boundary handling, combined as Mx + My + Mz - 2M
 //                (src/numerics/apply_flux_update_3d.jl:30-213,
 //                 src/numerics/pas_HLL.jl:238-298, flux_HLL.jl:318-330,
 //                 src/simulation_runner.jl:498-520)
-//   k_phase_EF   per cell: realizability pass and BGK collision
-//                (src/simulation_runner.jl:526-557)
+//   phase EF     four per-cell kernels (k_phase_EF.cu): realizability pass
+//                and BGK collision (src/simulation_runner.jl:526-557)
 // The loop predicate `t < tmax && nn < nnmax` is evaluated on the device, so
 // any number of steps can be queued without a host round trip.
 //
@@ -60,62 +61,105 @@ __global__ void __launch_bounds__(1024) k_cfl(const double* __restrict__ blockma
   }
 }
 
-// One directional HLL update of moment n of cell (i) along a line of Np
-// cells with stride `st`, at cell offset c0 of the line start.
-__device__ __forceinline__ double hll_line(const double* __restrict__ M, const double* __restrict__ F, const double* __restrict__ vmin,
-                                           const double* __restrict__ vmax, long long base, long long st, int Np, int i, double r) {
-  if (Np == 2) return M[base + st];  // pas_HLL with Np = 2 returns [M2, M2]
-  const int ip = i < 1 ? 1 : (i > Np - 2 ? Np - 2 : i);
-  // face j between cells j and j+1; Flux_j for j = ip-1 and ip
-  auto wface = [&](int j, double& ll, double& lr, double& ws) {
-    // W* at face j (j in 1..Np-2); j == 0 uses W*[1] with zero speeds
-    const int jj = j < 1 ? 1 : j;
-    const double a = vmin[base + st * jj], b = vmin[base + st * (jj + 1)];
-    const double c = vmax[base + st * jj], d = vmax[base + st * (jj + 1)];
-    const double l1 = jmin(a, b), l2 = jmax(c, d);
-    double w = 0.0;
-    if (fabs(l1 - l2) > 1e-10) {
-      const double mj = M[base + st * jj], mj1 = M[base + st * (jj + 1)];
-      const double fj = F[base + st * jj], fj1 = F[base + st * (jj + 1)];
-      w = (l1 * mj - l2 * mj1) / (l1 - l2) - (fj - fj1) / (l1 - l2);
-    }
-    ws = w;
-    if (j == 0) { ll = 0.0; lr = 0.0; } else { ll = l1; lr = l2; }
-  };
-  auto flux = [&](int j) {
-    double ll, lr, ws;
-    wface(j, ll, lr, ws);
-    // boundary-modified fluxes: F[0] := F[1], F[Np-1] := F[Np-2]
-    const int fa = j < 1 ? 1 : j;
-    const int fb = (j + 1 > Np - 2) ? Np - 2 : j + 1;
-    const double Fa = F[base + st * fa], Fb = F[base + st * fb];
-    const double Ma_ = M[base + st * j], Mb = M[base + st * (j + 1)];
-    return 0.5 * (Fa + Fb) - 0.5 * (fabs(ll) * (ws - Ma_) - fabs(lr) * (ws - Mb));
-  };
-  const double f1 = flux(ip), f0 = flux(ip - 1);
-  return M[base + st * ip] - r * (f1 - f0);
+// pas_HLL along one line of Np cells (stride `st`, line start `base`) for the
+// cell at position i of the line: the two faces it touches, with everything
+// that does not depend on the moment (clamped indices, HLL speeds of the
+// face, whether W* is formed) resolved once per cell.
+struct HllFace {
+  int jj, fa, fb, j;        // W* cell jj (and jj+1), flux cells fa, fb, face cells j, j+1 (offsets from base)
+  double l1, l2, ll, lr;
+  bool w;
+};
+struct HllLine {
+  long long base;
+  int st, ip;               // ip: offset of the clamped cell whose update is returned
+  int Np;
+  double r;                 // dt / ds
+  HllFace f0, f1;           // faces ip-1 and ip
+};
+
+__device__ __forceinline__ HllFace hll_face(const double* __restrict__ vmin, const double* __restrict__ vmax, long long base, int st,
+                                            int Np, int j) {
+  HllFace f;
+  const int jj = j < 1 ? 1 : j;  // face 0 uses W*[1] with zero speeds
+  const double a = vmin[base + st * jj], b = vmin[base + st * (jj + 1)];
+  const double c = vmax[base + st * jj], d = vmax[base + st * (jj + 1)];
+  f.l1 = jmin(a, b);
+  f.l2 = jmax(c, d);
+  f.w = fabs(f.l1 - f.l2) > 1e-10;
+  if (j == 0) { f.ll = 0.0; f.lr = 0.0; } else { f.ll = f.l1; f.lr = f.l2; }
+  f.jj = st * jj;
+  // boundary-modified fluxes: F[0] := F[1], F[Np-1] := F[Np-2]
+  f.fa = st * (j < 1 ? 1 : j);
+  f.fb = st * ((j + 1 > Np - 2) ? Np - 2 : j + 1);
+  f.j = st * j;
+  return f;
 }
 
-__global__ void __launch_bounds__(BS_HLL) k_hll(const double* __restrict__ M, const double* __restrict__ Fx, const double* __restrict__ Fy,
+__device__ __forceinline__ HllLine hll_setup(const double* __restrict__ vmin, const double* __restrict__ vmax, long long base, int st,
+                                             int Np, int i, double r) {
+  HllLine L;
+  L.base = base; L.st = st; L.Np = Np; L.r = r;
+  if (Np == 2) { L.ip = st; return L; }  // pas_HLL with Np = 2 returns [M2, M2]
+  const int ip = i < 1 ? 1 : (i > Np - 2 ? Np - 2 : i);
+  L.ip = st * ip;
+  L.f0 = hll_face(vmin, vmax, base, st, Np, ip - 1);
+  L.f1 = hll_face(vmin, vmax, base, st, Np, ip);
+  return L;
+}
+
+// flux_HLL at one face for one moment (M, F already offset to the moment;
+// `st` the line stride)
+__device__ __forceinline__ double hll_flux(const double* __restrict__ M, const double* __restrict__ F, long long base, int st,
+                                           const HllFace& f) {
+  double ws = 0.0;
+  if (f.w) {
+    const double mj = M[base + f.jj], mj1 = M[base + f.jj + st];
+    const double fj = F[base + f.jj], fj1 = F[base + f.jj + st];
+    ws = (f.l1 * mj - f.l2 * mj1) / (f.l1 - f.l2) - (fj - fj1) / (f.l1 - f.l2);
+  }
+  const double Fa = F[base + f.fa], Fb = F[base + f.fb];
+  const double Ma_ = M[base + f.j], Mb = M[base + f.j + st];
+  return 0.5 * (Fa + Fb) - 0.5 * (fabs(f.ll) * (ws - Ma_) - fabs(f.lr) * (ws - Mb));
+}
+
+// The x, y or z update of one moment of the cell (pas_HLL for that line).
+__device__ __forceinline__ double hll_update(const double* __restrict__ M, const double* __restrict__ F, const HllLine& L) {
+  if (L.Np == 2) return M[L.base + L.ip];
+  const double f1 = hll_flux(M, F, L.base, L.st, L.f1), f0 = hll_flux(M, F, L.base, L.st, L.f0);
+  return M[L.base + L.ip] - L.r * (f1 - f0);
+}
+
+// One thread per cell: the face speeds of the x, y and z lines are resolved
+// once, then the 35 moments are updated in turn (coalesced along x).
+#ifndef HQ_MINB_HLL
+#define HQ_MINB_HLL 3
+#endif
+__global__ void __launch_bounds__(BS_HLL, HQ_MINB_HLL) k_hll(const double* __restrict__ M, const double* __restrict__ Fx, const double* __restrict__ Fy,
                                                  const double* __restrict__ Fz, const double* __restrict__ vp, double* __restrict__ Mout,
                                                  const StepConst sc, const DevClock* clk) {
   if (!clk->active) return;
   const long long N = sc.N;
   const long long c = (long long)blockIdx.x * BS_HLL + threadIdx.x;
-  const int n = blockIdx.y;
   if (c >= N) return;
   const double dt = clk->dt;
   const int Nx = sc.Nx, Ny = sc.Ny, Nz = sc.Nz;
   const int i = int(c % Nx);
   const int j = int((c / Nx) % Ny);
   const int k = int(c / ((long long)Nx * Ny));
-  const long long mo = N * n;
-  const double* Mn = M + mo;
-  // x: line base at (0, j, k), stride 1
-  const double mx = hll_line(Mn, Fx + mo, vp, vp + N, c - i, 1, Nx, i, dt / sc.dx);
-  const double my = hll_line(Mn, Fy + mo, vp + 2 * N, vp + 3 * N, c - (long long)j * Nx, Nx, Ny, j, dt / sc.dy);
-  const double mz = (Nz == 1) ? Mn[c] : hll_line(Mn, Fz + mo, vp + 4 * N, vp + 5 * N, c - (long long)k * Nx * Ny, (long long)Nx * Ny, Nz, k, dt / sc.dz);
-  Mout[c + mo] = mx + my + mz - 2.0 * Mn[c];
+  const HllLine X = hll_setup(vp, vp + N, c - i, 1, Nx, i, dt / sc.dx);
+  const HllLine Y = hll_setup(vp + 2 * N, vp + 3 * N, c - (long long)j * Nx, Nx, Ny, j, dt / sc.dy);
+  HllLine Z;
+  if (Nz > 1) Z = hll_setup(vp + 4 * N, vp + 5 * N, c - (long long)k * Nx * Ny, Nx * Ny, Nz, k, dt / sc.dz);
+#pragma unroll 1
+  for (int n = 0; n < 35; ++n) {
+    const long long mo = N * n;
+    const double* Mn = M + mo;
+    const double mx = hll_update(Mn, Fx + mo, X);
+    const double my = hll_update(Mn, Fy + mo, Y);
+    const double mz = (Nz == 1) ? Mn[c] : hll_update(Mn, Fz + mo, Z);
+    Mout[c + mo] = mx + my + mz - 2.0 * Mn[c];
+  }
 }
 
 __global__ void k_set_clock(DevClock* clk, double t, long long nn) {
@@ -158,11 +202,10 @@ int cuda_fail(hyq_ctx* ctx, cudaError_t e, const char* what) {
 
 void enqueue_step(hyq_ctx* ctx, cudaStream_t s) {
   const long long N = ctx->N;
-  launch_phase_A(ctx->sc, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s);
+  launch_phase_A(ctx->sc, ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s);
   k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
-  dim3 gh(grid_of(N, BS_HLL), 35);
-  k_hll<<<gh, BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
-  launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->clk, s);
+  k_hll<<<grid_of(N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
+  launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->clk, s);
 }
 }  // namespace
 
@@ -174,7 +217,7 @@ void launch_cfl(const double* blockmax, const StepConst& sc, DevClock* clk, cuda
 }
 void launch_hll(const double* M, const double* Fx, const double* Fy, const double* Fz, const double* vp, double* Mout, const StepConst& sc,
                 const DevClock* clk, cudaStream_t s) {
-  k_hll<<<dim3(grid_of(sc.N, BS_HLL), 35), BS_HLL, 0, s>>>(M, Fx, Fy, Fz, vp, Mout, sc, clk);
+  k_hll<<<grid_of(sc.N, BS_HLL), BS_HLL, 0, s>>>(M, Fx, Fy, Fz, vp, Mout, sc, clk);
 }
 void launch_set_clock(DevClock* clk, double t, long long nn, cudaStream_t s) { k_set_clock<<<1, 1, 0, s>>>(clk, t, nn); }
 int report_error(int code, const char* msg) { return fail(nullptr, code, msg); }
@@ -193,6 +236,8 @@ int hyq_create(const hyq_params* p, hyq_ctx** out) {
     return fail(nullptr, HYQ_EINVAL, "grid must have Nx >= 2, Ny >= 2, Nz >= 1 (pas_HLL needs two cells per row)");
   if (!(p->CFL > 0) || !(p->Kn > 0) || !(p->dtmax > 0))
     return fail(nullptr, HYQ_EINVAL, "CFL, Kn and dtmax must be positive");
+  if ((long long)p->Nx * p->Ny * p->Nz >= (1LL << 31))
+    return fail(nullptr, HYQ_EINVAL, "grid must have fewer than 2^31 cells (in-line offsets are 32-bit)");
   hyq_ctx* ctx = new hyq_ctx();
   ctx->p = *p;
   ctx->device = p->device;
@@ -306,29 +351,28 @@ int hyq_advance_async(hyq_ctx* ctx, int64_t max_steps) {
 int hyq_advance_timed(hyq_ctx* ctx, int64_t steps, float* ms) {
   if (!ctx || !ms || steps < 0) return fail(ctx, HYQ_EINVAL, "bad argument");
   HQ_CHECK(ctx, cudaSetDevice(ctx->device));
-  cudaEvent_t ev[5];
-  for (int q = 0; q < 5; ++q) HQ_CHECK(ctx, cudaEventCreate(&ev[q]));
-  for (int q = 0; q < 4; ++q) ms[q] = 0.0f;
+  constexpr int K = HYQ_TIMED_SLOTS;
+  cudaEvent_t ev[K + 1];
+  for (int q = 0; q <= K; ++q) HQ_CHECK(ctx, cudaEventCreate(&ev[q]));
+  for (int q = 0; q < K; ++q) ms[q] = 0.0f;
   const long long N = ctx->N;
   cudaStream_t s = ctx->stream;
   for (int64_t it = 0; it < steps; ++it) {
     cudaEventRecord(ev[0], s);
-    launch_phase_A(ctx->sc, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s);
-    cudaEventRecord(ev[1], s);
+    launch_phase_A(ctx->sc, ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s, ev + 1);
     k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
-    cudaEventRecord(ev[2], s);
-    k_hll<<<dim3(grid_of(N, BS_HLL), 35), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
-    cudaEventRecord(ev[3], s);
-    launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->clk, s);
-    cudaEventRecord(ev[4], s);
-    HQ_CHECK(ctx, cudaEventSynchronize(ev[4]));
-    for (int q = 0; q < 4; ++q) {
+    cudaEventRecord(ev[6], s);
+    k_hll<<<grid_of(N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
+    cudaEventRecord(ev[7], s);
+    launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->clk, s, ev + 8);
+    HQ_CHECK(ctx, cudaEventSynchronize(ev[K]));
+    for (int q = 0; q < K; ++q) {
       float t = 0.0f;
       cudaEventElapsedTime(&t, ev[q], ev[q + 1]);
       ms[q] += t;
     }
   }
-  for (int q = 0; q < 5; ++q) cudaEventDestroy(ev[q]);
+  for (int q = 0; q <= K; ++q) cudaEventDestroy(ev[q]);
   HQ_CHECK(ctx, cudaGetLastError());
   return HYQ_OK;
 }

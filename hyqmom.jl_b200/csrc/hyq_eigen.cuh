@@ -499,18 +499,33 @@ HQN void closure_eigs(double m0, double m1, double m2, double m3, double m4, dou
   b2 = b2 * 5.0 / 2.0;
   if (!(isfinite(a0) && isfinite(a1) && isfinite(a2) && isfinite(b1) && isfinite(b2))) { vmin = qnan(); vmax = qnan(); return; }
   if (b1 >= 0.0 && b2 >= 0.0) {
+    // cyclic Jacobi; from the fourth sweep on, an off-diagonal entry too small
+    // to change either diagonal entry (|d| + 100|e| == |d|) is set to zero
+    // (Rutishauser's threshold rule).  p, q and kk are unrolled so that A
+    // stays in registers.
     double A[3][3] = {{a0, sqrt(b1), 0.0}, {sqrt(b1), a1, sqrt(b2)}, {0.0, sqrt(b2), a2}};
     for (int sweep = 0; sweep < 60; ++sweep) {
       const double off = fabs(A[0][1]) + fabs(A[0][2]) + fabs(A[1][2]);
       if (off == 0.0) break;
+#pragma unroll
       for (int p = 0; p < 2; ++p)
+#pragma unroll
         for (int q = p + 1; q < 3; ++q) {
           if (A[p][q] == 0.0) continue;
+          if (sweep >= 3) {
+            const double g = 100.0 * fabs(A[p][q]);
+            if (fabs(A[p][p]) + g == fabs(A[p][p]) && fabs(A[q][q]) + g == fabs(A[q][q])) {
+              A[p][q] = 0.0; A[q][p] = 0.0;
+              continue;
+            }
+          }
           const double theta = (A[q][q] - A[p][p]) / (2.0 * A[p][q]);
           double t = jsign(theta) / (fabs(theta) + sqrt(theta * theta + 1.0));
           if (theta == 0.0) t = 1.0;
           const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+#pragma unroll
           for (int kk = 0; kk < 3; ++kk) { const double akp = A[kk][p], akq = A[kk][q]; A[kk][p] = c * akp - s * akq; A[kk][q] = s * akp + c * akq; }
+#pragma unroll
           for (int kk = 0; kk < 3; ++kk) { const double apk = A[p][kk], aqk = A[q][kk]; A[p][kk] = c * apk - s * aqk; A[q][kk] = s * apk + c * aqk; }
         }
     }

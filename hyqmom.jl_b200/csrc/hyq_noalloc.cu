@@ -102,10 +102,10 @@ extern "C" int hyq_step_noalloc(const hyq_params* p, double* M, hyq_stats* stats
   cudaStream_t s = static_cast<cudaStream_t>(stream);
 
   launch_set_clock(clk, stats->t, (long long)stats->nn, s);
-  launch_phase_A(sc, M, Fx, Fy, Fz, vp, blockmax, clk, s);
+  launch_phase_A(sc, M, Mtmp, Fx, Fy, Fz, vp, blockmax, clk, s);
   launch_cfl(blockmax, sc, clk, s);
   launch_hll(M, Fx, Fy, Fz, vp, Mtmp, sc, clk, s);
-  launch_phase_EF(sc, Mtmp, M, clk, s);
+  launch_phase_EF(sc, Mtmp, M, Fx, Fy, Fz, clk, s);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "launch");
 
   DevClock h;

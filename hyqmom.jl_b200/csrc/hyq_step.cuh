@@ -22,6 +22,19 @@ struct StepConst {
   int nblocksA;
 };
 
+// Minimum resident blocks per SM requested from ptxas for the per-cell
+// kernels (bounds their registers): the closure kernels run best at 4 blocks
+// of 128 threads (128 registers), the eigenvalue kernels at 8 (64 registers);
+// measured on the 160x160x80 crossing-jets step.
+#ifndef HQ_MINB_CLOSURE
+#define HQ_MINB_CLOSURE 4
+#endif
+#ifndef HQ_MINB_EIG
+#define HQ_MINB_EIG 8
+#endif
+constexpr int MINB_CLOSURE = HQ_MINB_CLOSURE;
+constexpr int MINB_EIG = HQ_MINB_EIG;
+
 constexpr int BS_A = 128;
 constexpr int BS_EF = 128;
 constexpr int BS_HLL = 256;
@@ -30,9 +43,15 @@ constexpr int BS_CELLS = 128;
 inline int grid_of(long long n, int bs) { return int((n + bs - 1) / bs); }
 
 // launch wrappers (defined in k_phase_A.cu, k_phase_EF.cu, k_cells.cu)
-void launch_phase_A(const StepConst& sc, double* M, double* Fx, double* Fy, double* Fz, double* vp, double* blockmax, DevClock* clk,
-                    cudaStream_t s);
-void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, const DevClock* clk, cudaStream_t s);
+// Phase [A] in place on M; Mtmp, Fx, Fy, Fz carry its intermediate states,
+// and on completion Fx, Fy, Fz hold the fluxes (Mtmp is left as scratch).
+// ev (optional): five events recorded after the five kernels.
+void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, double* Fy, double* Fz, double* vp, double* blockmax,
+                    const DevClock* clk, cudaStream_t s, cudaEvent_t* ev = nullptr);
+// Phases [E]+[F] from Min to Mout; Fx, Fy, Fz are overwritten.
+// ev (optional): four events recorded after the four kernels.
+void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, double* Fx, double* Fy, double* Fz, const DevClock* clk,
+                     cudaStream_t s, cudaEvent_t* ev = nullptr);
 void launch_cells_phase_A(const double* M, long long n, int flag2D, double Ma, int positivity, double* Fx, double* Fy, double* Fz,
                           double* Mr, double* vp, cudaStream_t s);
 void launch_cells_flux(const double* M, long long n, int flag2D, double Ma, double* Fx, double* Fy, double* Fz, double* Mr, cudaStream_t s);

@@ -11,6 +11,7 @@ using namespace hyq;
 namespace hyqk {
 namespace {
 
+
 // One cell: in m[35]; out Fx, Fy, Fz, Mr (35 each) and vp[6].
 __device__ __noinline__ void cell_phase_A(const double* m, int flag2D, double Ma, int positivity, double* Fx, double* Fy, double* Fz, double* Mr,
                                           double* vp) {
@@ -30,25 +31,87 @@ __device__ __noinline__ void cell_phase_A(const double* m, int flag2D, double Ma
   vp[4] = jmin(v5zmin, v6zmin); vp[5] = jmax(v5zmax, v6zmax);
 }
 
-__global__ void __launch_bounds__(BS_A) k_phase_A(double* __restrict__ M, double* __restrict__ Fx, double* __restrict__ Fy,
-                                                   double* __restrict__ Fz, double* __restrict__ vp, double* __restrict__ blockmax,
-                                                   const StepConst sc, DevClock* clk) {
-  const bool active = (clk->t < sc.tmax) && (clk->nn < sc.nnmax);
-  if (!active) return;
-  const long long N = sc.N;
-  const long long c = (long long)blockIdx.x * BS_A + threadIdx.x;
+// Phase [A] runs as five kernels, one per-cell function each, so that every
+// kernel's code stays small (the fused cell_phase_A kernel was bound by
+// instruction fetch); the intermediate states go through buffers that are
+// dead during phase A:  M -A1-> Fx -A2-> Fy -A3-> Fz -A4-> Mtmp -A5-> M, with
+// the Jacobian speeds of A2-A4 parked in vp and combined in A5.
+__device__ __forceinline__ bool phase_A_active(const StepConst& sc, const DevClock* clk) {
+  return (clk->t < sc.tmax) && (clk->nn < sc.nnmax);
+}
+
+// A1: Flux_closure35_and_realizable_3D (realized moments only)
+__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure(const double* __restrict__ M, double* __restrict__ out, const StepConst sc,
+                                                              const DevClock* clk) {
+  if (!phase_A_active(sc, clk)) return;
+  const long long N = sc.N, c = (long long)blockIdx.x * BS_A + threadIdx.x;
+  if (c >= N) return;
+  double m[35], a[35];
+#pragma unroll
+  for (int n = 0; n < 35; ++n) m[n] = M[c + N * n];
+  flux_closure35(m, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, a);
+#pragma unroll
+  for (int n = 0; n < 35; ++n) out[c + N * n] = a[n];
+}
+
+// A2/A3: eigenvalues6_hyperbolic_3D along x (axis 1) or y (axis 2)
+__global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* __restrict__ in, double* __restrict__ out, double* __restrict__ vlo,
+                                                         double* __restrict__ vhi, int axis, const StepConst sc, const DevClock* clk) {
+  if (!phase_A_active(sc, clk)) return;
+  const long long N = sc.N, c = (long long)blockIdx.x * BS_A + threadIdx.x;
+  if (c >= N) return;
+  double m[35], r[35], lo, hi;
+#pragma unroll
+  for (int n = 0; n < 35; ++n) m[n] = in[c + N * n];
+  eigenvalues6(m, axis, sc.flag2D, sc.Ma, lo, hi, r);
+#pragma unroll
+  for (int n = 0; n < 35; ++n) out[c + N * n] = r[n];
+  vlo[c] = lo; vhi[c] = hi;
+}
+
+// A4: eigenvalues6z_hyperbolic_3D
+__global__ void __launch_bounds__(BS_A, MINB_EIG) k_A4_eigz(const double* __restrict__ in, double* __restrict__ out, double* __restrict__ vlo,
+                                                           double* __restrict__ vhi, const StepConst sc, const DevClock* clk) {
+  if (!phase_A_active(sc, clk)) return;
+  const long long N = sc.N, c = (long long)blockIdx.x * BS_A + threadIdx.x;
+  if (c >= N) return;
+  double m[35], r[35], lo, hi;
+#pragma unroll
+  for (int n = 0; n < 35; ++n) m[n] = in[c + N * n];
+  eigenvalues6z(m, sc.flag2D, sc.Ma, sc.positivity, lo, hi, r);
+#pragma unroll
+  for (int n = 0; n < 35; ++n) out[c + N * n] = r[n];
+  vlo[c] = lo; vhi[c] = hi;
+}
+
+// A5: closure of the realized moments with fluxes, 1-D closure speeds, the
+// six wave speeds and the NaN-propagating block max of |speed|
+__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A5_flux(const double* __restrict__ in, double* __restrict__ M, double* __restrict__ Fx,
+                                                           double* __restrict__ Fy, double* __restrict__ Fz, double* __restrict__ vp,
+                                                           double* __restrict__ blockmax, const StepConst sc, const DevClock* clk) {
+  if (!phase_A_active(sc, clk)) return;
+  const long long N = sc.N, c = (long long)blockIdx.x * BS_A + threadIdx.x;
   double local = 0.0;
   if (c < N) {
-    double m[35], fx[35], fy[35], fz[35], mr[35], v[6];
+    double m[35], fx[35], fy[35], fz[35], mr[35];
 #pragma unroll
-    for (int n = 0; n < 35; ++n) m[n] = M[c + N * n];
-    cell_phase_A(m, sc.flag2D, sc.Ma, sc.positivity, fx, fy, fz, mr, v);
+    for (int n = 0; n < 35; ++n) m[n] = in[c + N * n];
+    flux_closure35(m, sc.flag2D, sc.Ma, fx, fy, fz, mr);
 #pragma unroll
     for (int n = 0; n < 35; ++n) {
       Fx[c + N * n] = fx[n]; Fy[c + N * n] = fy[n]; Fz[c + N * n] = fz[n]; M[c + N * n] = mr[n];
     }
+    double v5[6];
+    closure_eigs(mr[0], mr[1], mr[2], mr[3], mr[4], v5[0], v5[1]);
+    closure_eigs(mr[0], mr[5], mr[9], mr[12], mr[14], v5[2], v5[3]);
+    closure_eigs(mr[0], mr[15], mr[19], mr[22], mr[24], v5[4], v5[5]);
 #pragma unroll
-    for (int q = 0; q < 6; ++q) { vp[c + N * q] = v[q]; local = nanmax(local, fabs(v[q])); }
+    for (int q = 0; q < 6; q += 2) {
+      const double lo = jmin(v5[q], vp[c + N * q]), hi = jmax(v5[q + 1], vp[c + N * (q + 1)]);
+      vp[c + N * q] = lo; vp[c + N * (q + 1)] = hi;
+      local = nanmax(local, fabs(lo));
+      local = nanmax(local, fabs(hi));
+    }
   }
   const double bm = block_nanmax<BS_A>(local);
   if (threadIdx.x == 0) blockmax[blockIdx.x] = bm;
@@ -67,9 +130,19 @@ __global__ void __launch_bounds__(BS_CELLS) k_cells_phase_A(const double* __rest
 
 }  // namespace
 
-void launch_phase_A(const StepConst& sc, double* M, double* Fx, double* Fy, double* Fz, double* vp, double* blockmax, DevClock* clk,
-                    cudaStream_t s) {
-  k_phase_A<<<sc.nblocksA, BS_A, 0, s>>>(M, Fx, Fy, Fz, vp, blockmax, sc, clk);
+void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, double* Fy, double* Fz, double* vp, double* blockmax,
+                    const DevClock* clk, cudaStream_t s, cudaEvent_t* ev) {
+  const long long N = sc.N;
+  k_A1_closure<<<sc.nblocksA, BS_A, 0, s>>>(M, Fx, sc, clk);
+  if (ev) cudaEventRecord(ev[0], s);
+  k_A_eig<<<sc.nblocksA, BS_A, 0, s>>>(Fx, Fy, vp, vp + N, 1, sc, clk);
+  if (ev) cudaEventRecord(ev[1], s);
+  k_A_eig<<<sc.nblocksA, BS_A, 0, s>>>(Fy, Fz, vp + 2 * N, vp + 3 * N, 2, sc, clk);
+  if (ev) cudaEventRecord(ev[2], s);
+  k_A4_eigz<<<sc.nblocksA, BS_A, 0, s>>>(Fz, Mtmp, vp + 4 * N, vp + 5 * N, sc, clk);
+  if (ev) cudaEventRecord(ev[3], s);
+  k_A5_flux<<<sc.nblocksA, BS_A, 0, s>>>(Mtmp, M, Fx, Fy, Fz, vp, blockmax, sc, clk);
+  if (ev) cudaEventRecord(ev[4], s);
 }
 void launch_cells_phase_A(const double* M, long long n, int flag2D, double Ma, int positivity, double* Fx, double* Fy, double* Fz,
                           double* Mr, double* vp, cudaStream_t s) {

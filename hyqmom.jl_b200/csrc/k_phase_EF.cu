@@ -8,34 +8,66 @@ using namespace hyq;
 namespace hyqk {
 namespace {
 
-__device__ __noinline__ void cell_phase_EF(double* m, int flag2D, double Ma, int positivity, double dt, double Kn) {
-  double a[35], b[35];
-  double v0, v1;
-  flux_closure35(m, flag2D, Ma, nullptr, nullptr, nullptr, a);
-  eigenvalues6(a, 1, flag2D, Ma, v0, v1, b);
-  eigenvalues6(b, 2, flag2D, Ma, v0, v1, a);
-  flux_closure35(a, flag2D, Ma, nullptr, nullptr, nullptr, m);
-  collision35(m, dt, Kn, positivity);
+
+// Phases [E]+[F] run as four kernels, one per-cell function each (small code
+// per kernel); intermediate states go through the flux buffers, dead after
+// the HLL sweep:  Mtmp -E1-> Fx -E2-> Fy -E3-> Fz -E4-> M.
+// E1: Flux_closure35_and_realizable_3D
+__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E1_closure(const double* __restrict__ in, double* __restrict__ out, const StepConst sc,
+                                                                const DevClock* clk) {
+  if (!clk->active) return;
+  const long long N = sc.N, c = (long long)blockIdx.x * BS_EF + threadIdx.x;
+  if (c >= N) return;
+  double m[35], a[35];
+#pragma unroll
+  for (int n = 0; n < 35; ++n) m[n] = in[c + N * n];
+  flux_closure35(m, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, a);
+#pragma unroll
+  for (int n = 0; n < 35; ++n) out[c + N * n] = a[n];
 }
 
-__global__ void __launch_bounds__(BS_EF) k_phase_EF(const double* __restrict__ Min, double* __restrict__ Mout, const StepConst sc,
-                                                     const DevClock* clk) {
+// E2/E3: eigenvalues6_hyperbolic_3D along x or y (corrected moments only)
+__global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* __restrict__ in, double* __restrict__ out, int axis, const StepConst sc,
+                                                           const DevClock* clk) {
   if (!clk->active) return;
-  const long long N = sc.N;
-  const long long c = (long long)blockIdx.x * BS_EF + threadIdx.x;
+  const long long N = sc.N, c = (long long)blockIdx.x * BS_EF + threadIdx.x;
   if (c >= N) return;
-  double m[35];
+  double m[35], r[35], v0, v1;
 #pragma unroll
-  for (int n = 0; n < 35; ++n) m[n] = Min[c + N * n];
-  cell_phase_EF(m, sc.flag2D, sc.Ma, sc.positivity, clk->dt, sc.Kn);
+  for (int n = 0; n < 35; ++n) m[n] = in[c + N * n];
+  eigenvalues6(m, axis, sc.flag2D, sc.Ma, v0, v1, r);
 #pragma unroll
-  for (int n = 0; n < 35; ++n) Mout[c + N * n] = m[n];
+  for (int n = 0; n < 35; ++n) out[c + N * n] = r[n];
+}
+
+// E4: Flux_closure35_and_realizable_3D, then collision35 with the step's dt
+__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E4_closure_bgk(const double* __restrict__ in, double* __restrict__ Mout, const StepConst sc,
+                                                                    const DevClock* clk) {
+  if (!clk->active) return;
+  const long long N = sc.N, c = (long long)blockIdx.x * BS_EF + threadIdx.x;
+  if (c >= N) return;
+  double m[35], a[35];
+#pragma unroll
+  for (int n = 0; n < 35; ++n) m[n] = in[c + N * n];
+  flux_closure35(m, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, a);
+  collision35(a, clk->dt, sc.Kn, sc.positivity);
+#pragma unroll
+  for (int n = 0; n < 35; ++n) Mout[c + N * n] = a[n];
 }
 
 }  // namespace
 
-void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, const DevClock* clk, cudaStream_t s) {
-  k_phase_EF<<<grid_of(sc.N, BS_EF), BS_EF, 0, s>>>(Min, Mout, sc, clk);
+void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, double* Fx, double* Fy, double* Fz, const DevClock* clk,
+                     cudaStream_t s, cudaEvent_t* ev) {
+  const int g = grid_of(sc.N, BS_EF);
+  k_E1_closure<<<g, BS_EF, 0, s>>>(Min, Fx, sc, clk);
+  if (ev) cudaEventRecord(ev[0], s);
+  k_E_eig<<<g, BS_EF, 0, s>>>(Fx, Fy, 1, sc, clk);
+  if (ev) cudaEventRecord(ev[1], s);
+  k_E_eig<<<g, BS_EF, 0, s>>>(Fy, Fz, 2, sc, clk);
+  if (ev) cudaEventRecord(ev[2], s);
+  k_E4_closure_bgk<<<g, BS_EF, 0, s>>>(Fz, Mout, sc, clk);
+  if (ev) cudaEventRecord(ev[3], s);
 }
 
 }  // namespace hyqk

@@ -88,10 +88,14 @@ int hyq_get_SC(hyq_ctx* ctx, double* S, double* C);
 /* cudaStream_t of the context, for callers that order their own work. */
 void* hyq_stream(hyq_ctx* ctx);
 
-/* Run `steps` steps launching the four step kernels individually (not the
- * graph) with CUDA events around each on the context stream; ms[4] receives
- * the summed device time of phase A, the CFL reduction, the HLL sweep and
- * phase E+F.  For profiling; results equal hyq_advance. */
+/* Run `steps` steps launching the step kernels individually (not the graph)
+ * with CUDA events around each on the context stream; ms[HYQ_TIMED_SLOTS]
+ * receives the summed device time of each kernel, in launch order:
+ * A1 closure, A2 x eigenvalues, A3 y eigenvalues, A4 z eigenvalues,
+ * A5 closure with fluxes and speeds, CFL reduction, HLL sweep,
+ * E1 closure, E2 x eigenvalues, E3 y eigenvalues, E4 closure + BGK.
+ * For profiling; results equal hyq_advance. */
+#define HYQ_TIMED_SLOTS 11
 int hyq_advance_timed(hyq_ctx* ctx, int64_t steps, float* ms);
 
 /* ---- allocation-free step ------------------------------------------------

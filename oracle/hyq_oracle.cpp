@@ -318,4 +318,45 @@ void hyqo_count_ops(int Nx, int Ny, int Nz, const double* M, double Kn, double M
   out[2] = (Nz > 1 ? 3.0 : 2.0) * 35.0 * 18.0 + 35.0 * 4.0;
 }
 
+// Per-kernel FP64 operation counts of the staged CUDA step, summed over cells:
+// out[0..4] = A1 closure, A2 x eigenvalues, A3 y eigenvalues, A4 z eigenvalues,
+// A5 closure with fluxes + 1-D closure speeds; out[5..8] = E1 closure,
+// E2 x eigenvalues, E3 y eigenvalues, E4 closure + BGK.  Same per-cell chain as
+// phase_A / phase_E + collision35.
+void hyqo_count_ops_stages(int Nx, int Ny, int Nz, const double* M, double Kn, double Ma, int flag2D, int positivity, double dt,
+                           double* out) {
+  const size_t N = size_t(Nx) * Ny * Nz;
+  unsigned long long c[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const Counted ma(Ma);
+  for (size_t q = 0; q < N; ++q) {
+    Counted m[35], a[35], b[35], fx[35], fy[35], fz[35], mr[35], v0, v1;
+    for (int n = 0; n < 35; ++n) m[n] = Counted(M[q + N * n]);
+    Counted::ops = 0; flux_closure35(m, flag2D, ma, fx, fy, fz, a); c[0] += Counted::ops;
+    Counted::ops = 0; eigenvalues6_hyperbolic_3D(a, 1, flag2D, ma, v0, v1, b); c[1] += Counted::ops;
+    Counted::ops = 0; eigenvalues6_hyperbolic_3D(b, 2, flag2D, ma, v0, v1, a); c[2] += Counted::ops;
+    Counted::ops = 0; eigenvalues6z_hyperbolic_3D(a, flag2D, ma, positivity != 0, v0, v1, b); c[3] += Counted::ops;
+    Counted::ops = 0;
+    flux_closure35(b, flag2D, ma, fx, fy, fz, mr);
+    {
+      Counted mx[5] = {mr[0], mr[1], mr[2], mr[3], mr[4]};
+      Counted my[5] = {mr[0], mr[5], mr[9], mr[12], mr[14]};
+      Counted mz[5] = {mr[0], mr[15], mr[19], mr[22], mr[24]};
+      Counted Mp, lo, hi;
+      closure_and_eigenvalues(mx, Mp, lo, hi);
+      closure_and_eigenvalues(my, Mp, lo, hi);
+      closure_and_eigenvalues(mz, Mp, lo, hi);
+    }
+    c[4] += Counted::ops;
+    // phases E + F on the realized state (the HLL update is not replayed here)
+    Counted::ops = 0; flux_closure35(mr, flag2D, ma, fx, fy, fz, a); c[5] += Counted::ops;
+    Counted::ops = 0; eigenvalues6_hyperbolic_3D(a, 1, flag2D, ma, v0, v1, b); c[6] += Counted::ops;
+    Counted::ops = 0; eigenvalues6_hyperbolic_3D(b, 2, flag2D, ma, v0, v1, a); c[7] += Counted::ops;
+    Counted::ops = 0;
+    flux_closure35(a, flag2D, ma, fx, fy, fz, b);
+    collision35<Counted>(b, Counted(dt), Counted(Kn), positivity != 0, mr);
+    c[8] += Counted::ops;
+  }
+  for (int k = 0; k < 9; ++k) out[k] = double(c[k]);
+}
+
 }  // extern "C"

@@ -649,7 +649,10 @@ template <class T> void closure_and_eigenvalues(const T (&mom)[5], T& Mp, T& vpm
   if (b[1] >= T(0) && b[2] >= T(0)) {
     using std::sqrt;
     T S3[3][3] = {{a[0], sqrt(b[1]), T(0)}, {sqrt(b[1]), a[1], sqrt(b[2])}, {T(0), sqrt(b[2]), a[2]}};
-    // symmetric eigenvalues by Jacobi rotation
+    // symmetric eigenvalues by cyclic Jacobi rotation; from the fourth sweep
+    // on, an off-diagonal entry too small to change either diagonal entry
+    // (|d| + 100|e| == |d|) is set to zero (Rutishauser's threshold rule), so
+    // the sweeps end after a few iterations instead of hunting round-off
     T A[3][3];
     for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) A[i][j] = S3[i][j];
     using std::fabs;
@@ -659,6 +662,13 @@ template <class T> void closure_and_eigenvalues(const T (&mom)[5], T& Mp, T& vpm
       for (int p = 0; p < 2; ++p)
         for (int q = p + 1; q < 3; ++q) {
           if (A[p][q] == T(0)) continue;
+          if (sweep >= 3) {
+            const T g = T(100) * fabs(A[p][q]);
+            if (fabs(A[p][p]) + g == fabs(A[p][p]) && fabs(A[q][q]) + g == fabs(A[q][q])) {
+              A[p][q] = T(0); A[q][p] = T(0);
+              continue;
+            }
+          }
           T theta = (A[q][q] - A[p][p]) / (T(2) * A[p][q]);
           T t = jsign(theta) / (fabs(theta) + sqrt(theta * theta + T(1)));
           if (theta == T(0)) t = T(1);

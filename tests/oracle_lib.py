@@ -165,6 +165,17 @@ def step(M, params, t):
     return dt, float(tt[0]), float(vm[0])
 
 
+def count_ops_stages(M, params, dt):
+    """Per-kernel FP64 op counts of the staged step, summed over cells (9)."""
+    M = np.asfortranarray(M, dtype=np.float64)
+    Nx, Ny, Nz, _ = M.shape
+    out = np.zeros(9)
+    p = params
+    load().hyqo_count_ops_stages(Nx, Ny, Nz, M.ctypes.data_as(_dp), ctypes.c_double(p["Kn"]), ctypes.c_double(p["Ma"]),
+                                 int(p["flag2D"]), int(p.get("positivity", True)), ctypes.c_double(dt), _p(out))
+    return out
+
+
 def count_ops(M, params, dt):
     M = np.asfortranarray(M, dtype=np.float64)
     Nx, Ny, Nz, _ = M.shape
