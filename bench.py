@@ -40,6 +40,11 @@ B_ALG = 2 * 35 * 8  # bytes per cell-step: state read once, written once
 # sweeps of 18 ops per moment plus the 4-op combination).
 KERNELS = ["A1_closure", "A2_eig_x", "A3_eig_y", "A4_eig_z", "A5_flux_speeds", "cfl", "hll",
            "E1_closure", "E2_eig_x", "E3_eig_y", "E4_closure_bgk"]
+# DRAM bytes (read + write) per cell of each kernel from one ncu capture of
+# the 96x96x48 case of the same workload (profiles/step_kernels_crossing96x96x48.md),
+# scaled to a launch by its cells: the local-memory traffic per cell does not
+# depend on the grid size.
+TRAFFIC_PER_CELL = {"A1_closure": 6968.0, "A2_eig_x": 3925.0, "A3_eig_y": 3925.0, "A5_flux_speeds": 9256.0}
 F_KERNEL = {"A1_closure": 7583.0, "A2_eig_x": 1696.2, "A3_eig_y": 1696.2, "A4_eig_z": 1708.2, "A5_flux_speeds": 9709.4,
             "cfl": 1.0, "hll": 2030.0, "E1_closure": 7583.0, "E2_eig_x": 1696.3, "E3_eig_y": 1696.3, "E4_closure_bgk": 8374.0}
 
@@ -253,7 +258,9 @@ def run_gpu(args, rank, world, local_rank):
     per_kernel = {k: {"ms": round(kern[k], 3), "tflops": round(F_KERNEL[k] * cells / (kern[k] * 1e-3) / 1e12, 3)}
                   for k in KERNELS if k not in ("cfl",)}
     step_tflops = F_ALG * cells / (ms / args.steps * 1e-3) / 1e12
-    roof = {"bound": "fp64", "achieved": ach, "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64, "traffic": None,
+    traffic = TRAFFIC_PER_CELL[dom] * cells if dom in TRAFFIC_PER_CELL else None
+    roof = {"bound": "fp64", "achieved": ach, "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64, "traffic": traffic,
+            "traffic_source": "ncu dram__bytes_read+write per cell on 96x96x48, scaled to this launch's cells",
             "peak_source": "measured in this run: FP64 DGEMM 8192^3 (cuBLAS via torch), best of 3",
             "dominant_kernel": "k_" + dom, "f_alg_per_cell": F_KERNEL[dom],
             "note": "built with -fmad=false: every counted op is one FP64 pipe instruction, so an FMA-free kernel tops out at peak/2",
