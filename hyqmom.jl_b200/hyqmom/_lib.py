@@ -37,7 +37,8 @@ _lib = None
 SYMBOLS = ["hyq_abi_version", "hyq_create", "hyq_destroy", "hyq_last_error", "hyq_set_state", "hyq_get_state",
            "hyq_set_state_device", "hyq_get_state_device", "hyq_set_clock", "hyq_advance", "hyq_advance_async",
            "hyq_synchronize", "hyq_stats_get", "hyq_advance_timed", "hyq_get_SC", "hyq_stream", "hyq_cells_flux_closure",
-           "hyq_cells_eigenvalues", "hyq_cells_closure_eigs", "hyq_cells_collision", "hyq_cells_phase_A", "hyq_step_noalloc"]
+           "hyq_cells_eigenvalues", "hyq_cells_closure_eigs", "hyq_cells_collision", "hyq_cells_phase_A", "hyq_step_noalloc", "hyq_batch_create", "hyq_batch_destroy", "hyq_batch_size",
+           "hyq_batch_member", "hyq_batch_stream", "hyq_batch_advance_async", "hyq_batch_advance"]
 NOALLOC_MAX_CELLS = 16384  # HYQ_NOALLOC_MAX_CELLS
 
 
@@ -74,6 +75,17 @@ def load(path=None):
     lib.hyq_cells_collision.argtypes = [vp, i64, dbl, dbl, i32, vp, vp]
     lib.hyq_cells_phase_A.argtypes = [vp, i64, i32, dbl, i32, vp, vp, vp, vp, vp, vp]
     lib.hyq_step_noalloc.argtypes = [ctypes.POINTER(HyqParams), vp, ctypes.POINTER(HyqStats), vp]
+    lib.hyq_batch_create.argtypes = [ctypes.POINTER(HyqParams), i32, ctypes.POINTER(vp)]
+    lib.hyq_batch_destroy.argtypes = [vp]
+    lib.hyq_batch_destroy.restype = None
+    lib.hyq_batch_size.argtypes = [vp]
+    lib.hyq_batch_size.restype = i32
+    lib.hyq_batch_member.argtypes = [vp, i32]
+    lib.hyq_batch_member.restype = vp
+    lib.hyq_batch_stream.argtypes = [vp]
+    lib.hyq_batch_stream.restype = vp
+    lib.hyq_batch_advance_async.argtypes = [vp, i64]
+    lib.hyq_batch_advance.argtypes = [vp, i64, ctypes.POINTER(i32), ctypes.POINTER(i32)]
     _lib = lib
     return lib
 

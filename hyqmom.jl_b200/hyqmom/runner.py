@@ -17,27 +17,37 @@ from . import ic as _ic
 from .snapshots import SnapshotWriter
 
 
+def params_struct(p, device=0):
+    """hyq_params of a reference-style parameter dict."""
+    xmin, xmax, ymin, ymax, zmin, zmax = _ic.extents(p)
+    return _lib.HyqParams(Nx=p["Nx"], Ny=p["Ny"], Nz=p["Nz"], flag2D=int(p["flag2D"]),
+                          positivity=int(bool(p.get("positivity", True))), device=device, nnmax=int(p["nnmax"]),
+                          tmax=float(p["tmax"]), Kn=float(p["Kn"]), Ma=float(p["Ma"]), CFL=float(p["CFL"]),
+                          dtmax=float(p["dtmax"]), xmin=xmin, xmax=xmax, ymin=ymin, ymax=ymax, zmin=zmin, zmax=zmax)
+
+
 class Solver:
     """One simulation domain on one GPU (a hyq_ctx)."""
 
-    def __init__(self, params, device=0):
+    def __init__(self, params, device=0, _handle=None):
         lib = _lib.load()
         p = params
-        xmin, xmax, ymin, ymax, zmin, zmax = _ic.extents(p)
-        hp = _lib.HyqParams(Nx=p["Nx"], Ny=p["Ny"], Nz=p["Nz"], flag2D=int(p["flag2D"]),
-                            positivity=int(bool(p.get("positivity", True))), device=device, nnmax=int(p["nnmax"]),
-                            tmax=float(p["tmax"]), Kn=float(p["Kn"]), Ma=float(p["Ma"]), CFL=float(p["CFL"]),
-                            dtmax=float(p["dtmax"]), xmin=xmin, xmax=xmax, ymin=ymin, ymax=ymax, zmin=zmin, zmax=zmax)
-        h = ctypes.c_void_p()
-        rc = lib.hyq_create(ctypes.byref(hp), ctypes.byref(h))
-        if rc != 0:
-            raise _lib.HyqError(f"{_lib.ERRORS.get(rc, rc)}: {lib.hyq_last_error(None).decode()}")
+        self._owns = _handle is None
+        if _handle is None:
+            hp = params_struct(p, device)
+            h = ctypes.c_void_p()
+            rc = lib.hyq_create(ctypes.byref(hp), ctypes.byref(h))
+            if rc != 0:
+                raise _lib.HyqError(f"{_lib.ERRORS.get(rc, rc)}: {lib.hyq_last_error(None).decode()}")
+        else:
+            h = ctypes.c_void_p(_handle)
         self._lib, self._h, self.params = lib, h, dict(p)
         self.shape = (p["Nx"], p["Ny"], p["Nz"], 35)
 
     def close(self):
         if self._h:
-            self._lib.hyq_destroy(self._h)
+            if self._owns:
+                self._lib.hyq_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -98,6 +108,56 @@ class Solver:
     @property
     def stream(self):
         return self._lib.hyq_stream(self._h)
+
+
+class BatchSolver:
+    """Independent domains stepped together (a hyq_batch): one CUDA graph
+    replay advances every member that is not done by one step of its own dt.
+    ``members[i]`` is a Solver view of member i (state, clock, stats)."""
+
+    def __init__(self, params_list, device=0):
+        lib = _lib.load()
+        n = len(params_list)
+        arr = (_lib.HyqParams * n)(*[params_struct(p, device) for p in params_list])
+        h = ctypes.c_void_p()
+        rc = lib.hyq_batch_create(arr, n, ctypes.byref(h))
+        if rc != 0:
+            raise _lib.HyqError(f"{_lib.ERRORS.get(rc, rc)}: {lib.hyq_last_error(None).decode()}")
+        self._lib, self._h = lib, h
+        self.members = [Solver(p, device, _handle=lib.hyq_batch_member(h, i)) for i, p in enumerate(params_list)]
+
+    def close(self):
+        if self._h:
+            for m in self.members:
+                m.close()
+            self._lib.hyq_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.members)
+
+    def _chk(self, rc):
+        if rc != 0:
+            raise _lib.HyqError(f"{_lib.ERRORS.get(rc, rc)}: {self._lib.hyq_last_error(None).decode()}")
+
+    def advance(self, max_steps):
+        """Returns (members done, members stopped by a non-finite wave speed)."""
+        nd, nf = ctypes.c_int32(), ctypes.c_int32()
+        self._chk(self._lib.hyq_batch_advance(self._h, int(max_steps), ctypes.byref(nd), ctypes.byref(nf)))
+        return nd.value, nf.value
+
+    def advance_async(self, max_steps):
+        self._chk(self._lib.hyq_batch_advance_async(self._h, int(max_steps)))
+
+    @property
+    def stream(self):
+        return self._lib.hyq_batch_stream(self._h)
 
 
 def _runner_params(params):

@@ -98,6 +98,29 @@ void* hyq_stream(hyq_ctx* ctx);
 #define HYQ_TIMED_SLOTS 11
 int hyq_advance_timed(hyq_ctx* ctx, int64_t steps, float* ms);
 
+/* ---- batched independent domains ------------------------------------------
+ * The reference runs one simulation per simulation_runner call; a sweep of
+ * many small domains (uneven grids, each with its own Ma, Kn, CFL, tmax,
+ * nnmax and dt) leaves most of a B200 idle when run one at a time.  A batch
+ * owns one ordinary context per member (hyq_batch_member returns it, for
+ * hyq_set_state / hyq_get_state / hyq_stats_get) and one CUDA graph holding
+ * every member's step as an independent branch: each replay advances every
+ * member that is not done by one step, all members' kernels in flight
+ * together.  Members stop on the device at their own tmax / nnmax or at a
+ * non-finite wave speed (their stats status > 0); that is not an error of
+ * the batch call.  Batch calls report failures through hyq_last_error(NULL). */
+typedef struct hyq_batch hyq_batch;
+int hyq_batch_create(const hyq_params* p, int32_t n, hyq_batch** out);  /* p[n], one device */
+void hyq_batch_destroy(hyq_batch* b);
+int32_t hyq_batch_size(const hyq_batch* b);
+hyq_ctx* hyq_batch_member(hyq_batch* b, int32_t i);  /* NULL when out of range */
+void* hyq_batch_stream(hyq_batch* b);                /* cudaStream_t of the replays */
+/* Queue max_steps replays (after waiting for the members' own streams). */
+int hyq_batch_advance_async(hyq_batch* b, int64_t max_steps);
+/* Same, then wait; ndone / nfailed (may be NULL) count members that are done
+ * and members that met a non-finite wave speed. */
+int hyq_batch_advance(hyq_batch* b, int64_t max_steps, int32_t* ndone, int32_t* nfailed);
+
 /* ---- allocation-free step ------------------------------------------------
  * No counterpart in the reference (its Julia loop allocates freely); added
  * for callers that must not allocate device memory while they step: a host
