@@ -334,6 +334,27 @@ HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
   return 0;
 }
 
+}  // namespace hyq
+#include "hyq_eig6.cuh"
+namespace hyq {
+
+// eig_real<6> of a flux Jacobian: the register-resident path (hyq_eig6.cuh)
+// when dgebal's search makes one of the two permutations it handles, else
+// the general code; identical results either way.
+HQD void eig_real_jac(double (&J)[6][6], double (&wr)[6], double (&wi)[6]) {
+  double h[36];
+#pragma unroll
+  for (int r = 0; r < 6; ++r)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) h[r * 6 + c] = J[r][c];
+  const int pat = e6::pattern(h);
+  if (pat < 0) { eig_real<6>(J, wr, wi); return; }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) { wr[i] = 0.0; wi[i] = 0.0; }
+  if (pat == 1) { e6::apply_pattern1(h); e6::solve<2>(h, wr, wi); }
+  else e6::solve<0>(h, wr, wi);
+}
+
 // compute_jacobian_eigenvalues for one 15-moment slice: extreme real parts
 // and max |imag|.  A non-finite Jacobian gives NaN (the reference's guard).
 struct EigOut { double vmin, vmax, imax; };
@@ -355,7 +376,7 @@ HQN EigOut jac_eigs(const double* ma) {
   EigOut o;
   if (!fin) { o.vmin = qnan(); o.vmax = qnan(); o.imax = qnan(); return o; }
   double wr[6], wi[6];
-  eig_real<6>(J, wr, wi);
+  eig_real_jac(J, wr, wi);
   // sort(real) with NaN last, first and last
   double mn = wr[0], mx = wr[0];
   bool anynan = (wr[0] != wr[0]);

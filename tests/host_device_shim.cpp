@@ -19,4 +19,17 @@ void sh_eig(const double* m, int axis, int flag2D, double Ma, int pos, double* v
 }
 void sh_closure(const double* mom, double* v) { closure_eigs(mom[0], mom[1], mom[2], mom[3], mom[4], v[0], v[1]); }
 void sh_coll(double* m, double dt, double Kn, int pos) { collision35(m, dt, Kn, pos); }
+// eig_real<6> and the register-resident flux-Jacobian path on the same
+// matrix: out[0..11] = general (wr, wi), out[12..23] = fast path, out[24] =
+// the permutation pattern the fast path recognised (-1: none, general code).
+void sh_eig6_both(const double* A, double* out) {
+  double J[6][6], K[6][6], h[36];
+  for (int i = 0; i < 6; ++i) for (int j = 0; j < 6; ++j) { J[i][j] = K[i][j] = A[i * 6 + j]; h[i * 6 + j] = A[i * 6 + j]; }
+  double wr[6], wi[6];
+  eig_real<6>(J, wr, wi);
+  for (int i = 0; i < 6; ++i) { out[i] = wr[i]; out[6 + i] = wi[i]; }
+  eig_real_jac(K, wr, wi);
+  for (int i = 0; i < 6; ++i) { out[12 + i] = wr[i]; out[18 + i] = wi[i]; }
+  out[24] = e6::pattern(h);
+}
 }

@@ -62,3 +62,40 @@ def test_per_cell_functions_bitwise(shim, states):
         mm = m.copy()
         shim.sh_coll(P(mm), ctypes.c_double(3e-3), ctypes.c_double(1.0), 1)
         assert np.array_equal(mm, ol.collision35(m, 3e-3, 1.0), equal_nan=True)
+
+
+def jacobians(states, seed=5):
+    """Flux Jacobians of every x and y slice of the evolved states, plus
+    perturbed copies (random entries zeroed, scaled, made NaN)."""
+    SL = [[0, 5, 9, 12, 14, 1, 6, 10, 13, 2, 7, 11, 3, 8, 4], list(range(15)),
+          [0, 15, 19, 22, 24, 1, 16, 20, 23, 2, 17, 21, 3, 18, 4]]
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in states:
+        for sl in SL:
+            out.append(ol.vec_fn("hyqo_jacobian6", m[sl], 36))
+    base = np.array(out)
+    extra = []
+    for J in base[rng.choice(len(base), 400, replace=False)]:
+        K = J.copy()
+        K[rng.integers(0, 36, size=rng.integers(1, 6))] = 0.0
+        extra.append(K)
+        extra.append(J * 10.0 ** rng.uniform(-150, 150))
+        K = J.copy()
+        K[rng.integers(0, 36)] = np.nan
+        extra.append(K)
+    extra.append(np.zeros(36))
+    extra.append(np.eye(6).ravel())
+    return np.concatenate([base, np.array(extra)])
+
+
+def test_fast_eigen_path_is_bitwise_general(shim, states):
+    """The register-resident path for the permutations dgebal finds on flux
+    Jacobians gives the general eig_real<6> results bit for bit."""
+    seen = {-1: 0, 0: 0, 1: 0}
+    out = np.zeros(25)
+    for A in jacobians(states):
+        shim.sh_eig6_both(P(np.ascontiguousarray(A)), P(out))
+        seen[int(out[24])] += 1
+        assert np.array_equal(out[:12], out[12:24], equal_nan=True), (A, out)
+    assert seen[1] > 100 and seen[0] > 0, seen
