@@ -177,6 +177,22 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def max_over_ranks(ms, dist=None, device="cpu"):
+    """The slowest rank's time (every rank gets it); ms itself with one rank."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, cells, steps, ms):
+    """Whole-job cell-steps/s of `world` replicas that each advanced `cells`
+    cells by `steps` steps in `ms` (the max over ranks)."""
+    return world * cells * steps / (ms * 1e-3)
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     torch.cuda.set_device(local_rank)
@@ -211,11 +227,8 @@ def run_gpu(args, rank, world, local_rank):
     ms = e0.elapsed_time(e1)
     st = s.stats()
     assert st["status"] == 0 and st["nn"] == args.warmup + args.steps, f"steps did not all run: {st}"
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * cells * args.steps / (ms * 1e-3)
+    ms = max_over_ranks(ms, dist, "cuda")
+    value = replica_throughput(world, cells, args.steps, ms)
 
     # per-kernel device time (individual launches, same stream)
     s.set_state(M0)
