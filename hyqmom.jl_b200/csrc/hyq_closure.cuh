@@ -135,9 +135,26 @@ HQN int realizable_3D(double* s) {
 
   // 2x2 minors of the six permutations
   double S220a = s[s220], S220b = s[s220], S202a = s[s202], S202b = s[s202], S022a = s[s022], S022b = s[s022];
+  // Of the six projections only their 2x2 and 3x3 leading minors and the
+  // leading 3x3 entries of permutations 0, 2, 5 are used below, so those are
+  // kept instead of the six Delta structs (a smaller per-thread frame; the
+  // values are the same).
   double d2[6], d3[6];
-  Delta P[6];
-  for (int p = 0; p < 6; ++p) { delta2star_p(s, p, P[p]); d2[p] = lead_det(P[p], 2); }
+  double Ee[3][6];  // (0,0),(0,1),(0,2),(1,1),(1,2),(2,2) of projections 0, 2, 5
+  auto keep = [&](int p, const Delta& Dp) {
+    d3[p] = lead_det(Dp, 3);
+    const int slot = (p == 0) ? 0 : (p == 2) ? 1 : (p == 5) ? 2 : -1;
+    if (slot >= 0) {
+      Ee[slot][0] = E_(Dp, 0, 0); Ee[slot][1] = E_(Dp, 0, 1); Ee[slot][2] = E_(Dp, 0, 2);
+      Ee[slot][3] = E_(Dp, 1, 1); Ee[slot][4] = E_(Dp, 1, 2); Ee[slot][5] = E_(Dp, 2, 2);
+    }
+  };
+  for (int p = 0; p < 6; ++p) {
+    Delta Dp;
+    delta2star_p(s, p, Dp);
+    d2[p] = lead_det(Dp, 2);
+    keep(p, Dp);
+  }
   int flag310 = 0;
   if (!fE11 && !fE44 && d2[0] < h2min) {
     s[s310] = realizability_S310(s[s110], s[s101], s[s011], s[s300], s[s210], s[s120], s[s201], s[s111], s[s310], s[s220], H200, beta);
@@ -175,9 +192,11 @@ HQN int realizable_3D(double* s) {
   if (flag310) {
     double dm = 0.0;
     for (int p = 0; p < 6; ++p) {
-      delta2star_p(s, p, P[p]);
-      const double d = lead_det(P[p], 2);
+      Delta Dp;
+      delta2star_p(s, p, Dp);
+      const double d = lead_det(Dp, 2);
       dm = (p == 0) ? d : jmin(dm, d);
+      keep(p, Dp);
     }
     if (dm < 0.0) flag220 = 1;
   }
@@ -188,9 +207,8 @@ HQN int realizable_3D(double* s) {
   S022b = s[s022];
   double S022c = s[s022];
   if (!fE11 && !fE22 && !fE33 && !fE55) {
-    d3[0] = lead_det(P[0], 3); d3[1] = lead_det(P[1], 3);
     if (d3[0] <= h2min || d3[1] <= h2min) {
-      const double e11 = E_(P[0], 0, 0), e12 = E_(P[0], 0, 1), e13 = E_(P[0], 0, 2), e22 = E_(P[0], 1, 1), e23 = E_(P[0], 1, 2), e33 = E_(P[0], 2, 2);
+      const double e11 = Ee[0][0], e12 = Ee[0][1], e13 = Ee[0][2], e22 = Ee[0][3], e23 = Ee[0][4], e33 = Ee[0][5];
       const double d23 = s[s211] - e23, d22 = s[s220] - e22, d33 = s[s202] - e33;
       if (e11 > diagmin) { S220a = d22 + e13 * e13 / e11; S202a = d33 + e12 * e12 / e11; }
       s[s211] = realizability_S211(e11, e22, e33, e12, e13, d23, s[s211], beta);
@@ -198,9 +216,8 @@ HQN int realizable_3D(double* s) {
     }
   }
   if (!fE22 && !fE33 && !fE44 && !fE55) {
-    d3[2] = lead_det(P[2], 3); d3[4] = lead_det(P[4], 3);
     if (d3[2] < h2min || d3[4] < h2min) {
-      const double e11 = E_(P[2], 0, 0), e12 = E_(P[2], 0, 1), e13 = E_(P[2], 0, 2), e22 = E_(P[2], 1, 1), e23 = E_(P[2], 1, 2), e33 = E_(P[2], 2, 2);
+      const double e11 = Ee[1][0], e12 = Ee[1][1], e13 = Ee[1][2], e22 = Ee[1][3], e23 = Ee[1][4], e33 = Ee[1][5];
       const double d23 = s[s121] - e23, d22 = s[s220] - e22, d33 = s[s022] - e33;
       if (e11 > diagmin) { S220b = d22 + e13 * e13 / e11; S022b = d33 + e12 * e12 / e11; }
       s[s121] = realizability_S211(e11, e22, e33, e12, e13, d23, s[s121], beta);
@@ -208,9 +225,8 @@ HQN int realizable_3D(double* s) {
     }
   }
   if (!fE22 && !fE33 && !fE55 && !fE66) {
-    d3[3] = lead_det(P[3], 3); d3[5] = lead_det(P[5], 3);
     if (d3[3] < h2min || d3[5] < h2min) {
-      const double e11 = E_(P[5], 0, 0), e12 = E_(P[5], 0, 1), e13 = E_(P[5], 0, 2), e22 = E_(P[5], 1, 1), e23 = E_(P[5], 1, 2), e33 = E_(P[5], 2, 2);
+      const double e11 = Ee[2][0], e12 = Ee[2][1], e13 = Ee[2][2], e22 = Ee[2][3], e23 = Ee[2][4], e33 = Ee[2][5];
       const double d23 = s[s112] - e23, d22 = s[s022] - e22, d33 = s[s202] - e33;
       if (e11 > diagmin) { S202c = d22 + e13 * e13 / e11; S022c = d33 + e12 * e12 / e11; }
       s[s112] = realizability_S211(e11, e22, e33, e12, e13, d23, s[s112], beta);
