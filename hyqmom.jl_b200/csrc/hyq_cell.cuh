@@ -147,6 +147,30 @@ HQN void shift_axis(double* A, int n, int axis, double sh) {
   }
 }
 
+// shift_axis with the store size and axis fixed at compile time and every
+// loop unrolled, so that a store held in a local array of the caller can stay
+// in registers; same operations in the same order as shift_axis.
+template <int N, int AXIS> HQD void shift_axis_r(double (&A)[N], double sh) {
+  double pw[6];
+  pw[0] = 1.0;
+#pragma unroll
+  for (int q = 1; q < 6; ++q) pw[q] = pw[q - 1] * sh;
+  const unsigned char* L = (N == 35) ? (AXIS == 0 ? T_L35X : AXIS == 1 ? T_L35Y : T_L35Z) : (AXIS == 0 ? T_L56X : AXIS == 1 ? T_L56Y : T_L56Z);
+  constexpr int stride = AXIS == 0 ? 36 : AXIS == 1 ? 6 : 1;
+#pragma unroll
+  for (int t = 0; t < N; ++t) {
+    const int q = L[t];
+    const int e = AXIS == 0 ? T_EX56I[q] : AXIS == 1 ? T_EX56J[q] : T_EX56K[q];
+    if (e == 0) continue;
+    const int base = T_EX56I[q] * 36 + T_EX56J[q] * 6 + T_EX56K[q] - e * stride;
+    double acc = 0.0;
+#pragma unroll
+    for (int a = 0; a <= 5; ++a)
+      if (a <= e) acc = acc + (double(T_BIN[e * 7 + a]) * pw[e - a]) * A[T_IDX56[base + a * stride]];
+    A[q] = acc;
+  }
+}
+
 // Central moments C (35-order, C000=1, first order 0) of raw M
 // (M4toC4_3D, src/autogen/M4toC4_3D.jl:42-55).
 HQD void raw_to_central(const double* M, double* C) {
@@ -167,6 +191,25 @@ HQD void central_to_raw(double M000, double u, double v, double w, double* A, in
   shift_axis(A, n, 1, v);
   shift_axis(A, n, 2, w);
   for (int q = 0; q < n; ++q) A[q] = M000 * A[q];
+}
+
+// raw_to_central / central_to_raw on caller-held arrays (register path).
+HQD void raw_to_central_r(const double* M, double (&C)[35]) {
+  const double inv = 1.0 / M[0];
+  const double u = M[1] * inv, v = M[5] * inv, w = M[15] * inv;
+#pragma unroll
+  for (int n = 0; n < 35; ++n) C[n] = M[n] * inv;
+  shift_axis_r<35, 0>(C, -u);
+  shift_axis_r<35, 1>(C, -v);
+  shift_axis_r<35, 2>(C, -w);
+  C[0] = 1.0; C[1] = 0.0; C[5] = 0.0; C[15] = 0.0;
+}
+template <int N> HQD void central_to_raw_r(double M000, double u, double v, double w, double (&A)[N]) {
+  shift_axis_r<N, 0>(A, u);
+  shift_axis_r<N, 1>(A, v);
+  shift_axis_r<N, 2>(A, w);
+#pragma unroll
+  for (int q = 0; q < N; ++q) A[q] = M000 * A[q];
 }
 
 // Standardized moments S (35-order) from central C (M2CS4_35,

@@ -399,7 +399,7 @@ HQN void flux_closure35(const double* M4, int flag2D, double Ma, double* Fx, dou
   const double M000 = M4[0];
   const double u = M4[1] / M000, v = M4[5] / M000, w = M4[15] / M000;
   double C[35], S[35];
-  raw_to_central(M4, C);
+  raw_to_central_r(M4, C);
   central_to_std(C, S);
   const double C200 = jmax(EPS, C[2]), C020 = jmax(EPS, C[9]), C002 = jmax(EPS, C[19]);
   double s[NS];
@@ -447,6 +447,7 @@ HQN void flux_closure35(const double* M4, int flag2D, double Ma, double* Fx, dou
   px[4] = pow4(sx); py[4] = pow4(sy); pz[4] = pow4(sz);
   px[5] = pow5(sx); py[5] = pow5(sy); pz[5] = pow5(sz);
   double A[56];
+#pragma unroll
   for (int q = 0; q < 56; ++q) {
     const int i = T_EX56I[q], j = T_EX56J[q], k = T_EX56K[q];
     const int o = i + j + k;
@@ -465,7 +466,8 @@ HQN void flux_closure35(const double* M4, int flag2D, double Ma, double* Fx, dou
     }
     A[q] = val;
   }
-  central_to_raw(M000, u, v, w, A, 56);
+  central_to_raw_r<56>(M000, u, v, w, A);
+#pragma unroll
   for (int n = 0; n < 35; ++n) {
     Mr[n] = A[n];
     if (Fx) Fx[n] = A[T_FX[n]];
