@@ -17,7 +17,7 @@ namespace hyq {
 // The body is the closed form d(m32,m23,m14)/dC chained with dC/dW, derived
 // symbolically from the 2-D HyQMOM closure by codegen/gen_jacobian6.py; the
 // CPU oracle includes the same generated body.
-HQN void jacobian6_rows(const double* m, double* r3, double* r5, double* r6) {
+HQD void jacobian6_rows(const double* m, double* r3, double* r5, double* r6) {
   typedef double R;
 #include "gen_jacobian6.inc"
 }
@@ -341,14 +341,17 @@ namespace hyq {
 // eig_real<6> of a flux Jacobian: the register-resident path (hyq_eig6.cuh)
 // when dgebal's search makes one of the two permutations it handles, else
 // the general code; identical results either way.
-HQD void eig_real_jac(double (&J)[6][6], double (&wr)[6], double (&wi)[6]) {
-  double h[36];
-#pragma unroll
-  for (int r = 0; r < 6; ++r)
-#pragma unroll
-    for (int c = 0; c < 6; ++c) h[r * 6 + c] = J[r][c];
+HQD void eig_real_jac(double (&h)[36], double (&wr)[6], double (&wi)[6]) {
   const int pat = e6::pattern(h);
-  if (pat < 0) { eig_real<6>(J, wr, wi); return; }
+  if (pat < 0) {
+    double J[6][6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) J[r][c] = h[r * 6 + c];
+    eig_real<6>(J, wr, wi);
+    return;
+  }
 #pragma unroll
   for (int i = 0; i < 6; ++i) { wr[i] = 0.0; wi[i] = 0.0; }
   if (pat == 1) { e6::apply_pattern1(h); e6::solve<2>(h, wr, wi); }
@@ -361,25 +364,24 @@ struct EigOut { double vmin, vmax, imax; };
 HQN EigOut jac_eigs(const double* ma) {
   double r3[6], r5[6], r6[6];
   jacobian6_rows(ma, r3, r5, r6);
-  double J[6][6];
+  double h[36];  // the Jacobian, row-major, held in registers
 #pragma unroll
-  for (int i = 0; i < 6; ++i)
-#pragma unroll
-    for (int j = 0; j < 6; ++j) J[i][j] = 0.0;
-  J[0][1] = 1.0; J[1][2] = 1.0; J[3][4] = 1.0;
+  for (int i = 0; i < 36; ++i) h[i] = 0.0;
+  h[0 * 6 + 1] = 1.0; h[1 * 6 + 2] = 1.0; h[3 * 6 + 4] = 1.0;
   bool fin = true;
 #pragma unroll
   for (int j = 0; j < 6; ++j) {
-    J[2][j] = r3[j]; J[4][j] = r5[j]; J[5][j] = r6[j];
+    h[2 * 6 + j] = r3[j]; h[4 * 6 + j] = r5[j]; h[5 * 6 + j] = r6[j];
     fin = fin && isfinite(r3[j]) && isfinite(r5[j]) && isfinite(r6[j]);
   }
   EigOut o;
   if (!fin) { o.vmin = qnan(); o.vmax = qnan(); o.imax = qnan(); return o; }
   double wr[6], wi[6];
-  eig_real_jac(J, wr, wi);
+  eig_real_jac(h, wr, wi);
   // sort(real) with NaN last, first and last
   double mn = wr[0], mx = wr[0];
   bool anynan = (wr[0] != wr[0]);
+#pragma unroll
   for (int q = 1; q < 6; ++q) {
     if (wr[q] != wr[q]) { anynan = true; continue; }
     if (mn != mn || wr[q] < mn) mn = wr[q];
@@ -388,6 +390,7 @@ HQN EigOut jac_eigs(const double* ma) {
   o.vmin = mn;
   o.vmax = anynan ? qnan() : mx;
   double im = fabs(wi[0]);
+#pragma unroll
   for (int q = 1; q < 6; ++q) im = jmax(im, fabs(wi[q]));
   o.imax = im;
   return o;

@@ -28,8 +28,10 @@ void sh_eig6_both(const double* A, double* out) {
   double wr[6], wi[6];
   eig_real<6>(J, wr, wi);
   for (int i = 0; i < 6; ++i) { out[i] = wr[i]; out[6 + i] = wi[i]; }
-  eig_real_jac(K, wr, wi);
+  eig_real_jac(h, wr, wi);
   for (int i = 0; i < 6; ++i) { out[12 + i] = wr[i]; out[18 + i] = wi[i]; }
-  out[24] = e6::pattern(h);
+  double h2[36];
+  for (int i = 0; i < 36; ++i) h2[i] = A[i];
+  out[24] = e6::pattern(h2);
 }
 }
