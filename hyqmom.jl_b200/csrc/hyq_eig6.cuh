@@ -20,6 +20,10 @@ __host__ __device__ constexpr int IX(int r, int c) { return (r < 0 || c < 0 || r
 
 // nrm2 / dlarfg of eig_real with a compile-time length (same operation order)
 template <int n> HQD double nrm2_s(const double* x) {
+  double sq = 0.0;
+#pragma unroll
+  for (int i = 0; i < n; ++i) sq = sq + x[i] * x[i];
+  if (sq >= 1e-280 && sq <= 1.7976931348623157e308) return sqrt(sq);
   double scale = 0.0, ssq = 1.0;
 #pragma unroll
   for (int i = 0; i < n; ++i) {

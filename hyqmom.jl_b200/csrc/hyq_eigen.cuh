@@ -37,7 +37,13 @@ HQD double dlapy2(double x, double y) {
   const double r = z / w;
   return w * sqrt(1.0 + r * r);
 }
+// Euclidean norm: the plain sum of squares and its square root (as
+// OpenBLAS computes it), with the scaled LAPACK dnrm2 recurrence when that
+// sum would lose range (over- or underflow, NaN).
 HQD double nrm2(const double* x, int n, int inc) {
+  double sq = 0.0;
+  for (int i = 0; i < n; ++i) sq = sq + x[i * inc] * x[i * inc];
+  if (sq >= 1e-280 && sq <= 1.7976931348623157e308) return sqrt(sq);
   double scale = 0.0, ssq = 1.0;
   for (int i = 0; i < n; ++i) {
     const double xi = x[i * inc];

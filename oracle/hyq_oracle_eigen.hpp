@@ -139,8 +139,15 @@ template <class T> T dlapy2(T x, T y) {
   T r = z / w;
   return w * sqrt(T(1) + r * r);
 }
+// Euclidean norm.  OpenBLAS (Julia's BLAS) forms the plain sum of squares
+// and its square root; this does the same in FP64 and falls back to the
+// scaled LAPACK dnrm2 recurrence when that sum would lose range (over- or
+// underflow, NaN).
 template <class T> T nrm2(const T* x, int n, int inc) {
   using std::fabs; using std::sqrt;
+  T sq = T(0);
+  for (int i = 0; i < n; ++i) sq = sq + x[i * inc] * x[i * inc];
+  if (sq >= T(1e-280) && sq <= T(1.7976931348623157e308)) return sqrt(sq);
   T scale = T(0), ssq = T(1);
   for (int i = 0; i < n; ++i) {
     T xi = x[i * inc];
