@@ -194,11 +194,12 @@ HQD void central_to_raw(double M000, double u, double v, double w, double* A, in
 }
 
 // raw_to_central / central_to_raw on caller-held arrays (register path).
-HQD void raw_to_central_r(const double* M, double (&C)[35]) {
+// (M[n * st]: the moments may be read straight from a moment-major field)
+HQD void raw_to_central_r(const double* M, long long st, double (&C)[35]) {
   const double inv = 1.0 / M[0];
-  const double u = M[1] * inv, v = M[5] * inv, w = M[15] * inv;
+  const double u = M[1 * st] * inv, v = M[5 * st] * inv, w = M[15 * st] * inv;
 #pragma unroll
-  for (int n = 0; n < 35; ++n) C[n] = M[n] * inv;
+  for (int n = 0; n < 35; ++n) C[n] = M[n * st] * inv;
   shift_axis_r<35, 0>(C, -u);
   shift_axis_r<35, 1>(C, -v);
   shift_axis_r<35, 2>(C, -w);

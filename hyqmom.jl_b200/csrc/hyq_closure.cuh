@@ -392,14 +392,18 @@ HQD int s28_of(int i, int j, int k) { return T_S28[i * 36 + j * 6 + k]; }
 HQD int f5_of(int i, int j, int k) { return T_F5[i * 36 + j * 6 + k]; }
 
 // Flux_closure35_and_realizable_3D: fluxes F (x,y,z) of order-4 moments and the
-// realizable moments Mr.  Any of Fx/Fy/Fz may be null (not needed).
-HQN void flux_closure35(const double* M4, int flag2D, double Ma, double* Fx, double* Fy, double* Fz, double* Mr) {
+// realizable moments Mr.  Any of Fx/Fy/Fz may be null (not needed).  Moment n
+// is read from M4[n * ist] and written to Mr[n * mst], Fx[n * fst], ...: the
+// step kernels pass the cell's entry of the moment-major fields (stride N)
+// so that nothing is staged through per-thread arrays.
+HQN void flux_closure35(const double* M4, int flag2D, double Ma, double* Fx, double* Fy, double* Fz, double* Mr, long long ist = 1,
+                        long long mst = 1, long long fst = 1) {
   const double s3max = 4.0 + fabs(Ma) / 2.0;
   const double h2min = 1e-8;
   const double M000 = M4[0];
-  const double u = M4[1] / M000, v = M4[5] / M000, w = M4[15] / M000;
+  const double u = M4[1 * ist] / M000, v = M4[5 * ist] / M000, w = M4[15 * ist] / M000;
   double C[35], S[35];
-  raw_to_central_r(M4, C);
+  raw_to_central_r(M4, ist, C);
   central_to_std(C, S);
   const double C200 = jmax(EPS, C[2]), C020 = jmax(EPS, C[9]), C002 = jmax(EPS, C[19]);
   double s[NS];
@@ -469,10 +473,10 @@ HQN void flux_closure35(const double* M4, int flag2D, double Ma, double* Fx, dou
   central_to_raw_r<56>(M000, u, v, w, A);
 #pragma unroll
   for (int n = 0; n < 35; ++n) {
-    Mr[n] = A[n];
-    if (Fx) Fx[n] = A[T_FX[n]];
-    if (Fy) Fy[n] = A[T_FY[n]];
-    if (Fz) Fz[n] = A[T_FZ[n]];
+    Mr[n * mst] = A[n];
+    if (Fx) Fx[n * fst] = A[T_FX[n]];
+    if (Fy) Fy[n * fst] = A[T_FY[n]];
+    if (Fz) Fz[n * fst] = A[T_FZ[n]];
   }
 }
 

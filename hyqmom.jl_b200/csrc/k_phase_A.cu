@@ -46,12 +46,7 @@ __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure(const double*
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N, c = (long long)blockIdx.x * BS_A + threadIdx.x;
   if (c >= N) return;
-  double m[35], a[35];
-#pragma unroll
-  for (int n = 0; n < 35; ++n) m[n] = M[c + N * n];
-  flux_closure35(m, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, a);
-#pragma unroll
-  for (int n = 0; n < 35; ++n) out[c + N * n] = a[n];
+  flux_closure35(M + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
 }
 
 // A2/A3: eigenvalues6_hyperbolic_3D along x (axis 1) or y (axis 2)
@@ -93,18 +88,12 @@ __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A5_flux(const double* __
   const long long N = sc.N, c = (long long)blockIdx.x * BS_A + threadIdx.x;
   double local = 0.0;
   if (c < N) {
-    double m[35], fx[35], fy[35], fz[35], mr[35];
-#pragma unroll
-    for (int n = 0; n < 35; ++n) m[n] = in[c + N * n];
-    flux_closure35(m, sc.flag2D, sc.Ma, fx, fy, fz, mr);
-#pragma unroll
-    for (int n = 0; n < 35; ++n) {
-      Fx[c + N * n] = fx[n]; Fy[c + N * n] = fy[n]; Fz[c + N * n] = fz[n]; M[c + N * n] = mr[n];
-    }
+    flux_closure35(in + c, sc.flag2D, sc.Ma, Fx + c, Fy + c, Fz + c, M + c, N, N, N);
+    const double* mr = M + c;  // the realized moments this thread just wrote, stride N
     double v5[6];
-    closure_eigs(mr[0], mr[1], mr[2], mr[3], mr[4], v5[0], v5[1]);
-    closure_eigs(mr[0], mr[5], mr[9], mr[12], mr[14], v5[2], v5[3]);
-    closure_eigs(mr[0], mr[15], mr[19], mr[22], mr[24], v5[4], v5[5]);
+    closure_eigs(mr[0], mr[1 * N], mr[2 * N], mr[3 * N], mr[4 * N], v5[0], v5[1]);
+    closure_eigs(mr[0], mr[5 * N], mr[9 * N], mr[12 * N], mr[14 * N], v5[2], v5[3]);
+    closure_eigs(mr[0], mr[15 * N], mr[19 * N], mr[22 * N], mr[24 * N], v5[4], v5[5]);
 #pragma unroll
     for (int q = 0; q < 6; q += 2) {
       const double lo = jmin(v5[q], vp[c + N * q]), hi = jmax(v5[q + 1], vp[c + N * (q + 1)]);

@@ -18,12 +18,7 @@ __global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E1_closure(const double
   if (!clk->active) return;
   const long long N = sc.N, c = (long long)blockIdx.x * BS_EF + threadIdx.x;
   if (c >= N) return;
-  double m[35], a[35];
-#pragma unroll
-  for (int n = 0; n < 35; ++n) m[n] = in[c + N * n];
-  flux_closure35(m, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, a);
-#pragma unroll
-  for (int n = 0; n < 35; ++n) out[c + N * n] = a[n];
+  flux_closure35(in + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
 }
 
 // E2/E3: eigenvalues6_hyperbolic_3D along x or y (corrected moments only)
@@ -46,10 +41,8 @@ __global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E4_closure_bgk(const do
   if (!clk->active) return;
   const long long N = sc.N, c = (long long)blockIdx.x * BS_EF + threadIdx.x;
   if (c >= N) return;
-  double m[35], a[35];
-#pragma unroll
-  for (int n = 0; n < 35; ++n) m[n] = in[c + N * n];
-  flux_closure35(m, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, a);
+  double a[35];
+  flux_closure35(in + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, a, N, 1);
   collision35(a, clk->dt, sc.Kn, sc.positivity);
 #pragma unroll
   for (int n = 0; n < 35; ++n) Mout[c + N * n] = a[n];
