@@ -453,10 +453,14 @@ HQN void correct_for_real(const double* M, int pa_i, int pa_j, int pb_i, int pb_
 }
 
 // eigenvalues6_hyperbolic_3D for axis 1 (x) or 2 (y).
-HQN void eigenvalues6(const double* M, int axis, int flag2D, double Ma, double& vmin, double& vmax, double* Mr) {
+// Moment n is read from M[n * ist] and written to Mr[n * ost] (the step
+// kernels pass the cell's entry of the moment-major fields, stride N); M and
+// Mr must not overlap.
+HQN void eigenvalues6(const double* M, int axis, int flag2D, double Ma, double& vmin, double& vmax, double* Mr, long long ist = 1,
+                      long long ost = 1) {
   const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
   double a[15], b[15];
-  for (int n = 0; n < 15; ++n) { a[n] = M[SLICE[sa][n]]; b[n] = M[SLICE[sb][n]]; }
+  for (int n = 0; n < 15; ++n) { a[n] = M[SLICE[sa][n] * ist]; b[n] = M[SLICE[sb][n] * ist]; }
   EigOut ea = jac_eigs(a), eb = jac_eigs(b);
   auto combine = [&]() {
     vmin = ea.vmin; vmax = ea.vmax;
@@ -464,39 +468,40 @@ HQN void eigenvalues6(const double* M, int axis, int flag2D, double Ma, double& 
   };
   combine();
 #pragma unroll
-  for (int n = 0; n < 35; ++n) Mr[n] = M[n];
+  for (int n = 0; n < 35; ++n) Mr[n * ost] = M[n * ist];
   const double thr = 1000.0 * EPS;
   const bool ca = ea.imax > thr, cb = eb.imax > thr;
   if (ca || cb) {
-    double Mc[35];
+    double Ml[35], Mc[35];
+    for (int n = 0; n < 35; ++n) Ml[n] = M[n * ist];
     // pair a is always the UV plane; pair b is UW (x) or VW (y)
-    correct_for_real(M, 0, 1, axis == 1 ? 0 : 1, 2, (ca ? 1 : 0) | (cb ? 2 : 0), flag2D, Ma, Mc);
+    correct_for_real(Ml, 0, 1, axis == 1 ? 0 : 1, 2, (ca ? 1 : 0) | (cb ? 2 : 0), flag2D, Ma, Mc);
     for (int n = 0; n < 15; ++n) { a[n] = Mc[SLICE[sa][n]]; b[n] = Mc[SLICE[sb][n]]; }
     ea = jac_eigs(a); eb = jac_eigs(b);
     combine();
-#pragma unroll
-    for (int n = 0; n < 35; ++n) Mr[n] = Mc[n];
+    for (int n = 0; n < 35; ++n) Mr[n * ost] = Mc[n];
   }
 }
 
-// eigenvalues6z_hyperbolic_3D
-HQN void eigenvalues6z(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr) {
-#pragma unroll
-  for (int n = 0; n < 35; ++n) Mr[n] = M[n];
-  if (positivity && M[0] <= 0.0) Mr[0] = jmax(M[0], 1e-14);
+// eigenvalues6z_hyperbolic_3D (strides as eigenvalues6)
+HQN void eigenvalues6z(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr, long long ist = 1,
+                       long long ost = 1) {
   double Mw[35];
 #pragma unroll
-  for (int n = 0; n < 35; ++n) Mw[n] = M[n];
-  Mw[0] = Mr[0];
+  for (int n = 0; n < 35; ++n) Mw[n] = M[n * ist];
+  if (positivity && Mw[0] <= 0.0) Mw[0] = jmax(Mw[0], 1e-14);
   if (positivity && Mw[0] > 1e-15) {
     const double m000 = Mw[0];
-    const double vx = M[2] / m000 - sq(M[1] / m000), vy = M[9] / m000 - sq(M[5] / m000), vz = M[19] / m000 - sq(M[15] / m000);
+    const double vx = M[2 * ist] / m000 - sq(M[1 * ist] / m000), vy = M[9 * ist] / m000 - sq(M[5 * ist] / m000),
+                 vz = M[19 * ist] / m000 - sq(M[15 * ist] / m000);
     if (vx < 0.0 || vy < 0.0 || vz < 0.0) {
-      flux_closure35(M, flag2D, Ma, nullptr, nullptr, nullptr, Mr);
-#pragma unroll
-      for (int n = 0; n < 35; ++n) Mw[n] = Mr[n];
+      flux_closure35(M, flag2D, Ma, nullptr, nullptr, nullptr, Mw, ist, 1);
     }
   }
+  // Mr: the input with its density floored or, after the negative-variance
+  // re-realization, that closure -- Mw in both cases
+#pragma unroll
+  for (int n = 0; n < 35; ++n) Mr[n * ost] = Mw[n];
   double a[15], b[15];
   for (int n = 0; n < 15; ++n) { a[n] = Mw[WUI[n]]; b[n] = Mw[SLICE[3][n]]; }
   EigOut ea = jac_eigs(a), eb = jac_eigs(b);
@@ -505,11 +510,14 @@ HQN void eigenvalues6z(const double* M, int flag2D, double Ma, int positivity, d
   const double thr = 1000.0 * EPS;
   const bool ca = ea.imax > thr, cb = eb.imax > thr;
   if (ca || cb) {
-    correct_for_real(M, 0, 2, 1, 2, (ca ? 1 : 0) | (cb ? 2 : 0), flag2D, Ma, Mr);
-    for (int n = 0; n < 15; ++n) { a[n] = Mr[WUI[n]]; b[n] = Mr[SLICE[3][n]]; }
+    double Ml[35], Mc[35];
+    for (int n = 0; n < 35; ++n) Ml[n] = M[n * ist];
+    correct_for_real(Ml, 0, 2, 1, 2, (ca ? 1 : 0) | (cb ? 2 : 0), flag2D, Ma, Mc);
+    for (int n = 0; n < 15; ++n) { a[n] = Mc[WUI[n]]; b[n] = Mc[SLICE[3][n]]; }
     ea = jac_eigs(a); eb = jac_eigs(b);
     vmin = jmin(ea.vmin, eb.vmin);
     vmax = jmax(ea.vmax, eb.vmax);
+    for (int n = 0; n < 35; ++n) Mr[n * ost] = Mc[n];
   }
 }
 

@@ -55,12 +55,8 @@ __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* __restri
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N, c = (long long)blockIdx.x * BS_A + threadIdx.x;
   if (c >= N) return;
-  double m[35], r[35], lo, hi;
-#pragma unroll
-  for (int n = 0; n < 35; ++n) m[n] = in[c + N * n];
-  eigenvalues6(m, axis, sc.flag2D, sc.Ma, lo, hi, r);
-#pragma unroll
-  for (int n = 0; n < 35; ++n) out[c + N * n] = r[n];
+  double lo, hi;
+  eigenvalues6(in + c, axis, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
   vlo[c] = lo; vhi[c] = hi;
 }
 
@@ -70,12 +66,8 @@ __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A4_eigz(const double* __rest
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N, c = (long long)blockIdx.x * BS_A + threadIdx.x;
   if (c >= N) return;
-  double m[35], r[35], lo, hi;
-#pragma unroll
-  for (int n = 0; n < 35; ++n) m[n] = in[c + N * n];
-  eigenvalues6z(m, sc.flag2D, sc.Ma, sc.positivity, lo, hi, r);
-#pragma unroll
-  for (int n = 0; n < 35; ++n) out[c + N * n] = r[n];
+  double lo, hi;
+  eigenvalues6z(in + c, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out + c, N, N);
   vlo[c] = lo; vhi[c] = hi;
 }
 

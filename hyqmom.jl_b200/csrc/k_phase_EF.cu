@@ -27,12 +27,8 @@ __global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* __restr
   if (!clk->active) return;
   const long long N = sc.N, c = (long long)blockIdx.x * BS_EF + threadIdx.x;
   if (c >= N) return;
-  double m[35], r[35], v0, v1;
-#pragma unroll
-  for (int n = 0; n < 35; ++n) m[n] = in[c + N * n];
-  eigenvalues6(m, axis, sc.flag2D, sc.Ma, v0, v1, r);
-#pragma unroll
-  for (int n = 0; n < 35; ++n) out[c + N * n] = r[n];
+  double v0, v1;
+  eigenvalues6(in + c, axis, sc.flag2D, sc.Ma, v0, v1, out + c, N, N);
 }
 
 // E4: Flux_closure35_and_realizable_3D, then collision35 with the step's dt
