@@ -64,24 +64,26 @@ __global__ void __launch_bounds__(1024) k_cfl(const double* __restrict__ blockma
 }
 
 // pas_HLL along one line of Np cells (stride `st`, line start `base`) for the
-// cell at position i of the line: the two faces it touches, with everything
-// that does not depend on the moment (clamped indices, HLL speeds of the
-// face, whether W* is formed) resolved once per cell.
+// cell at position i of the line.  Its update reads the clamped cell ip and
+// its two neighbours only (cells L = ip-1, C = ip, R = ip+1); everything
+// that does not depend on the moment -- the HLL speeds of the two faces,
+// whether W* is formed, and which of L, C, R the boundary rules substitute
+// -- is resolved once per cell.
 struct HllFace {
-  int jj, fa, fb, j;        // W* cell jj (and jj+1), flux cells fa, fb, face cells j, j+1 (offsets from base)
   double l1, l2, ll, lr;
   bool w;
 };
 struct HllLine {
-  long long base;
-  int st, ip;               // ip: offset of the clamped cell whose update is returned
-  int Np;
+  long long base;           // offset of cell L
+  int st;
+  bool two;                 // Np == 2: pas_HLL returns [M2, M2]
+  bool sh0;                 // ip == 1: face ip-1 uses W*[1] and F[1] (cell C)
+  bool sh1;                 // ip + 1 == Np - 1: face ip uses F[Np-2] (cell C)
   double r;                 // dt / ds
   HllFace f0, f1;           // faces ip-1 and ip
 };
 
-__device__ __forceinline__ HllFace hll_face(const double* __restrict__ vmin, const double* __restrict__ vmax, long long base, int st,
-                                            int Np, int j) {
+__device__ __forceinline__ HllFace hll_face(const double* __restrict__ vmin, const double* __restrict__ vmax, long long base, int st, int j) {
   HllFace f;
   const int jj = j < 1 ? 1 : j;  // face 0 uses W*[1] with zero speeds
   const double a = vmin[base + st * jj], b = vmin[base + st * (jj + 1)];
@@ -90,46 +92,43 @@ __device__ __forceinline__ HllFace hll_face(const double* __restrict__ vmin, con
   f.l2 = jmax(c, d);
   f.w = fabs(f.l1 - f.l2) > 1e-10;
   if (j == 0) { f.ll = 0.0; f.lr = 0.0; } else { f.ll = f.l1; f.lr = f.l2; }
-  f.jj = st * jj;
-  // boundary-modified fluxes: F[0] := F[1], F[Np-1] := F[Np-2]
-  f.fa = st * (j < 1 ? 1 : j);
-  f.fb = st * ((j + 1 > Np - 2) ? Np - 2 : j + 1);
-  f.j = st * j;
   return f;
 }
 
 __device__ __forceinline__ HllLine hll_setup(const double* __restrict__ vmin, const double* __restrict__ vmax, long long base, int st,
                                              int Np, int i, double r) {
   HllLine L;
-  L.base = base; L.st = st; L.Np = Np; L.r = r;
-  if (Np == 2) { L.ip = st; return L; }  // pas_HLL with Np = 2 returns [M2, M2]
+  L.st = st; L.r = r;
+  L.two = (Np == 2);
+  if (L.two) { L.base = base; L.sh0 = L.sh1 = false; return L; }
   const int ip = i < 1 ? 1 : (i > Np - 2 ? Np - 2 : i);
-  L.ip = st * ip;
-  L.f0 = hll_face(vmin, vmax, base, st, Np, ip - 1);
-  L.f1 = hll_face(vmin, vmax, base, st, Np, ip);
+  L.base = base + (long long)st * (ip - 1);
+  L.sh0 = (ip == 1);
+  L.sh1 = (ip + 1 > Np - 2);
+  L.f0 = hll_face(vmin, vmax, base, st, ip - 1);
+  L.f1 = hll_face(vmin, vmax, base, st, ip);
   return L;
 }
 
-// flux_HLL at one face for one moment (M, F already offset to the moment;
-// `st` the line stride)
-__device__ __forceinline__ double hll_flux(const double* __restrict__ M, const double* __restrict__ F, long long base, int st,
-                                           const HllFace& f) {
+// flux_HLL at one face for one moment from the W* pair (mj, mj1, fj, fj1),
+// the boundary-modified fluxes (Fa, Fb) and the face's cells (Ma_, Mb)
+__device__ __forceinline__ double hll_flux(const HllFace& f, double mj, double mj1, double fj, double fj1, double Fa, double Fb, double Ma_,
+                                           double Mb) {
   double ws = 0.0;
-  if (f.w) {
-    const double mj = M[base + f.jj], mj1 = M[base + f.jj + st];
-    const double fj = F[base + f.jj], fj1 = F[base + f.jj + st];
-    ws = (f.l1 * mj - f.l2 * mj1) / (f.l1 - f.l2) - (fj - fj1) / (f.l1 - f.l2);
-  }
-  const double Fa = F[base + f.fa], Fb = F[base + f.fb];
-  const double Ma_ = M[base + f.j], Mb = M[base + f.j + st];
+  if (f.w) ws = (f.l1 * mj - f.l2 * mj1) / (f.l1 - f.l2) - (fj - fj1) / (f.l1 - f.l2);
   return 0.5 * (Fa + Fb) - 0.5 * (fabs(f.ll) * (ws - Ma_) - fabs(f.lr) * (ws - Mb));
 }
 
-// The x, y or z update of one moment of the cell (pas_HLL for that line).
+// The x, y or z update of one moment of the cell (pas_HLL for that line);
+// M, F already offset to the moment.
 __device__ __forceinline__ double hll_update(const double* __restrict__ M, const double* __restrict__ F, const HllLine& L) {
-  if (L.Np == 2) return M[L.base + L.ip];
-  const double f1 = hll_flux(M, F, L.base, L.st, L.f1), f0 = hll_flux(M, F, L.base, L.st, L.f0);
-  return M[L.base + L.ip] - L.r * (f1 - f0);
+  if (L.two) return M[L.base + L.st];
+  const long long o = L.base;
+  const double mL = M[o], mC = M[o + L.st], mR = M[o + 2 * L.st];
+  const double fL = F[o], fC = F[o + L.st], fR = F[o + 2 * L.st];
+  const double f1 = hll_flux(L.f1, mC, mR, fC, fR, fC, L.sh1 ? fC : fR, mC, mR);
+  const double f0 = L.sh0 ? hll_flux(L.f0, mC, mR, fC, fR, fC, fC, mL, mC) : hll_flux(L.f0, mL, mC, fL, fC, fL, fC, mL, mC);
+  return mC - L.r * (f1 - f0);
 }
 
 // One thread per cell: the face speeds of the x, y and z lines are resolved
