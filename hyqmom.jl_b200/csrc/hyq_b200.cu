@@ -1,6 +1,6 @@
 // libhyqmom_b200.so: kernels and C-ABI of the HyQMOM explicit step on B200.
 //
-// One step = eleven launches on the context stream, captured once in a CUDA
+// One step = thirteen launches on the context stream, captured once in a CUDA
 // graph and replayed:
 //   phase A      five per-cell kernels (k_phase_A.cu): closure +
 //                realizability, x, y and z flux-Jacobian eigenvalues with
@@ -15,7 +15,8 @@
 //                (src/numerics/apply_flux_update_3d.jl:30-213,
 //                 src/numerics/pas_HLL.jl:238-298, flux_HLL.jl:318-330,
 //                 src/simulation_runner.jl:498-520)
-//   phase EF     four per-cell kernels (k_phase_EF.cu): realizability pass
+//   phase EF     per-cell kernels (k_phase_EF.cu): realizability pass, with
+//                the eigen corrections of listed cells in their own pass,
 //                and BGK collision (src/simulation_runner.jl:526-557)
 // The loop predicate `t < tmax && nn < nnmax` is evaluated on the device, so
 // any number of steps can be queued without a host round trip.
@@ -206,7 +207,7 @@ void enqueue_step(hyq_ctx* ctx, cudaStream_t s) {
   launch_phase_A(ctx->sc, ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s);
   k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
   k_hll<<<grid_of(N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
-  launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->clk, s);
+  launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->clk, s);
 }
 }  // namespace
 
@@ -365,7 +366,7 @@ int hyq_advance_timed(hyq_ctx* ctx, int64_t steps, float* ms) {
     cudaEventRecord(ev[6], s);
     k_hll<<<grid_of(N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
     cudaEventRecord(ev[7], s);
-    launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->clk, s, ev + 8);
+    launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->clk, s, ev + 8);
     HQ_CHECK(ctx, cudaEventSynchronize(ev[K]));
     for (int q = 0; q < K; ++q) {
       float t = 0.0f;

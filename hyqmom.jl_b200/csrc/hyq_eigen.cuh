@@ -483,6 +483,19 @@ HQN void eigenvalues6(const double* M, int axis, int flag2D, double Ma, double& 
   }
 }
 
+// Which of eigenvalues6's two planes need the complex-eigenvalue correction
+// (bit 0: first slice, bit 1: second), from the same Jacobians and the same
+// test; phase E only needs the corrected moments, so its kernels decide here
+// and leave the corrections to a separate pass over the flagged cells.
+HQN int eigenvalues6_flags(const double* M, int axis, long long ist) {
+  const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
+  double a[15], b[15];
+  for (int n = 0; n < 15; ++n) { a[n] = M[SLICE[sa][n] * ist]; b[n] = M[SLICE[sb][n] * ist]; }
+  const EigOut ea = jac_eigs(a), eb = jac_eigs(b);
+  const double thr = 1000.0 * EPS;
+  return (ea.imax > thr ? 1 : 0) | (eb.imax > thr ? 2 : 0);
+}
+
 // eigenvalues6z_hyperbolic_3D (strides as eigenvalues6)
 HQN void eigenvalues6z(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr, long long ist = 1,
                        long long ost = 1) {

@@ -105,7 +105,7 @@ extern "C" int hyq_step_noalloc(const hyq_params* p, double* M, hyq_stats* stats
   launch_phase_A(sc, M, Mtmp, Fx, Fy, Fz, vp, blockmax, clk, s);
   launch_cfl(blockmax, sc, clk, s);
   launch_hll(M, Fx, Fy, Fz, vp, Mtmp, sc, clk, s);
-  launch_phase_EF(sc, Mtmp, M, Fx, Fy, Fz, clk, s);
+  launch_phase_EF(sc, Mtmp, M, Fx, Fy, Fz, vp, clk, s);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(e, "launch");
 
   DevClock h;

@@ -9,26 +9,59 @@ namespace hyqk {
 namespace {
 
 
-// Phases [E]+[F] run as four kernels, one per-cell function each (small code
-// per kernel); intermediate states go through the flux buffers, dead after
-// the HLL sweep:  Mtmp -E1-> Fx -E2-> Fy -E3-> Fz -E4-> M.
-// E1: Flux_closure35_and_realizable_3D
-__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E1_closure(const double* __restrict__ in, double* __restrict__ out, const StepConst sc,
-                                                                const DevClock* clk) {
+// Phases [E]+[F] run as per-function kernels (small code per kernel);
+// intermediate states go through the flux buffers, dead after the HLL sweep:
+//   Mtmp -E1-> Fx -E2-> Fy -E3-> Fz -E4-> M.
+// E2/E3 copy the moments and list the cells whose Jacobians have complex
+// eigenvalues; k_E_fix then corrects only those cells, so that a few such
+// cells no longer hold every lane of their warps in the correction.  The
+// lists live in the wave-speed buffer vp, dead after the HLL sweep
+// (vp[0..N): entries (cell << 2) | planes; two counters after them).
+__device__ __forceinline__ unsigned int* fix_counters(double* vp, long long N) { return reinterpret_cast<unsigned int*>(vp + N); }
+
+// E1: Flux_closure35_and_realizable_3D; also resets the two fix counters
+__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E1_closure(const double* __restrict__ in, double* __restrict__ out, double* vp,
+                                                                const StepConst sc, const DevClock* clk) {
   if (!clk->active) return;
   const long long N = sc.N, c = (long long)blockIdx.x * BS_EF + threadIdx.x;
+  if (c == 0) { unsigned int* cnt = fix_counters(vp, N); cnt[0] = 0; cnt[1] = 0; }
   if (c >= N) return;
   flux_closure35(in + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
 }
 
-// E2/E3: eigenvalues6_hyperbolic_3D along x or y (corrected moments only)
-__global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* __restrict__ in, double* __restrict__ out, int axis, const StepConst sc,
-                                                           const DevClock* clk) {
+// E2/E3: eigenvalues6_hyperbolic_3D along x or y: copy, and list the cells
+// that need the correction (counter `which` of the two)
+__global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* __restrict__ in, double* __restrict__ out, double* vp, int axis,
+                                                           int which, const StepConst sc, const DevClock* clk) {
   if (!clk->active) return;
   const long long N = sc.N, c = (long long)blockIdx.x * BS_EF + threadIdx.x;
   if (c >= N) return;
-  double v0, v1;
-  eigenvalues6(in + c, axis, sc.flag2D, sc.Ma, v0, v1, out + c, N, N);
+  const int planes = eigenvalues6_flags(in + c, axis, N);
+#pragma unroll
+  for (int n = 0; n < 35; ++n) out[c + N * n] = in[c + N * n];
+  if (planes) {
+    const unsigned int slot = atomicAdd(fix_counters(vp, N) + which, 1u);
+    reinterpret_cast<unsigned long long*>(vp)[slot] = ((unsigned long long)c << 2) | (unsigned long long)planes;
+  }
+}
+
+// The correction of the listed cells (correct_moments_for_real_eigenvalues,
+// as in eigenvalues6), grid-stride over the list
+__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E_fix(const double* __restrict__ in, double* __restrict__ out, const double* vp,
+                                                               int axis, int which, const StepConst sc, const DevClock* clk) {
+  if (!clk->active) return;
+  const long long N = sc.N;
+  const unsigned int count = reinterpret_cast<const unsigned int*>(vp + N)[which];
+  const unsigned long long* list = reinterpret_cast<const unsigned long long*>(vp);
+  for (unsigned int e = blockIdx.x * BS_EF + threadIdx.x; e < count; e += gridDim.x * BS_EF) {
+    const unsigned long long v = list[e];
+    const long long c = (long long)(v >> 2);
+    const int planes = int(v & 3ull);
+    double Ml[35], Mc[35];
+    for (int n = 0; n < 35; ++n) Ml[n] = in[c + N * n];
+    correct_for_real(Ml, 0, 1, axis == 1 ? 0 : 1, 2, planes, sc.flag2D, sc.Ma, Mc);
+    for (int n = 0; n < 35; ++n) out[c + N * n] = Mc[n];
+  }
 }
 
 // E4: Flux_closure35_and_realizable_3D, then collision35 with the step's dt
@@ -46,14 +79,17 @@ __global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E4_closure_bgk(const do
 
 }  // namespace
 
-void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, double* Fx, double* Fy, double* Fz, const DevClock* clk,
-                     cudaStream_t s, cudaEvent_t* ev) {
+void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, double* Fx, double* Fy, double* Fz, double* vp,
+                     const DevClock* clk, cudaStream_t s, cudaEvent_t* ev) {
   const int g = grid_of(sc.N, BS_EF);
-  k_E1_closure<<<g, BS_EF, 0, s>>>(Min, Fx, sc, clk);
+  const int gfix = g < 148 * 8 ? g : 148 * 8;
+  k_E1_closure<<<g, BS_EF, 0, s>>>(Min, Fx, vp, sc, clk);
   if (ev) cudaEventRecord(ev[0], s);
-  k_E_eig<<<g, BS_EF, 0, s>>>(Fx, Fy, 1, sc, clk);
+  k_E_eig<<<g, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk);
+  k_E_fix<<<gfix, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk);
   if (ev) cudaEventRecord(ev[1], s);
-  k_E_eig<<<g, BS_EF, 0, s>>>(Fy, Fz, 2, sc, clk);
+  k_E_eig<<<g, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk);
+  k_E_fix<<<gfix, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk);
   if (ev) cudaEventRecord(ev[2], s);
   k_E4_closure_bgk<<<g, BS_EF, 0, s>>>(Fz, Mout, sc, clk);
   if (ev) cudaEventRecord(ev[3], s);
