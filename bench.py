@@ -45,8 +45,8 @@ KERNELS = ["A1_closure", "A2_eig_x", "A3_eig_y", "A4_eig_z", "A5_flux_speeds", "
 # the 96x96x48 case of the same workload (profiles/step_kernels_crossing96x96x48.md),
 # scaled to a launch by its cells: the local-memory traffic per cell does not
 # depend on the grid size.
-TRAFFIC_PER_CELL = {"A1_closure": 6977.0, "A2_eig_x": 3648.0, "A3_eig_y": 3649.0, "A4_eig_z": 3678.0, "A5_flux_speeds": 9289.0,
-                    "hll": 1727.0, "E1_closure": 6872.0, "E2_eig_x": 3636.0, "E3_eig_y": 3636.0, "E4_closure_bgk": 7254.0}
+TRAFFIC_PER_CELL = {"A1_closure": 3221.0, "A2_eig_x": 1720.0, "A3_eig_y": 1725.0, "A4_eig_z": 2326.0, "A5_flux_speeds": 4487.0,
+                    "hll": 1609.0, "E1_closure": 3211.0, "E2_eig_x": 1443.0, "E3_eig_y": 1424.0, "E4_closure_bgk": 3951.0}
 F_KERNEL = {"A1_closure": 7583.0, "A2_eig_x": 1696.2, "A3_eig_y": 1696.2, "A4_eig_z": 1708.2, "A5_flux_speeds": 9709.4,
             "cfl": 1.0, "hll": 2030.0, "E1_closure": 7583.0, "E2_eig_x": 1696.3, "E3_eig_y": 1696.3, "E4_closure_bgk": 8374.0}
 
