@@ -6,8 +6,9 @@
 // leaves the 4 x 4 active block of rows/columns 2..5.  For that case this file
 // repeats the operations of eig_real<6> -- the same expressions in the same
 // order -- with every matrix index a compile-time constant, so the 36 entries
-// stay in registers instead of local memory.  Any other case goes to
-// eig_real<6>.  tests/test_device_code_on_host.py checks the two bit for bit.
+// stay in registers instead of local memory (solve<K> also covers the
+// unpermuted case, K = 0, which the device code leaves to the general path).
+// Any other case goes to eig_real<6>.  tests/test_device_code_on_host.py checks the two bit for bit.
 #pragma once
 
 namespace hyq {

@@ -345,11 +345,13 @@ HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
 namespace hyq {
 
 // eig_real<6> of a flux Jacobian: the register-resident path (hyq_eig6.cuh)
-// when dgebal's search makes one of the two permutations it handles, else
-// the general code; identical results either way.
+// when dgebal's search isolates columns 0 and 5, else the general code;
+// identical results either way.
 HQD void eig_real_jac(double (&h)[36], double (&wr)[6], double (&wi)[6]) {
-  const int pat = e6::pattern(h);
-  if (pat < 0) {
+  // only the usual permutation takes the register path: instantiating the
+  // unpermuted case too (3 % of the Jacobians) made the kernels slower
+  // through the larger code
+  if (e6::pattern(h) != 1) {
     double J[6][6];
 #pragma unroll
     for (int r = 0; r < 6; ++r)
@@ -360,8 +362,8 @@ HQD void eig_real_jac(double (&h)[36], double (&wr)[6], double (&wi)[6]) {
   }
 #pragma unroll
   for (int i = 0; i < 6; ++i) { wr[i] = 0.0; wi[i] = 0.0; }
-  if (pat == 1) { e6::apply_pattern1(h); e6::solve<2>(h, wr, wi); }
-  else e6::solve<0>(h, wr, wi);
+  e6::apply_pattern1(h);
+  e6::solve<2>(h, wr, wi);
 }
 
 // compute_jacobian_eigenvalues for one 15-moment slice: extreme real parts

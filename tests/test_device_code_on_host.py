@@ -90,8 +90,9 @@ def jacobians(states, seed=5):
 
 
 def test_fast_eigen_path_is_bitwise_general(shim, states):
-    """The register-resident path for the permutations dgebal finds on flux
-    Jacobians gives the general eig_real<6> results bit for bit."""
+    """The register-resident path for the permutation dgebal usually finds on
+    flux Jacobians gives the general eig_real<6> results bit for bit (the
+    other patterns are recognised and left to the general code)."""
     seen = {-1: 0, 0: 0, 1: 0}
     out = np.zeros(25)
     for A in jacobians(states):
