@@ -100,14 +100,18 @@ HQN int realizable_3D(double* s) {
   if (E_(D, 0, 0) < 0.0) { realizability_S210(s[s110], s[s101], s[s011], s[s300], s[s210], s[s201], H200, beta); fE11 = 1; }
   if (E_(D, 3, 3) < 0.0) { realizability_S210(s[s110], s[s011], s[s101], s[s030], s[s120], s[s021], H020, beta); fE44 = 1; }
   if (E_(D, 5, 5) < 0.0) { realizability_S210(s[s011], s[s101], s[s110], s[s003], s[s012], s[s102], H002, beta); fE66 = 1; }
+  // delta2star_p is a pure function of s, so a projection of an unchanged s
+  // is reused below instead of recomputed (same values as the reference's
+  // recomputation); `written` records writes to s since D was formed
+  bool written = (fE11 | fE44 | fE66) != 0;
   const double S111r = realizability_S111(s[s110], s[s101], s[s011], s[s210], s[s201], s[s120], s[s021], s[s102], s[s012], s[s111]);
-  if (S111r != s[s111]) s[s111] = S111r;
+  if (S111r != s[s111]) { s[s111] = S111r; written = true; }
   const double S220_310 = realizability_S310_220(s[s110], s[s101], s[s011], s[s210], s[s120], s[s111], s[s220]);
   const double S202_310 = realizability_S310_220(s[s101], s[s110], s[s011], s[s201], s[s102], s[s111], s[s202]);
   const double S022_310 = realizability_S310_220(s[s011], s[s110], s[s101], s[s021], s[s012], s[s111], s[s022]);
   double S220_diag = s[s220], S202_diag = s[s202], S022_diag = s[s022];
   // lower_bound_S220: projection diagonal of the current moments
-  delta2star_p(s, 0, D);
+  if (written) delta2star_p(s, 0, D);
   const double lb0 = D.q[TRI[1][1]], lb1 = D.q[TRI[2][2]], lb2 = D.q[TRI[4][4]];
   if (s[s220] < lb0) { S220_diag = lb0; fE22 = 1; flag220 = 1; }
   if (s[s202] < lb1) { S202_diag = lb1; fE33 = 1; flag220 = 1; }
@@ -135,26 +139,35 @@ HQN int realizable_3D(double* s) {
 
   // 2x2 minors of the six permutations
   double S220a = s[s220], S220b = s[s220], S202a = s[s202], S202b = s[s202], S022a = s[s022], S022b = s[s022];
-  // Of the six projections only their 2x2 and 3x3 leading minors and the
-  // leading 3x3 entries of permutations 0, 2, 5 are used below, so those are
-  // kept instead of the six Delta structs (a smaller per-thread frame; the
-  // values are the same).
-  double d2[6], d3[6];
+  // Of the six projections only their 2x2, 3x3 and 4x4 leading minors and
+  // the leading 3x3 entries of permutations 0, 2, 5 are used below (the 4x4
+  // minors while s is unchanged), so those are kept instead of the six Delta
+  // structs (a smaller per-thread frame; the values are the same).
+  double d2[6], d3[6], d4[6];
   double Ee[3][6];  // (0,0),(0,1),(0,2),(1,1),(1,2),(2,2) of projections 0, 2, 5
   auto keep = [&](int p, const Delta& Dp) {
     d3[p] = lead_det(Dp, 3);
+    d4[p] = lead_det(Dp, 4);
     const int slot = (p == 0) ? 0 : (p == 2) ? 1 : (p == 5) ? 2 : -1;
     if (slot >= 0) {
       Ee[slot][0] = E_(Dp, 0, 0); Ee[slot][1] = E_(Dp, 0, 1); Ee[slot][2] = E_(Dp, 0, 2);
       Ee[slot][3] = E_(Dp, 1, 1); Ee[slot][4] = E_(Dp, 1, 2); Ee[slot][5] = E_(Dp, 2, 2);
     }
   };
+  // D is still the projection 0 of s unless the bound_minor1 block wrote s
+  const bool reuseD = (fE11 | fE22 | fE33 | fE44 | fE55 | fE66) == 0;
   for (int p = 0; p < 6; ++p) {
+    if (p == 0 && reuseD) {
+      d2[0] = lead_det(D, 2);
+      keep(0, D);
+      continue;
+    }
     Delta Dp;
     delta2star_p(s, p, Dp);
     d2[p] = lead_det(Dp, 2);
     keep(p, Dp);
   }
+  bool fresh = true;  // d2..Ee are those of the current s
   int flag310 = 0;
   if (!fE11 && !fE44 && d2[0] < h2min) {
     s[s310] = realizability_S310(s[s110], s[s101], s[s011], s[s300], s[s210], s[s120], s[s201], s[s111], s[s310], s[s220], H200, beta);
@@ -213,6 +226,7 @@ HQN int realizable_3D(double* s) {
       if (e11 > diagmin) { S220a = d22 + e13 * e13 / e11; S202a = d33 + e12 * e12 / e11; }
       s[s211] = realizability_S211(e11, e22, e33, e12, e13, d23, s[s211], beta);
       flag220 = 1;
+      fresh = false;
     }
   }
   if (!fE22 && !fE33 && !fE44 && !fE55) {
@@ -222,6 +236,7 @@ HQN int realizable_3D(double* s) {
       if (e11 > diagmin) { S220b = d22 + e13 * e13 / e11; S022b = d33 + e12 * e12 / e11; }
       s[s121] = realizability_S211(e11, e22, e33, e12, e13, d23, s[s121], beta);
       flag220 = 1;
+      fresh = false;
     }
   }
   if (!fE22 && !fE33 && !fE55 && !fE66) {
@@ -231,6 +246,7 @@ HQN int realizable_3D(double* s) {
       if (e11 > diagmin) { S202c = d22 + e13 * e13 / e11; S022c = d33 + e12 * e12 / e11; }
       s[s112] = realizability_S211(e11, e22, e33, e12, e13, d23, s[s112], beta);
       flag220 = 1;
+      fresh = false;
     }
   }
   const double S220_211 = jmax(S220a, S220b), S202_211 = jmax(S202a, S202c), S022_211 = jmax(S022b, S022c);
@@ -241,9 +257,10 @@ HQN int realizable_3D(double* s) {
   for (int q = 0; q < 6; ++q) {
     // order of the reference: E1, E3 (S220), E2, E4 (S202), E5, E6 (S022)
     const int p = (q == 0) ? 0 : (q == 1) ? 2 : (q == 2) ? 1 : (q == 3) ? 3 : (q == 4) ? 4 : 5;
+    lo[q] = cur[q]; hi[q] = cur[q];
+    if (fresh && !(d4[p] < 0.0)) continue;  // its projection is the kept one
     Delta E;
     delta2star_p(s, p, E);
-    lo[q] = cur[q]; hi[q] = cur[q];
     if (lead_det(E, 4) < 0.0) {
       flag220 = 1;
       const double ex = -E_(E, 1, 1) + E_(E, 0, 3);
