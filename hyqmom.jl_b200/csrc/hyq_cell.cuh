@@ -470,44 +470,63 @@ HQN void delta2star_p(const double* s, int P, Delta& D) {
 HQD double E_(const Delta& D, int a, int b) { return D.e[TRI[a][b]]; }
 
 // Leading K x K minor determinant with Julia det semantics (triangular
-// shortcut, else LU with partial pivoting and reciprocal row scaling).
-HQN double lead_det(const Delta& D, int K) {
-  double A[4][4];
+// shortcut, else LU with partial pivoting and reciprocal row scaling); K is
+// fixed at compile time and every loop unrolled (row swaps through
+// compile-time selects), so the K x K block stays in registers.
+template <int K> HQD double lead_det_k(const Delta& D) {
+  double A[K][K];
+#pragma unroll
   for (int i = 0; i < K; ++i)
+#pragma unroll
     for (int j = 0; j < K; ++j) A[i][j] = E_(D, i, j);
   bool triu = true, tril = true;
+#pragma unroll
   for (int i = 0; i < K; ++i)
+#pragma unroll
     for (int j = 0; j < K; ++j) {
       if (i > j && A[i][j] != 0.0) triu = false;
       if (i < j && A[i][j] != 0.0) tril = false;
     }
   if (triu || tril) {
     double p = 1.0;
+#pragma unroll
     for (int i = 0; i < K; ++i) p = p * A[i][i];
     return p;
   }
   int swaps = 0;
   bool singular = false;
+#pragma unroll
   for (int k = 0; k < K; ++k) {
     int p = k;
     double amax = fabs(A[k][k]);
+#pragma unroll
     for (int i = k + 1; i < K; ++i)
       if (fabs(A[i][k]) > amax) { amax = fabs(A[i][k]); p = i; }
     if (p != k) {
-      for (int j = 0; j < K; ++j) { const double t = A[k][j]; A[k][j] = A[p][j]; A[p][j] = t; }
+#pragma unroll
+      for (int i = k + 1; i < K; ++i)
+        if (p == i) {
+#pragma unroll
+          for (int j = 0; j < K; ++j) { const double t = A[k][j]; A[k][j] = A[i][j]; A[i][j] = t; }
+        }
       ++swaps;
     }
     if (A[k][k] == 0.0) { singular = true; continue; }
     const double r = 1.0 / A[k][k];
+#pragma unroll
     for (int i = k + 1; i < K; ++i) A[i][k] = A[i][k] * r;
+#pragma unroll
     for (int i = k + 1; i < K; ++i)
+#pragma unroll
       for (int j = k + 1; j < K; ++j) A[i][j] = A[i][j] - A[i][k] * A[k][j];
   }
   if (singular) return 0.0;
   double P = 1.0;
+#pragma unroll
   for (int i = 0; i < K; ++i) P = P * A[i][i];
   return (swaps & 1) ? -P : P;
 }
+
 
 // --------------------------------------------------- cubic (Cardano) roots
 // Reference form (rootsR / rootsR_X_Y): for c3 X^3 + c2 X^2 + c1 X + c0,

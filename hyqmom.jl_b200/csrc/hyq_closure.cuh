@@ -146,8 +146,8 @@ HQN int realizable_3D(double* s) {
   double d2[6], d3[6], d4[6];
   double Ee[3][6];  // (0,0),(0,1),(0,2),(1,1),(1,2),(2,2) of projections 0, 2, 5
   auto keep = [&](int p, const Delta& Dp) {
-    d3[p] = lead_det(Dp, 3);
-    d4[p] = lead_det(Dp, 4);
+    d3[p] = lead_det_k<3>(Dp);
+    d4[p] = lead_det_k<4>(Dp);
     const int slot = (p == 0) ? 0 : (p == 2) ? 1 : (p == 5) ? 2 : -1;
     if (slot >= 0) {
       Ee[slot][0] = E_(Dp, 0, 0); Ee[slot][1] = E_(Dp, 0, 1); Ee[slot][2] = E_(Dp, 0, 2);
@@ -158,13 +158,13 @@ HQN int realizable_3D(double* s) {
   const bool reuseD = (fE11 | fE22 | fE33 | fE44 | fE55 | fE66) == 0;
   for (int p = 0; p < 6; ++p) {
     if (p == 0 && reuseD) {
-      d2[0] = lead_det(D, 2);
+      d2[0] = lead_det_k<2>(D);
       keep(0, D);
       continue;
     }
     Delta Dp;
     delta2star_p(s, p, Dp);
-    d2[p] = lead_det(Dp, 2);
+    d2[p] = lead_det_k<2>(Dp);
     keep(p, Dp);
   }
   bool fresh = true;  // d2..Ee are those of the current s
@@ -207,7 +207,7 @@ HQN int realizable_3D(double* s) {
     for (int p = 0; p < 6; ++p) {
       Delta Dp;
       delta2star_p(s, p, Dp);
-      const double d = lead_det(Dp, 2);
+      const double d = lead_det_k<2>(Dp);
       dm = (p == 0) ? d : jmin(dm, d);
       keep(p, Dp);
     }
@@ -261,7 +261,7 @@ HQN int realizable_3D(double* s) {
     if (fresh && !(d4[p] < 0.0)) continue;  // its projection is the kept one
     Delta E;
     delta2star_p(s, p, E);
-    if (lead_det(E, 4) < 0.0) {
+    if (lead_det_k<4>(E) < 0.0) {
       flag220 = 1;
       const double ex = -E_(E, 1, 1) + E_(E, 0, 3);
       const double d22 = cur[q] - E_(E, 1, 1);
