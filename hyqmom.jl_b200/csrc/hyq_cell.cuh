@@ -1,10 +1,10 @@
 // Per-cell FP64 physics of the HyQMOM explicit step, device code for sm_100a.
 //
-// One thread owns one cell: its 35 moments live in registers, the closure,
-// realizability projection, eigen-solves and BGK relaxation run as straight
-// FP64 code.  Moment transforms are fully unrolled over compile-time
-// exponent tables so they stay in registers; the 6x6 eigen-solve keeps its
-// Hessenberg matrix in thread-local memory (L1 resident).
+// One thread owns one cell; the closure, realizability projection,
+// eigen-solves and BGK relaxation run as straight FP64 code.  Work arrays
+// that are indexed with compile-time constants (the moment transforms of the
+// closure, the leading-minor determinants, the usual case of the 6x6
+// eigen-solve) stay in registers; the rest lives in thread-local memory.
 //
 // Reference functions restated here (HyQMOM.jl):
 //   src/numerics/Flux_closure35_and_realizable_3D.jl:33-234
@@ -22,7 +22,8 @@
 // rootsR_X_Y are the Cardano roots of determinant cubics (real fast-math sqrt,
 // so three real roots give NaN exactly like the reference); jacobian6 is the
 // Jacobian of the closed 2-D x-fluxes (m32, m23, m14) with respect to
-// (m02, m12, m22, m03, m13, m04), evaluated by forward differentiation.
+// (m02, m12, m22, m03, m13, m04), in a closed form generated symbolically
+// (gen_jacobian6.inc).
 #pragma once
 #include <cstdint>
 #include <cmath>
