@@ -72,6 +72,7 @@ __global__ void __launch_bounds__(1024) k_cfl(const double* __restrict__ blockma
 // -- is resolved once per cell.
 struct HllFace {
   double l1, l2, ll, lr;
+  double rinv;              // 1 / (l1 - l2), for div_by
   bool w;
 };
 struct HllLine {
@@ -92,6 +93,7 @@ __device__ __forceinline__ HllFace hll_face(const double* __restrict__ vmin, con
   f.l1 = jmin(a, b);
   f.l2 = jmax(c, d);
   f.w = fabs(f.l1 - f.l2) > 1e-10;
+  f.rinv = 1.0 / (f.l1 - f.l2);
   if (j == 0) { f.ll = 0.0; f.lr = 0.0; } else { f.ll = f.l1; f.lr = f.l2; }
   return f;
 }
@@ -116,7 +118,12 @@ __device__ __forceinline__ HllLine hll_setup(const double* __restrict__ vmin, co
 __device__ __forceinline__ double hll_flux(const HllFace& f, double mj, double mj1, double fj, double fj1, double Fa, double Fb, double Ma_,
                                            double Mb) {
   double ws = 0.0;
-  if (f.w) ws = (f.l1 * mj - f.l2 * mj1) / (f.l1 - f.l2) - (fj - fj1) / (f.l1 - f.l2);
+  if (f.w) {
+    // the two divisions by l1 - l2 of the reference, through the face's
+    // reciprocal (div_by returns the IEEE quotient bit for bit)
+    const double d = f.l1 - f.l2;
+    ws = div_by(f.l1 * mj - f.l2 * mj1, d, f.rinv) - div_by(fj - fj1, d, f.rinv);
+  }
   return 0.5 * (Fa + Fb) - 0.5 * (fabs(f.ll) * (ws - Ma_) - fabs(f.lr) * (ws - Mb));
 }
 
@@ -135,7 +142,7 @@ __device__ __forceinline__ double hll_update(const double* __restrict__ M, const
 // One thread per cell: the face speeds of the x, y and z lines are resolved
 // once, then the 35 moments are updated in turn (coalesced along x).
 #ifndef HQ_MINB_HLL
-#define HQ_MINB_HLL 3
+#define HQ_MINB_HLL 4
 #endif
 __global__ void __launch_bounds__(BS_HLL, HQ_MINB_HLL) k_hll(const double* __restrict__ M, const double* __restrict__ Fx, const double* __restrict__ Fy,
                                                  const double* __restrict__ Fz, const double* __restrict__ vp, double* __restrict__ Mout,

@@ -89,6 +89,25 @@ HQD double hcbrt(double x) {
   return x < 0.0 ? -y : y;
 }
 
+// a / d when the reciprocal r = 1.0 / d (IEEE-rounded) is already known, as
+// in the HLL star state where the same d divides all 35 moments: q = a r
+// is within an ulp of a / d, the remainder a - q d is exact with one fused
+// multiply-add, and q + (a - q d) r rounds to the correctly rounded quotient
+// (Markstein's correction step, IBM J. Res. Dev. 34(1), 1990).  A zero a
+// gives the signed zero a r (the sign of a / d); outside the normal range of
+// the quotient (and for Inf/NaN) it falls back to a / d.  The result equals
+// a / d bit for bit; tests/test_device_code_on_host.py checks that on random
+// operands.
+HQD double div_by(double a, double d, double r) {
+  const double q = a * r;
+  if (fabs(q) > 1e-290 && fabs(q) < 1e290) {
+    const double e = fma(-q, d, a);
+    return fma(e, r, q);
+  }
+  if (a == 0.0) return q;
+  return a / d;
+}
+
 // 35-moment order (src/utils/moment_idx.jl:73-76) as exponent tables.
 __device__ constexpr int T_EXI[35] = {0,1,2,3,4,0,1,2,3,0,1,2,0,1,0,0,1,2,3,0,1,2,0,1,0,0,1,2,0,1,0,0,1,0,0};
 __device__ constexpr int T_EXJ[35] = {0,0,0,0,0,1,1,1,1,2,2,2,3,3,4,0,0,0,0,0,0,0,0,0,0,1,1,1,2,2,3,1,1,1,2};

@@ -4,7 +4,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
-using std::sqrt; using std::fabs; using std::isfinite; using std::isinf; using std::signbit; using std::rint; using std::ldexp; using std::frexp; using std::fmax;
+using std::sqrt; using std::fabs; using std::isfinite; using std::isinf; using std::signbit; using std::rint; using std::ldexp; using std::frexp; using std::fmax; using std::fma;
 static inline double __longlong_as_double(long long x) { double d; std::memcpy(&d, &x, 8); return d; }
 #define __device__
 #define __forceinline__ inline
@@ -19,6 +19,29 @@ void sh_eig(const double* m, int axis, int flag2D, double Ma, int pos, double* v
 }
 void sh_closure(const double* mom, double* v) { closure_eigs(mom[0], mom[1], mom[2], mom[3], mom[4], v[0], v[1]); }
 void sh_coll(double* m, double dt, double Kn, int pos) { collision35(m, dt, Kn, pos); }
+// div_by against plain division on n pseudo-random operand pairs (exponents
+// within +-e of 1, significands random or all ones); returns the mismatches
+long long sh_div_check(long long n, int e, unsigned long long seed) {
+  unsigned long long x = seed | 1ull;
+  auto next = [&]() { x ^= x << 13; x ^= x >> 7; x ^= x << 17; return x; };
+  auto mk = [&](int mode) {
+    unsigned long long m = next() & 0xFFFFFFFFFFFFFull;
+    if (mode == 1) m = 0xFFFFFFFFFFFFFull;
+    const int ex = int(next() % (unsigned long long)(2 * e + 1)) - e;
+    unsigned long long b = ((unsigned long long)(ex + 1023) << 52) | m | ((next() & 1) << 63);
+    double v; std::memcpy(&v, &b, 8); return v;
+  };
+  long long bad = 0;
+  for (long long i = 0; i < n; ++i) {
+    const double d = mk(int(i & 1));
+    double a = mk(int((i >> 1) & 1));
+    if ((i & 15) == 3) a = 0.0;
+    if ((i & 15) == 7) a = -0.0;
+    const double q1 = div_by(a, d, 1.0 / d), q2 = a / d;
+    if (std::memcmp(&q1, &q2, 8) != 0) ++bad;
+  }
+  return bad;
+}
 // eig_real<6> and the register-resident flux-Jacobian path on the same
 // matrix: out[0..11] = general (wr, wi), out[12..23] = fast path, out[24] =
 // the permutation pattern the fast path recognised (-1: none, general code).

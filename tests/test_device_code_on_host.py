@@ -100,3 +100,12 @@ def test_fast_eigen_path_is_bitwise_general(shim, states):
         seen[int(out[24])] += 1
         assert np.array_equal(out[:12], out[12:24], equal_nan=True), (A, out)
     assert seen[1] > 100 and seen[0] > 0, seen
+
+
+def test_reciprocal_division_is_ieee_division(shim):
+    """div_by (the HLL star state's division through a shared reciprocal,
+    with Markstein's correction) equals the IEEE quotient bit for bit."""
+    shim.sh_div_check.restype = ctypes.c_longlong
+    shim.sh_div_check.argtypes = [ctypes.c_longlong, ctypes.c_int, ctypes.c_ulonglong]
+    assert shim.sh_div_check(20_000_000, 40, 12345) == 0
+    assert shim.sh_div_check(5_000_000, 300, 777) == 0
