@@ -281,7 +281,9 @@ template <int I, int K, int L> HQD int qr_window(double (&h)[36], double (&wr)[6
     double rt1r, rt1i, rt2r, rt2i;
     if (s == 0.0) { rt1r = rt1i = rt2r = rt2i = 0.0; }
     else {
-      h11 = h11 / s; h21 = h21 / s; h12 = h12 / s; h22 = h22 / s;
+      // four quotients by s through one reciprocal (div_by: bit-identical)
+      const double rs = 1.0 / s;
+      h11 = div_by(h11, s, rs); h21 = div_by(h21, s, rs); h12 = div_by(h12, s, rs); h22 = div_by(h22, s, rs);
       const double tr = (h11 + h22) / 2.0;
       const double det = (h11 - tr) * (h22 - tr) - h12 * h21;
       const double rtdisc = sqrt(fabs(det));
@@ -302,12 +304,14 @@ template <int I, int K, int L> HQD int qr_window(double (&h)[36], double (&wr)[6
       if (!stop && q >= lq) {
         double h21s = H6(q + 1, q);
         double s2 = fabs(H6(q, q) - rt2r) + fabs(rt2i) + fabs(h21s);
-        h21s = H6(q + 1, q) / s2;
-        v0 = h21s * H6(q, q + 1) + (H6(q, q) - rt1r) * ((H6(q, q) - rt2r) / s2) - rt1i * (rt2i / s2);
+        const double rs2 = 1.0 / s2;
+        h21s = div_by(H6(q + 1, q), s2, rs2);
+        v0 = h21s * H6(q, q + 1) + (H6(q, q) - rt1r) * div_by(H6(q, q) - rt2r, s2, rs2) - rt1i * div_by(rt2i, s2, rs2);
         v1 = h21s * (H6(q, q) + H6(q + 1, q + 1) - rt1r - rt2r);
         v2 = h21s * H6(q + 2, q + 1);
         s2 = fabs(v0) + fabs(v1) + fabs(v2);
-        v0 = v0 / s2; v1 = v1 / s2; v2 = v2 / s2;
+        const double rv = 1.0 / s2;
+        v0 = div_by(v0, s2, rv); v1 = div_by(v1, s2, rv); v2 = div_by(v2, s2, rv);
         m = q;
         if (q == lq) stop = true;
         else {
