@@ -38,6 +38,7 @@ B_ALG = 2 * 35 * 8  # bytes per cell-step: state read once, written once
 # The step's kernels in launch order (hyq_advance_timed slots) and their FP64
 # operations per cell from the same count (CFL: one max per cell; HLL: three
 # sweeps of 18 ops per moment plus the 4-op combination).
+E2E_SLABS = 8
 LAUNCHES_PER_STEP = 13  # the eleven timed kernels and the two correction passes of E2/E3
 KERNELS = ["A1_closure", "A2_eig_x", "A3_eig_y", "A4_eig_z", "A5_flux_speeds", "cfl", "hll",
            "E1_closure", "E2_eig_x", "E3_eig_y", "E4_closure_bgk"]
@@ -241,25 +242,22 @@ def run_gpu(args, rank, world, local_rank):
     s._chk(s._lib.hyq_advance_timed(s._h, ksteps, kms))
     kern = {k: kms[i] / ksteps for i, k in enumerate(KERNELS)}
 
-    # end to end through the public API: each step copies the host (pinned)
-    # state in, advances one step and reads the state back, on the same steps
-    # as the device-timed run (warm-up steps first, on the device)
+    # end to end through the public API: each step uploads the host state
+    # (pinned) and downloads the result (hyq_step_host, the copies overlapped
+    # slab by slab with the per-cell phases), on the same steps as the
+    # device-timed run (warm-up steps first, on the device)
     s.set_state(M0)
     s.advance(args.warmup)
-    Mh = torch.empty(35 * cells, dtype=torch.float64).pin_memory()
-    s._chk(s._lib.hyq_get_state(s._h, ctypes.c_void_p(Mh.data_ptr())))
-    st0 = s.stats()
-    tt, nn = st0["t"], st0["nn"]
+    Mh_flat = torch.empty(35 * cells, dtype=torch.float64).pin_memory()
+    Mh = Mh_flat.numpy().reshape(M0.shape, order="F")
+    s._chk(s._lib.hyq_get_state(s._h, ctypes.c_void_p(Mh_flat.data_ptr())))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        s._chk(s._lib.hyq_set_state(s._h, ctypes.c_void_p(Mh.data_ptr())))
-        s.set_clock(tt, nn)
-        tt, nn, _ = s.advance(1)
-        s._chk(s._lib.hyq_get_state(s._h, ctypes.c_void_p(Mh.data_ptr())))
+        s.step_host(Mh, nslabs=E2E_SLABS)
     e2e_s = time.perf_counter() - t0
-    e2e = {"value": world * cells * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": Mh.numel() * 8,
-           "d2h_bytes_per_step": Mh.numel() * 8}
+    e2e = {"value": world * cells * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": Mh_flat.numel() * 8,
+           "d2h_bytes_per_step": Mh_flat.numel() * 8, "api": f"hyq_step_host, {E2E_SLABS} slabs, pinned host state"}
     s.close()
     if rank != 0:
         if dist is not None:

@@ -189,6 +189,9 @@ struct hyq_ctx {
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // hyq_step_host: copy stream and per-slab events, made on first use
+  cudaStream_t cstream = nullptr;
+  std::vector<cudaEvent_t> up, down;
   std::string err;
 };
 
@@ -303,6 +306,10 @@ void hyq_destroy(hyq_ctx* ctx) {
   double* bufs[] = {ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax};
   for (double* b : bufs) if (b) cudaFree(b);
   if (ctx->clk) cudaFree(ctx->clk);
+  if (ctx->cstream) cudaStreamSynchronize(ctx->cstream);
+  for (cudaEvent_t e : ctx->up) cudaEventDestroy(e);
+  for (cudaEvent_t e : ctx->down) cudaEventDestroy(e);
+  if (ctx->cstream) cudaStreamDestroy(ctx->cstream);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -408,6 +415,59 @@ int hyq_advance(hyq_ctx* ctx, int64_t max_steps, double* t, int64_t* nn, int32_t
   if (r) return r;
   hyq_stats st;
   r = hyq_stats_get(ctx, &st);
+  if (r) return r;
+  if (t) *t = st.t;
+  if (nn) *nn = st.nn;
+  if (done) *done = st.done;
+  if (st.status > 0)
+    return fail(ctx, HYQ_ENONFINITE,
+                "non-finite CFL wave speed at step " + std::to_string(st.status) +
+                    " (a flux Jacobian with Inf/NaN entries; the reference's eigvals throws there)");
+  return HYQ_OK;
+}
+
+int hyq_step_host(hyq_ctx* ctx, const double* M_in, double* M_out, int32_t nslabs, double* t, int64_t* nn, int32_t* done) {
+  if (!ctx || !M_in || !M_out || nslabs < 1) return fail(ctx, HYQ_EINVAL, "bad argument");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  const long long N = ctx->N;
+  // slabs of whole 128-cell blocks (the per-block CFL maxima stay aligned)
+  const long long nblk = (N + BS_A - 1) / BS_A;
+  const int S = (int)((nslabs < nblk) ? nslabs : nblk);
+  if (!ctx->cstream) HQ_CHECK(ctx, cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking));
+  while ((int)ctx->up.size() < S) {
+    cudaEvent_t a, b;
+    HQ_CHECK(ctx, cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+    HQ_CHECK(ctx, cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+    ctx->up.push_back(a);
+    ctx->down.push_back(b);
+  }
+  std::vector<long long> cut(S + 1);
+  for (int k = 0; k <= S; ++k) cut[k] = (k == S) ? N : ((nblk * k) / S) * BS_A;
+  const size_t pitch = sizeof(double) * (size_t)N;
+  cudaStream_t s = ctx->stream, cs = ctx->cstream;
+  // upload slab k, then phase A on slab k while slab k+1 is uploading
+  for (int k = 0; k < S; ++k) {
+    const long long c0 = cut[k], c1 = cut[k + 1];
+    HQ_CHECK(ctx, cudaMemcpy2DAsync(ctx->M + c0, pitch, M_in + c0, pitch, sizeof(double) * (size_t)(c1 - c0), 35, cudaMemcpyHostToDevice, cs));
+    HQ_CHECK(ctx, cudaEventRecord(ctx->up[k], cs));
+    HQ_CHECK(ctx, cudaStreamWaitEvent(s, ctx->up[k], 0));
+    launch_phase_A(ctx->sc, ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s, nullptr, c0, c1);
+  }
+  // the CFL reduction and the HLL sweep need every cell
+  k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
+  k_hll<<<grid_of(N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
+  // phases E+F slab by slab, each slab downloaded as soon as it is done
+  for (int k = 0; k < S; ++k) {
+    const long long c0 = cut[k], c1 = cut[k + 1];
+    launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->clk, s, nullptr, c0, c1);
+    HQ_CHECK(ctx, cudaEventRecord(ctx->down[k], s));
+    HQ_CHECK(ctx, cudaStreamWaitEvent(cs, ctx->down[k], 0));
+    HQ_CHECK(ctx, cudaMemcpy2DAsync(M_out + c0, pitch, ctx->M + c0, pitch, sizeof(double) * (size_t)(c1 - c0), 35, cudaMemcpyDeviceToHost, cs));
+  }
+  HQ_CHECK(ctx, cudaGetLastError());
+  HQ_CHECK(ctx, cudaStreamSynchronize(cs));
+  hyq_stats st;
+  const int r = hyq_stats_get(ctx, &st);
   if (r) return r;
   if (t) *t = st.t;
   if (nn) *nn = st.nn;

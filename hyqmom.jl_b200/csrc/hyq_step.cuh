@@ -45,14 +45,15 @@ inline int grid_of(long long n, int bs) { return int((n + bs - 1) / bs); }
 // launch wrappers (defined in k_phase_A.cu, k_phase_EF.cu, k_cells.cu)
 // Phase [A] in place on M; Mtmp, Fx, Fy, Fz carry its intermediate states,
 // and on completion Fx, Fy, Fz hold the fluxes (Mtmp is left as scratch).
-// ev (optional): five events recorded after the five kernels.
+// ev (optional): five events recorded after the five kernels.  [c0, c1):
+// the cells to process (default all; c0 a multiple of BS_A).
 void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, double* Fy, double* Fz, double* vp, double* blockmax,
-                    const DevClock* clk, cudaStream_t s, cudaEvent_t* ev = nullptr);
+                    const DevClock* clk, cudaStream_t s, cudaEvent_t* ev = nullptr, long long c0 = 0, long long c1 = -1);
 // Phases [E]+[F] from Min to Mout; Fx, Fy, Fz are overwritten and vp (6N
 // doubles, dead after the HLL sweep) holds the correction lists.
 // ev (optional): four events recorded after E1, E2, E3 and E4.
 void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, double* Fx, double* Fy, double* Fz, double* vp,
-                     const DevClock* clk, cudaStream_t s, cudaEvent_t* ev = nullptr);
+                     const DevClock* clk, cudaStream_t s, cudaEvent_t* ev = nullptr, long long c0 = 0, long long c1 = -1);
 void launch_cells_phase_A(const double* M, long long n, int flag2D, double Ma, int positivity, double* Fx, double* Fy, double* Fz,
                           double* Mr, double* vp, cudaStream_t s);
 void launch_cells_flux(const double* M, long long n, int flag2D, double Ma, double* Fx, double* Fy, double* Fz, double* Mr, cudaStream_t s);

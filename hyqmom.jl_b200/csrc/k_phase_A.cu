@@ -42,19 +42,20 @@ __device__ __forceinline__ bool phase_A_active(const StepConst& sc, const DevClo
 
 // A1: Flux_closure35_and_realizable_3D (realized moments only)
 __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure(const double* __restrict__ M, double* __restrict__ out, const StepConst sc,
-                                                              const DevClock* clk) {
+                                                              const DevClock* clk, long long c0, long long c1) {
   if (!phase_A_active(sc, clk)) return;
-  const long long N = sc.N, c = (long long)blockIdx.x * BS_A + threadIdx.x;
-  if (c >= N) return;
+  const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
+  if (c >= c1) return;
   flux_closure35(M + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
 }
 
 // A2/A3: eigenvalues6_hyperbolic_3D along x (axis 1) or y (axis 2)
 __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* __restrict__ in, double* __restrict__ out, double* __restrict__ vlo,
-                                                         double* __restrict__ vhi, int axis, const StepConst sc, const DevClock* clk) {
+                                                         double* __restrict__ vhi, int axis, const StepConst sc, const DevClock* clk,
+                                                         long long c0, long long c1) {
   if (!phase_A_active(sc, clk)) return;
-  const long long N = sc.N, c = (long long)blockIdx.x * BS_A + threadIdx.x;
-  if (c >= N) return;
+  const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
+  if (c >= c1) return;
   double lo, hi;
   eigenvalues6(in + c, axis, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
   vlo[c] = lo; vhi[c] = hi;
@@ -62,10 +63,11 @@ __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* __restri
 
 // A4: eigenvalues6z_hyperbolic_3D
 __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A4_eigz(const double* __restrict__ in, double* __restrict__ out, double* __restrict__ vlo,
-                                                           double* __restrict__ vhi, const StepConst sc, const DevClock* clk) {
+                                                           double* __restrict__ vhi, const StepConst sc, const DevClock* clk,
+                                                           long long c0, long long c1) {
   if (!phase_A_active(sc, clk)) return;
-  const long long N = sc.N, c = (long long)blockIdx.x * BS_A + threadIdx.x;
-  if (c >= N) return;
+  const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
+  if (c >= c1) return;
   double lo, hi;
   eigenvalues6z(in + c, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out + c, N, N);
   vlo[c] = lo; vhi[c] = hi;
@@ -75,11 +77,12 @@ __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A4_eigz(const double* __rest
 // six wave speeds and the NaN-propagating block max of |speed|
 __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A5_flux(const double* __restrict__ in, double* __restrict__ M, double* __restrict__ Fx,
                                                            double* __restrict__ Fy, double* __restrict__ Fz, double* __restrict__ vp,
-                                                           double* __restrict__ blockmax, const StepConst sc, const DevClock* clk) {
+                                                           double* __restrict__ blockmax, const StepConst sc, const DevClock* clk,
+                                                           long long c0, long long c1) {
   if (!phase_A_active(sc, clk)) return;
-  const long long N = sc.N, c = (long long)blockIdx.x * BS_A + threadIdx.x;
+  const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
   double local = 0.0;
-  if (c < N) {
+  if (c < c1) {
     flux_closure35(in + c, sc.flag2D, sc.Ma, Fx + c, Fy + c, Fz + c, M + c, N, N, N);
     const double* mr = M + c;  // the realized moments this thread just wrote, stride N
     double v5[6];
@@ -95,7 +98,7 @@ __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A5_flux(const double* __
     }
   }
   const double bm = block_nanmax<BS_A>(local);
-  if (threadIdx.x == 0) blockmax[blockIdx.x] = bm;
+  if (threadIdx.x == 0) blockmax[c0 / BS_A + blockIdx.x] = bm;  // c0 is a multiple of BS_A
 }
 
 __global__ void __launch_bounds__(BS_CELLS) k_cells_phase_A(const double* __restrict__ M, long long n, int flag2D, double Ma, int positivity,
@@ -112,17 +115,19 @@ __global__ void __launch_bounds__(BS_CELLS) k_cells_phase_A(const double* __rest
 }  // namespace
 
 void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, double* Fy, double* Fz, double* vp, double* blockmax,
-                    const DevClock* clk, cudaStream_t s, cudaEvent_t* ev) {
+                    const DevClock* clk, cudaStream_t s, cudaEvent_t* ev, long long c0, long long c1) {
   const long long N = sc.N;
-  k_A1_closure<<<sc.nblocksA, BS_A, 0, s>>>(M, Fx, sc, clk);
+  if (c1 < 0) c1 = N;
+  const int g = grid_of(c1 - c0, BS_A);
+  k_A1_closure<<<g, BS_A, 0, s>>>(M, Fx, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
-  k_A_eig<<<sc.nblocksA, BS_A, 0, s>>>(Fx, Fy, vp, vp + N, 1, sc, clk);
+  k_A_eig<<<g, BS_A, 0, s>>>(Fx, Fy, vp, vp + N, 1, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[1], s);
-  k_A_eig<<<sc.nblocksA, BS_A, 0, s>>>(Fy, Fz, vp + 2 * N, vp + 3 * N, 2, sc, clk);
+  k_A_eig<<<g, BS_A, 0, s>>>(Fy, Fz, vp + 2 * N, vp + 3 * N, 2, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[2], s);
-  k_A4_eigz<<<sc.nblocksA, BS_A, 0, s>>>(Fz, Mtmp, vp + 4 * N, vp + 5 * N, sc, clk);
+  k_A4_eigz<<<g, BS_A, 0, s>>>(Fz, Mtmp, vp + 4 * N, vp + 5 * N, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[3], s);
-  k_A5_flux<<<sc.nblocksA, BS_A, 0, s>>>(Mtmp, M, Fx, Fy, Fz, vp, blockmax, sc, clk);
+  k_A5_flux<<<g, BS_A, 0, s>>>(Mtmp, M, Fx, Fy, Fz, vp, blockmax, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[4], s);
 }
 void launch_cells_phase_A(const double* M, long long n, int flag2D, double Ma, int positivity, double* Fx, double* Fy, double* Fz,

@@ -21,21 +21,21 @@ __device__ __forceinline__ unsigned int* fix_counters(double* vp, long long N) {
 
 // E1: Flux_closure35_and_realizable_3D; also resets the two fix counters
 __global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E1_closure(const double* __restrict__ in, double* __restrict__ out, double* vp,
-                                                                const StepConst sc, const DevClock* clk) {
+                                                                const StepConst sc, const DevClock* clk, long long c0, long long c1) {
   if (!clk->active) return;
-  const long long N = sc.N, c = (long long)blockIdx.x * BS_EF + threadIdx.x;
-  if (c == 0) { unsigned int* cnt = fix_counters(vp, N); cnt[0] = 0; cnt[1] = 0; }
-  if (c >= N) return;
+  const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
+  if (c == c0) { unsigned int* cnt = fix_counters(vp, N); cnt[0] = 0; cnt[1] = 0; }
+  if (c >= c1) return;
   flux_closure35(in + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
 }
 
 // E2/E3: eigenvalues6_hyperbolic_3D along x or y: copy, and list the cells
 // that need the correction (counter `which` of the two)
 __global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* __restrict__ in, double* __restrict__ out, double* vp, int axis,
-                                                           int which, const StepConst sc, const DevClock* clk) {
+                                                           int which, const StepConst sc, const DevClock* clk, long long c0, long long c1) {
   if (!clk->active) return;
-  const long long N = sc.N, c = (long long)blockIdx.x * BS_EF + threadIdx.x;
-  if (c >= N) return;
+  const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
+  if (c >= c1) return;
   const int planes = eigenvalues6_flags(in + c, axis, N);
 #pragma unroll
   for (int n = 0; n < 35; ++n) out[c + N * n] = in[c + N * n];
@@ -66,10 +66,10 @@ __global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E_fix(const double* __r
 
 // E4: Flux_closure35_and_realizable_3D, then collision35 with the step's dt
 __global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E4_closure_bgk(const double* __restrict__ in, double* __restrict__ Mout, const StepConst sc,
-                                                                    const DevClock* clk) {
+                                                                    const DevClock* clk, long long c0, long long c1) {
   if (!clk->active) return;
-  const long long N = sc.N, c = (long long)blockIdx.x * BS_EF + threadIdx.x;
-  if (c >= N) return;
+  const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
+  if (c >= c1) return;
   double a[35];
   flux_closure35(in + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, a, N, 1);
   collision35(a, clk->dt, sc.Kn, sc.positivity);
@@ -80,18 +80,19 @@ __global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E4_closure_bgk(const do
 }  // namespace
 
 void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, double* Fx, double* Fy, double* Fz, double* vp,
-                     const DevClock* clk, cudaStream_t s, cudaEvent_t* ev) {
-  const int g = grid_of(sc.N, BS_EF);
+                     const DevClock* clk, cudaStream_t s, cudaEvent_t* ev, long long c0, long long c1) {
+  if (c1 < 0) c1 = sc.N;
+  const int g = grid_of(c1 - c0, BS_EF);
   const int gfix = g < 148 * 8 ? g : 148 * 8;
-  k_E1_closure<<<g, BS_EF, 0, s>>>(Min, Fx, vp, sc, clk);
+  k_E1_closure<<<g, BS_EF, 0, s>>>(Min, Fx, vp, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
-  k_E_eig<<<g, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk);
+  k_E_eig<<<g, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk, c0, c1);
   k_E_fix<<<gfix, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk);
   if (ev) cudaEventRecord(ev[1], s);
-  k_E_eig<<<g, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk);
+  k_E_eig<<<g, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk, c0, c1);
   k_E_fix<<<gfix, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk);
   if (ev) cudaEventRecord(ev[2], s);
-  k_E4_closure_bgk<<<g, BS_EF, 0, s>>>(Fz, Mout, sc, clk);
+  k_E4_closure_bgk<<<g, BS_EF, 0, s>>>(Fz, Mout, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[3], s);
 }
 

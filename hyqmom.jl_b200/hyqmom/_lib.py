@@ -36,7 +36,7 @@ _lib = None
 # exported symbols (include/hyqmom.h)
 SYMBOLS = ["hyq_abi_version", "hyq_create", "hyq_destroy", "hyq_last_error", "hyq_set_state", "hyq_get_state",
            "hyq_set_state_device", "hyq_get_state_device", "hyq_set_clock", "hyq_advance", "hyq_advance_async",
-           "hyq_synchronize", "hyq_stats_get", "hyq_advance_timed", "hyq_get_SC", "hyq_stream", "hyq_cells_flux_closure",
+           "hyq_synchronize", "hyq_stats_get", "hyq_advance_timed", "hyq_step_host", "hyq_get_SC", "hyq_stream", "hyq_cells_flux_closure",
            "hyq_cells_eigenvalues", "hyq_cells_closure_eigs", "hyq_cells_collision", "hyq_cells_phase_A", "hyq_step_noalloc", "hyq_batch_create", "hyq_batch_destroy", "hyq_batch_size",
            "hyq_batch_member", "hyq_batch_stream", "hyq_batch_advance_async", "hyq_batch_advance"]
 NOALLOC_MAX_CELLS = 16384  # HYQ_NOALLOC_MAX_CELLS
@@ -65,6 +65,7 @@ def load(path=None):
     lib.hyq_advance_async.argtypes = [vp, i64]
     lib.hyq_synchronize.argtypes = [vp]
     lib.hyq_advance_timed.argtypes = [vp, i64, ctypes.POINTER(ctypes.c_float)]
+    lib.hyq_step_host.argtypes = [vp, vp, vp, i32, dp, ctypes.POINTER(i64), ctypes.POINTER(i32)]
     lib.hyq_stats_get.argtypes = [vp, ctypes.POINTER(HyqStats)]
     lib.hyq_get_SC.argtypes = [vp, vp, vp]
     lib.hyq_stream.argtypes = [vp]

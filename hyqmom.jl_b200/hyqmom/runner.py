@@ -97,6 +97,20 @@ class Solver:
     def advance_async(self, max_steps):
         self._chk(self._lib.hyq_advance_async(self._h, int(max_steps)))
 
+    def step_host(self, M_in, M_out=None, nslabs=8):
+        """One step on a host state (Fortran-ordered (Nx,Ny,Nz,35) float64),
+        the copies overlapped with the per-cell phases; returns (t, nn, done).
+        M_out defaults to M_in (updated in place)."""
+        M_out = M_in if M_out is None else M_out
+        for a in (M_in, M_out):
+            assert a.shape == self.shape and a.dtype == np.float64 and a.flags["F_CONTIGUOUS"]
+        t = ctypes.c_double()
+        nn = ctypes.c_int64()
+        done = ctypes.c_int32()
+        self._chk(self._lib.hyq_step_host(self._h, M_in.ctypes.data, M_out.ctypes.data, int(nslabs), ctypes.byref(t),
+                                          ctypes.byref(nn), ctypes.byref(done)))
+        return t.value, nn.value, bool(done.value)
+
     def synchronize(self):
         self._chk(self._lib.hyq_synchronize(self._h))
 

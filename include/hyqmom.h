@@ -81,6 +81,17 @@ int hyq_advance_async(hyq_ctx* ctx, int64_t max_steps);
 int hyq_synchronize(hyq_ctx* ctx);
 int hyq_stats_get(hyq_ctx* ctx, hyq_stats* out);
 
+/* One step of the reference loop on a host state, the host<->device copies
+ * overlapped with the per-cell phases: the state goes up in `nslabs` chunks
+ * of whole z-planes' cells while phase [A] runs on the chunks already there,
+ * and comes back chunk by chunk as phases [E]+[F] finish them (the CFL
+ * reduction and the HLL sweep need every cell and run in between).  M_in and
+ * M_out are host (Nx,Ny,Nz,35) column-major buffers and may be the same; in
+ * pinned memory the copies run asynchronously.  The step uses the context's
+ * clock (t, nn) like hyq_advance(ctx, 1, ...), with the same outputs and
+ * return codes; the device state is left equal to M_out. */
+int hyq_step_host(hyq_ctx* ctx, const double* M_in, double* M_out, int32_t nslabs, double* t, int64_t* nn, int32_t* done);
+
 /* Standardized and central moment fields of the current state, host
  * (Nx,Ny,Nz,35) buffers (either may be NULL). */
 int hyq_get_SC(hyq_ctx* ctx, double* S, double* C);
