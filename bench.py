@@ -38,7 +38,7 @@ B_ALG = 2 * 35 * 8  # bytes per cell-step: state read once, written once
 # The step's kernels in launch order (hyq_advance_timed slots) and their FP64
 # operations per cell from the same count (CFL: one max per cell; HLL: three
 # sweeps of 18 ops per moment plus the 4-op combination).
-E2E_SLABS = 8
+E2E_SLABS = 4
 LAUNCHES_PER_STEP = 13  # the eleven timed kernels and the two correction passes of E2/E3
 KERNELS = ["A1_closure", "A2_eig_x", "A3_eig_y", "A4_eig_z", "A5_flux_speeds", "cfl", "hll",
            "E1_closure", "E2_eig_x", "E3_eig_y", "E4_closure_bgk"]
