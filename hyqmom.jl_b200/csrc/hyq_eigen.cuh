@@ -345,12 +345,13 @@ HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
 namespace hyq {
 
 // eig_real<6> of a flux Jacobian: the register-resident path (hyq_eig6.cuh)
-// when dgebal's search isolates columns 0 and 5, else the general code;
-// identical results either way.
+// when dgebal's search isolates columns 0 and 5 (pattern 1, the usual case on
+// smooth states), else the general code; identical results either way.  No
+// isolation at all (pattern 0: round-off-sized entries in the first column,
+// common once the flow has developed) also goes to the general code: an
+// unrolled register path for it made the step kernels slower through its
+// code size, even in a pass over only such cells.
 HQD void eig_real_jac(double (&h)[36], double (&wr)[6], double (&wi)[6]) {
-  // only the usual permutation takes the register path: instantiating the
-  // unpermuted case too (3 % of the Jacobians) made the kernels slower
-  // through the larger code
   if (e6::pattern(h) != 1) {
     double J[6][6];
 #pragma unroll
@@ -366,10 +367,23 @@ HQD void eig_real_jac(double (&h)[36], double (&wr)[6], double (&wi)[6]) {
   e6::solve<2>(h, wr, wi);
 }
 
+// Pattern 1 only: false (nothing computed) for any other permutation, whose
+// Jacobians the step kernels leave to a separate pass over listed cells.
+HQD bool eig_real_jac_p1(double (&h)[36], double (&wr)[6], double (&wi)[6]) {
+  if (e6::pattern(h) != 1) return false;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) { wr[i] = 0.0; wi[i] = 0.0; }
+  e6::apply_pattern1(h);
+  e6::solve<2>(h, wr, wi);
+  return true;
+}
+
 // compute_jacobian_eigenvalues for one 15-moment slice: extreme real parts
 // and max |imag|.  A non-finite Jacobian gives NaN (the reference's guard).
-struct EigOut { double vmin, vmax, imax; };
-HQN EigOut jac_eigs(const double* ma) {
+// FAST: pattern-1 Jacobians only; any other sets `deferred` and leaves the
+// rest unset.
+struct EigOut { double vmin, vmax, imax; bool deferred; };
+template <bool FAST> HQN EigOut jac_eigs_t(const double* ma) {
   double r3[6], r5[6], r6[6];
   jacobian6_rows(ma, r3, r5, r6);
   double h[36];  // the Jacobian, row-major, held in registers
@@ -383,9 +397,14 @@ HQN EigOut jac_eigs(const double* ma) {
     fin = fin && isfinite(r3[j]) && isfinite(r5[j]) && isfinite(r6[j]);
   }
   EigOut o;
+  o.deferred = false;
   if (!fin) { o.vmin = qnan(); o.vmax = qnan(); o.imax = qnan(); return o; }
   double wr[6], wi[6];
-  eig_real_jac(h, wr, wi);
+  if (FAST) {
+    if (!eig_real_jac_p1(h, wr, wi)) { o.deferred = true; return o; }
+  } else {
+    eig_real_jac(h, wr, wi);
+  }
   // sort(real) with NaN last, first and last
   double mn = wr[0], mx = wr[0];
   bool anynan = (wr[0] != wr[0]);
@@ -403,6 +422,7 @@ HQN EigOut jac_eigs(const double* ma) {
   o.imax = im;
   return o;
 }
+HQD EigOut jac_eigs(const double* ma) { return jac_eigs_t<false>(ma); }
 
 // axis_moment_slice (src/utils/axis_moment_slice.jl:31-54), 0-based
 __device__ constexpr int SLICE[4][15] = {{0, 5, 9, 12, 14, 1, 6, 10, 13, 2, 7, 11, 3, 8, 4},
@@ -457,13 +477,16 @@ HQN void correct_for_real(const double* M, int pa_i, int pa_j, int pb_i, int pb_
 // eigenvalues6_hyperbolic_3D for axis 1 (x) or 2 (y).
 // Moment n is read from M[n * ist] and written to Mr[n * ost] (the step
 // kernels pass the cell's entry of the moment-major fields, stride N); M and
-// Mr must not overlap.
-HQN void eigenvalues6(const double* M, int axis, int flag2D, double Ma, double& vmin, double& vmax, double* Mr, long long ist = 1,
-                      long long ost = 1) {
+// Mr must not overlap.  FAST: returns true, with vmin, vmax and Mr not (or not
+// all) written, when a Jacobian needs the code outside the pattern-1 path.
+template <bool FAST>
+HQN bool eigenvalues6_t(const double* M, int axis, int flag2D, double Ma, double& vmin, double& vmax, double* Mr, long long ist,
+                        long long ost) {
   const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
   double a[15], b[15];
   for (int n = 0; n < 15; ++n) { a[n] = M[SLICE[sa][n] * ist]; b[n] = M[SLICE[sb][n] * ist]; }
-  EigOut ea = jac_eigs(a), eb = jac_eigs(b);
+  EigOut ea = jac_eigs_t<FAST>(a), eb = jac_eigs_t<FAST>(b);
+  if (FAST && (ea.deferred || eb.deferred)) return true;
   auto combine = [&]() {
     vmin = ea.vmin; vmax = ea.vmax;
     if (eb.vmin == eb.vmin || eb.vmax == eb.vmax) { vmin = jmin(vmin, eb.vmin); vmax = jmax(vmax, eb.vmax); }
@@ -479,28 +502,37 @@ HQN void eigenvalues6(const double* M, int axis, int flag2D, double Ma, double& 
     // pair a is always the UV plane; pair b is UW (x) or VW (y)
     correct_for_real(Ml, 0, 1, axis == 1 ? 0 : 1, 2, (ca ? 1 : 0) | (cb ? 2 : 0), flag2D, Ma, Mc);
     for (int n = 0; n < 15; ++n) { a[n] = Mc[SLICE[sa][n]]; b[n] = Mc[SLICE[sb][n]]; }
-    ea = jac_eigs(a); eb = jac_eigs(b);
+    ea = jac_eigs_t<FAST>(a); eb = jac_eigs_t<FAST>(b);
+    if (FAST && (ea.deferred || eb.deferred)) return true;
     combine();
     for (int n = 0; n < 35; ++n) Mr[n * ost] = Mc[n];
   }
+  return false;
+}
+HQD void eigenvalues6(const double* M, int axis, int flag2D, double Ma, double& vmin, double& vmax, double* Mr, long long ist = 1,
+                      long long ost = 1) {
+  eigenvalues6_t<false>(M, axis, flag2D, Ma, vmin, vmax, Mr, ist, ost);
 }
 
 // Which of eigenvalues6's two planes need the complex-eigenvalue correction
 // (bit 0: first slice, bit 1: second), from the same Jacobians and the same
 // test; phase E only needs the corrected moments, so its kernels decide here
 // and leave the corrections to a separate pass over the flagged cells.
-HQN int eigenvalues6_flags(const double* M, int axis, long long ist) {
+// FAST: -1 when a Jacobian needs the code outside the pattern-1 path.
+template <bool FAST> HQN int eigenvalues6_flags_t(const double* M, int axis, long long ist) {
   const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
   double a[15], b[15];
   for (int n = 0; n < 15; ++n) { a[n] = M[SLICE[sa][n] * ist]; b[n] = M[SLICE[sb][n] * ist]; }
-  const EigOut ea = jac_eigs(a), eb = jac_eigs(b);
+  const EigOut ea = jac_eigs_t<FAST>(a), eb = jac_eigs_t<FAST>(b);
+  if (FAST && (ea.deferred || eb.deferred)) return -1;
   const double thr = 1000.0 * EPS;
   return (ea.imax > thr ? 1 : 0) | (eb.imax > thr ? 2 : 0);
 }
 
-// eigenvalues6z_hyperbolic_3D (strides as eigenvalues6)
-HQN void eigenvalues6z(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr, long long ist = 1,
-                       long long ost = 1) {
+// eigenvalues6z_hyperbolic_3D (strides and FAST as eigenvalues6_t)
+template <bool FAST>
+HQN bool eigenvalues6z_t(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr, long long ist,
+                         long long ost) {
   double Mw[35];
 #pragma unroll
   for (int n = 0; n < 35; ++n) Mw[n] = M[n * ist];
@@ -519,7 +551,8 @@ HQN void eigenvalues6z(const double* M, int flag2D, double Ma, int positivity, d
   for (int n = 0; n < 35; ++n) Mr[n * ost] = Mw[n];
   double a[15], b[15];
   for (int n = 0; n < 15; ++n) { a[n] = Mw[WUI[n]]; b[n] = Mw[SLICE[3][n]]; }
-  EigOut ea = jac_eigs(a), eb = jac_eigs(b);
+  EigOut ea = jac_eigs_t<FAST>(a), eb = jac_eigs_t<FAST>(b);
+  if (FAST && (ea.deferred || eb.deferred)) return true;
   vmin = jmin(ea.vmin, eb.vmin);
   vmax = jmax(ea.vmax, eb.vmax);
   const double thr = 1000.0 * EPS;
@@ -529,11 +562,17 @@ HQN void eigenvalues6z(const double* M, int flag2D, double Ma, int positivity, d
     for (int n = 0; n < 35; ++n) Ml[n] = M[n * ist];
     correct_for_real(Ml, 0, 2, 1, 2, (ca ? 1 : 0) | (cb ? 2 : 0), flag2D, Ma, Mc);
     for (int n = 0; n < 15; ++n) { a[n] = Mc[WUI[n]]; b[n] = Mc[SLICE[3][n]]; }
-    ea = jac_eigs(a); eb = jac_eigs(b);
+    ea = jac_eigs_t<FAST>(a); eb = jac_eigs_t<FAST>(b);
+    if (FAST && (ea.deferred || eb.deferred)) return true;
     vmin = jmin(ea.vmin, eb.vmin);
     vmax = jmax(ea.vmax, eb.vmax);
     for (int n = 0; n < 35; ++n) Mr[n * ost] = Mc[n];
   }
+  return false;
+}
+HQD void eigenvalues6z(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr, long long ist = 1,
+                       long long ost = 1) {
+  eigenvalues6z_t<false>(M, flag2D, Ma, positivity, vmin, vmax, Mr, ist, ost);
 }
 
 // closure_and_eigenvalues with N = 2: extreme eigenvalues of the 3x3 Jacobi

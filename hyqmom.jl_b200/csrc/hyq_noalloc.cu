@@ -9,8 +9,9 @@
 // context; this entry point instead uses one fixed scratch array that is part
 // of the library's device image, so no call allocates.
 //
-// The scratch array holds the fluxes, the realized state, the wave speeds,
-// the per-block maxima and the device clock of ONE step of at most
+// The scratch array holds the fluxes, the realized state, the wave speeds
+// with the step's lists of cells left to a second pass, the per-block maxima
+// and the device clock of ONE step of at most
 // HYQ_NOALLOC_MAX_CELLS cells.  Every call on a device shares it: calls that
 // overlap on one device (two host threads, or two streams without ordering
 // between them) race on the scratch and give wrong results.  Nothing in it
@@ -36,8 +37,8 @@ constexpr long long kMax = HYQ_NOALLOC_MAX_CELLS;
 constexpr long long kClock = 0;                                   // DevClock (<= 256 B)
 constexpr long long kBlockmax = 32;                               // ceil(kMax / BS_A) maxima
 constexpr long long kBlockmaxLen = ((kMax + BS_A - 1) / BS_A + 31) / 32 * 32;
-constexpr long long kVp = kBlockmax + kBlockmaxLen;               // 6 * kMax wave speeds
-constexpr long long kFx = kVp + 6 * kMax;                         // 35 * kMax each
+constexpr long long kVp = kBlockmax + kBlockmaxLen;               // 6 * kMax wave speeds + cell lists
+constexpr long long kFx = kVp + 7 * kMax + 32;                    // 35 * kMax each
 constexpr long long kFy = kFx + 35 * kMax;
 constexpr long long kFz = kFy + 35 * kMax;
 constexpr long long kMtmp = kFz + 35 * kMax;

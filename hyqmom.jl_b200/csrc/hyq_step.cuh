@@ -32,8 +32,19 @@ struct StepConst {
 #ifndef HQ_MINB_EIG
 #define HQ_MINB_EIG 8
 #endif
+// The passes over listed cells (complete eigen-solve, corrections) run at the
+// eigenvalue kernels' occupancy (fewer resident blocks with more registers
+// were slower), a grid of FIX_BLOCKS blocks striding over the list.
+#ifndef HQ_MINB_FIX
+#define HQ_MINB_FIX 8
+#endif
+#ifndef HQ_FIX_BLOCKS
+#define HQ_FIX_BLOCKS (148 * 8)
+#endif
 constexpr int MINB_CLOSURE = HQ_MINB_CLOSURE;
 constexpr int MINB_EIG = HQ_MINB_EIG;
+constexpr int MINB_FIX = HQ_MINB_FIX;
+constexpr int FIX_BLOCKS = HQ_FIX_BLOCKS;
 
 constexpr int BS_A = 128;
 constexpr int BS_EF = 128;
@@ -45,7 +56,9 @@ inline int grid_of(long long n, int bs) { return int((n + bs - 1) / bs); }
 // launch wrappers (defined in k_phase_A.cu, k_phase_EF.cu, k_cells.cu)
 // Phase [A] in place on M; Mtmp, Fx, Fy, Fz carry its intermediate states,
 // and on completion Fx, Fy, Fz hold the fluxes (Mtmp is left as scratch).
-// ev (optional): five events recorded after the five kernels.  [c0, c1):
+// vp: 7N + 2 doubles, the six wave-speed arrays and the list of cells left
+// to the complete eigen-solve.  ev (optional): five events recorded after
+// A1, A2, A3, A4 (each with its pass over listed cells) and A5.  [c0, c1):
 // the cells to process (default all; c0 a multiple of BS_A).
 void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, double* Fy, double* Fz, double* vp, double* blockmax,
                     const DevClock* clk, cudaStream_t s, cudaEvent_t* ev = nullptr, long long c0 = 0, long long c1 = -1);

@@ -36,41 +36,63 @@ __device__ __noinline__ void cell_phase_A(const double* m, int flag2D, double Ma
 // instruction fetch); the intermediate states go through buffers that are
 // dead during phase A:  M -A1-> Fx -A2-> Fy -A3-> Fz -A4-> Mtmp -A5-> M, with
 // the Jacobian speeds of A2-A4 parked in vp and combined in A5.
+// The eigenvalue kernels A2-A4 solve only Jacobians of the usual permutation
+// (pattern 1) in their 64-register code and list the cells with any other
+// Jacobian; k_A_fix then runs the complete eigenvalue function on the listed
+// cells, densely packed into warps and with the registers the full 6 x 6
+// eigen-solve needs.  The list lives in vp[6N..7N) (cell indices as unsigned
+// ints, three counters after the first N of them), one list per kernel in
+// turn.
 __device__ __forceinline__ bool phase_A_active(const StepConst& sc, const DevClock* clk) {
   return (clk->t < sc.tmax) && (clk->nn < sc.nnmax);
 }
+__device__ __forceinline__ unsigned int* defer_list(double* vp, long long N) { return reinterpret_cast<unsigned int*>(vp + 6 * N); }
 
-// A1: Flux_closure35_and_realizable_3D (realized moments only)
-__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure(const double* __restrict__ M, double* __restrict__ out, const StepConst sc,
-                                                              const DevClock* clk, long long c0, long long c1) {
+// A1: Flux_closure35_and_realizable_3D (realized moments only); also resets
+// the three deferral counters
+__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure(const double* __restrict__ M, double* __restrict__ out, double* vp,
+                                                              const StepConst sc, const DevClock* clk, long long c0, long long c1) {
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
+  if (c == c0) { unsigned int* cnt = defer_list(vp, N) + N; cnt[0] = 0; cnt[1] = 0; cnt[2] = 0; }
   if (c >= c1) return;
   flux_closure35(M + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
 }
 
-// A2/A3: eigenvalues6_hyperbolic_3D along x (axis 1) or y (axis 2)
-__global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* __restrict__ in, double* __restrict__ out, double* __restrict__ vlo,
-                                                         double* __restrict__ vhi, int axis, const StepConst sc, const DevClock* clk,
-                                                         long long c0, long long c1) {
+// A2/A3: eigenvalues6_hyperbolic_3D along x (axis 1) or y (axis 2); A4
+// (axis 3): eigenvalues6z_hyperbolic_3D.  Deferred cells go to list `axis - 1`.
+__global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* __restrict__ in, double* __restrict__ out, double* vp,
+                                                         int axis, const StepConst sc, const DevClock* clk, long long c0, long long c1) {
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
   if (c >= c1) return;
   double lo, hi;
-  eigenvalues6(in + c, axis, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
-  vlo[c] = lo; vhi[c] = hi;
+  const bool deferred = axis == 3 ? eigenvalues6z_t<true>(in + c, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out + c, N, N)
+                                  : eigenvalues6_t<true>(in + c, axis, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
+  if (deferred) {
+    unsigned int* list = defer_list(vp, N);
+    list[atomicAdd(list + N + (axis - 1), 1u)] = (unsigned int)c;
+  } else {
+    double* v = vp + 2 * (axis - 1) * N;
+    v[c] = lo; v[c + N] = hi;
+  }
 }
 
-// A4: eigenvalues6z_hyperbolic_3D
-__global__ void __launch_bounds__(BS_A, MINB_EIG) k_A4_eigz(const double* __restrict__ in, double* __restrict__ out, double* __restrict__ vlo,
-                                                           double* __restrict__ vhi, const StepConst sc, const DevClock* clk,
-                                                           long long c0, long long c1) {
+// The listed cells of k_A_eig, grid-stride over the list
+__global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* __restrict__ in, double* __restrict__ out, double* vp, int axis,
+                                                         const StepConst sc, const DevClock* clk) {
   if (!phase_A_active(sc, clk)) return;
-  const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
-  if (c >= c1) return;
-  double lo, hi;
-  eigenvalues6z(in + c, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out + c, N, N);
-  vlo[c] = lo; vhi[c] = hi;
+  const long long N = sc.N;
+  const unsigned int* list = defer_list(vp, N);
+  const unsigned int count = list[N + (axis - 1)];
+  double* v = vp + 2 * (axis - 1) * N;
+  for (unsigned int e = blockIdx.x * BS_A + threadIdx.x; e < count; e += gridDim.x * BS_A) {
+    const long long c = list[e];
+    double lo, hi;
+    if (axis == 3) eigenvalues6z_t<false>(in + c, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out + c, N, N);
+    else eigenvalues6_t<false>(in + c, axis, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
+    v[c] = lo; v[c + N] = hi;
+  }
 }
 
 // A5: closure of the realized moments with fluxes, 1-D closure speeds, the
@@ -119,13 +141,17 @@ void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, do
   const long long N = sc.N;
   if (c1 < 0) c1 = N;
   const int g = grid_of(c1 - c0, BS_A);
-  k_A1_closure<<<g, BS_A, 0, s>>>(M, Fx, sc, clk, c0, c1);
+  const int gfix = g < FIX_BLOCKS ? g : FIX_BLOCKS;
+  k_A1_closure<<<g, BS_A, 0, s>>>(M, Fx, vp, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
-  k_A_eig<<<g, BS_A, 0, s>>>(Fx, Fy, vp, vp + N, 1, sc, clk, c0, c1);
+  k_A_eig<<<g, BS_A, 0, s>>>(Fx, Fy, vp, 1, sc, clk, c0, c1);
+  k_A_fix<<<gfix, BS_A, 0, s>>>(Fx, Fy, vp, 1, sc, clk);
   if (ev) cudaEventRecord(ev[1], s);
-  k_A_eig<<<g, BS_A, 0, s>>>(Fy, Fz, vp + 2 * N, vp + 3 * N, 2, sc, clk, c0, c1);
+  k_A_eig<<<g, BS_A, 0, s>>>(Fy, Fz, vp, 2, sc, clk, c0, c1);
+  k_A_fix<<<gfix, BS_A, 0, s>>>(Fy, Fz, vp, 2, sc, clk);
   if (ev) cudaEventRecord(ev[2], s);
-  k_A4_eigz<<<g, BS_A, 0, s>>>(Fz, Mtmp, vp + 4 * N, vp + 5 * N, sc, clk, c0, c1);
+  k_A_eig<<<g, BS_A, 0, s>>>(Fz, Mtmp, vp, 3, sc, clk, c0, c1);
+  k_A_fix<<<gfix, BS_A, 0, s>>>(Fz, Mtmp, vp, 3, sc, clk);
   if (ev) cudaEventRecord(ev[3], s);
   k_A5_flux<<<g, BS_A, 0, s>>>(Mtmp, M, Fx, Fy, Fz, vp, blockmax, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[4], s);

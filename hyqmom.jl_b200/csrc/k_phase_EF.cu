@@ -13,10 +13,12 @@ namespace {
 // intermediate states go through the flux buffers, dead after the HLL sweep:
 //   Mtmp -E1-> Fx -E2-> Fy -E3-> Fz -E4-> M.
 // E2/E3 copy the moments and list the cells whose Jacobians have complex
-// eigenvalues; k_E_fix then corrects only those cells, so that a few such
-// cells no longer hold every lane of their warps in the correction.  The
-// lists live in the wave-speed buffer vp, dead after the HLL sweep
-// (vp[0..N): entries (cell << 2) | planes; two counters after them).
+// eigenvalues, and the cells with a Jacobian outside the usual permutation
+// (pattern 1, the only one their 64-register code solves); k_E_fix then
+// decides and corrects only those cells, so that a few such cells no longer
+// hold every lane of their warps.  The lists live in the wave-speed buffer
+// vp, dead after the HLL sweep (vp[0..N): entries (cell << 2) | planes,
+// planes = 0 for a cell still to be decided; two counters after them).
 __device__ __forceinline__ unsigned int* fix_counters(double* vp, long long N) { return reinterpret_cast<unsigned int*>(vp + N); }
 
 // E1: Flux_closure35_and_realizable_3D; also resets the two fix counters
@@ -30,25 +32,27 @@ __global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E1_closure(const double
 }
 
 // E2/E3: eigenvalues6_hyperbolic_3D along x or y: copy, and list the cells
-// that need the correction (counter `which` of the two)
+// that need the correction or the complete eigen-solve (counter `which`)
 __global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* __restrict__ in, double* __restrict__ out, double* vp, int axis,
                                                            int which, const StepConst sc, const DevClock* clk, long long c0, long long c1) {
   if (!clk->active) return;
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
   if (c >= c1) return;
-  const int planes = eigenvalues6_flags(in + c, axis, N);
+  const int planes = eigenvalues6_flags_t<true>(in + c, axis, N);
 #pragma unroll
   for (int n = 0; n < 35; ++n) out[c + N * n] = in[c + N * n];
   if (planes) {
     const unsigned int slot = atomicAdd(fix_counters(vp, N) + which, 1u);
-    reinterpret_cast<unsigned long long*>(vp)[slot] = ((unsigned long long)c << 2) | (unsigned long long)planes;
+    reinterpret_cast<unsigned long long*>(vp)[slot] = ((unsigned long long)c << 2) | (unsigned long long)(planes < 0 ? 0 : planes);
   }
 }
 
-// The correction of the listed cells (correct_moments_for_real_eigenvalues,
-// as in eigenvalues6), grid-stride over the list
-__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E_fix(const double* __restrict__ in, double* __restrict__ out, const double* vp,
-                                                               int axis, int which, const StepConst sc, const DevClock* clk) {
+// The listed cells: the planes from the complete eigen-solve where k_E_eig
+// left them undecided, then the correction
+// (correct_moments_for_real_eigenvalues, as in eigenvalues6); grid-stride
+// over the list
+__global__ void __launch_bounds__(BS_EF, MINB_FIX) k_E_fix(const double* __restrict__ in, double* __restrict__ out, const double* vp,
+                                                           int axis, int which, const StepConst sc, const DevClock* clk) {
   if (!clk->active) return;
   const long long N = sc.N;
   const unsigned int count = reinterpret_cast<const unsigned int*>(vp + N)[which];
@@ -56,7 +60,9 @@ __global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E_fix(const double* __r
   for (unsigned int e = blockIdx.x * BS_EF + threadIdx.x; e < count; e += gridDim.x * BS_EF) {
     const unsigned long long v = list[e];
     const long long c = (long long)(v >> 2);
-    const int planes = int(v & 3ull);
+    int planes = int(v & 3ull);
+    if (planes == 0) planes = eigenvalues6_flags_t<false>(in + c, axis, N);
+    if (planes == 0) continue;
     double Ml[35], Mc[35];
     for (int n = 0; n < 35; ++n) Ml[n] = in[c + N * n];
     correct_for_real(Ml, 0, 1, axis == 1 ? 0 : 1, 2, planes, sc.flag2D, sc.Ma, Mc);
@@ -83,7 +89,7 @@ void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, doubl
                      const DevClock* clk, cudaStream_t s, cudaEvent_t* ev, long long c0, long long c1) {
   if (c1 < 0) c1 = sc.N;
   const int g = grid_of(c1 - c0, BS_EF);
-  const int gfix = g < 148 * 8 ? g : 148 * 8;
+  const int gfix = g < FIX_BLOCKS ? g : FIX_BLOCKS;
   k_E1_closure<<<g, BS_EF, 0, s>>>(Min, Fx, vp, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
   k_E_eig<<<g, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk, c0, c1);

@@ -102,10 +102,11 @@ void* hyq_stream(hyq_ctx* ctx);
 /* Run `steps` steps launching the step kernels individually (not the graph)
  * with CUDA events around each on the context stream; ms[HYQ_TIMED_SLOTS]
  * receives the summed device time of each kernel, in launch order:
- * A1 closure, A2 x eigenvalues, A3 y eigenvalues, A4 z eigenvalues,
+ * A1 closure, A2 x eigenvalues, A3 y eigenvalues, A4 z eigenvalues (each
+ * with its pass over the cells it left to the complete eigen-solve),
  * A5 closure with fluxes and speeds, CFL reduction, HLL sweep,
  * E1 closure, E2 x eigenvalues, E3 y eigenvalues (each with its pass that
- * corrects the listed cells), E4 closure + BGK.
+ * decides and corrects the listed cells), E4 closure + BGK.
  * For profiling; results equal hyq_advance. */
 #define HYQ_TIMED_SLOTS 11
 int hyq_advance_timed(hyq_ctx* ctx, int64_t steps, float* ms);
