@@ -124,33 +124,45 @@ HQD void dlanv2(double a, double b, double c, double d, double& rt1r, double& rt
   else { rt1i = sqrt(fabs(b)) * sqrt(fabs(c)); rt2i = -rt1i; }
 }
 
+// Loops of the general eigen-solve below stay rolled on the device: its
+// passes over listed cells wait mostly on instruction fetch, and the compact
+// code made them 1.3x faster on late crossing-jet states than the unrolled.
+#ifndef HQ_GEN_ROLLED
+#define HQ_GEN_ROLLED 1
+#endif
+#if defined(__CUDACC__) && HQ_GEN_ROLLED
+#define HQ_ROLLED _Pragma("unroll 1")
+#else
+#define HQ_ROLLED
+#endif
+
 // Eigenvalues of the N x N row-major matrix A (overwritten).  Returns 0 on
 // success, > 0 when the QR iteration limit was reached.
 template <int N>
 HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
-  for (int i = 0; i < N; ++i) { wr[i] = 0.0; wi[i] = 0.0; }
+  HQ_ROLLED for (int i = 0; i < N; ++i) { wr[i] = 0.0; wi[i] = 0.0; }
   int k = 0, l = N - 1;
   auto swapij = [&](int j, int m) {
     if (j == m) return;
-    for (int r = 0; r <= l; ++r) { const double t = A[r][j]; A[r][j] = A[r][m]; A[r][m] = t; }
-    for (int c = k; c < N; ++c) { const double t = A[j][c]; A[j][c] = A[m][c]; A[m][c] = t; }
+    HQ_ROLLED for (int r = 0; r <= l; ++r) { const double t = A[r][j]; A[r][j] = A[r][m]; A[r][m] = t; }
+    HQ_ROLLED for (int c = k; c < N; ++c) { const double t = A[j][c]; A[j][c] = A[m][c]; A[m][c] = t; }
   };
   bool found = true;
   while (found && l >= 0) {
     found = false;
     if (l == 0) break;
-    for (int j = l; j >= 0; --j) {
+    HQ_ROLLED for (int j = l; j >= 0; --j) {
       bool zero = true;
-      for (int i = 0; i <= l; ++i) { if (i == j) continue; if (A[j][i] != 0.0) { zero = false; break; } }
+      HQ_ROLLED for (int i = 0; i <= l; ++i) { if (i == j) continue; if (A[j][i] != 0.0) { zero = false; break; } }
       if (zero) { swapij(j, l); --l; found = true; break; }
     }
   }
   found = true;
   while (found) {
     found = false;
-    for (int j = k; j <= l; ++j) {
+    HQ_ROLLED for (int j = k; j <= l; ++j) {
       bool zero = true;
-      for (int i = k; i <= l; ++i) { if (i == j) continue; if (A[i][j] != 0.0) { zero = false; break; } }
+      HQ_ROLLED for (int i = k; i <= l; ++i) { if (i == j) continue; if (A[i][j] != 0.0) { zero = false; break; } }
       if (zero) { swapij(j, k); ++k; found = true; break; }
     }
   }
@@ -158,28 +170,28 @@ HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
     const double radix = 2.0, factor = 0.95;
     const double sfmin1 = SAFMIN / ULP, sfmax1 = 1.0 / sfmin1, sfmin2 = sfmin1 * radix, sfmax2 = 1.0 / sfmin2;
     double scal[N];
-    for (int i = 0; i < N; ++i) scal[i] = 1.0;
+    HQ_ROLLED for (int i = 0; i < N; ++i) scal[i] = 1.0;
     bool noconv = true;
     int guard = 0;
     while (noconv && guard++ < 1000) {
       noconv = false;
-      for (int i = k; i <= l; ++i) {
+      HQ_ROLLED for (int i = k; i <= l; ++i) {
         double col[N], row[N];
-        for (int r = k; r <= l; ++r) col[r - k] = A[r][i];
-        for (int c2 = k; c2 <= l; ++c2) row[c2 - k] = A[i][c2];
+        HQ_ROLLED for (int r = k; r <= l; ++r) col[r - k] = A[r][i];
+        HQ_ROLLED for (int c2 = k; c2 <= l; ++c2) row[c2 - k] = A[i][c2];
         double c = nrm2(col, l - k + 1, 1), r = nrm2(row, l - k + 1, 1);
         double ca = 0.0, ra = 0.0;
-        for (int rr = 0; rr <= l; ++rr) ca = jmax(ca, fabs(A[rr][i]));
-        for (int cc = k; cc < N; ++cc) ra = jmax(ra, fabs(A[i][cc]));
+        HQ_ROLLED for (int rr = 0; rr <= l; ++rr) ca = jmax(ca, fabs(A[rr][i]));
+        HQ_ROLLED for (int cc = k; cc < N; ++cc) ra = jmax(ra, fabs(A[i][cc]));
         if (c == 0.0 || r == 0.0) continue;
         if (!isfinite(c + ca + r + ra)) return -1;  // LAPACK dgebal: NaN -> error return
         double g = r / radix, f = 1.0;
         const double s = c + r;
-        for (int guard2 = 0; guard2 < 2200 && !(c >= g || jmax(jmax(f, c), ca) >= sfmax2 || jmin(jmin(r, g), ra) <= sfmin2); ++guard2) {
+        HQ_ROLLED for (int guard2 = 0; guard2 < 2200 && !(c >= g || jmax(jmax(f, c), ca) >= sfmax2 || jmin(jmin(r, g), ra) <= sfmin2); ++guard2) {
           f = f * radix; c = c * radix; ca = ca * radix; r = r / radix; g = g / radix; ra = ra / radix;
         }
         g = c / radix;
-        for (int guard3 = 0; guard3 < 2200 && !(g < r || jmax(r, ra) >= sfmax2 || jmin(jmin(jmin(f, c), g), ca) <= sfmin2); ++guard3) {
+        HQ_ROLLED for (int guard3 = 0; guard3 < 2200 && !(g < r || jmax(r, ra) >= sfmax2 || jmin(jmin(jmin(f, c), g), ca) <= sfmin2); ++guard3) {
           f = f / radix; c = c / radix; g = g / radix; ca = ca / radix; r = r * radix; ra = ra * radix;
         }
         if ((c + r) >= factor * s) continue;
@@ -188,37 +200,37 @@ HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
         g = 1.0 / f;
         scal[i] = scal[i] * f;
         noconv = true;
-        for (int cc = k; cc < N; ++cc) A[i][cc] = A[i][cc] * g;
-        for (int rr = 0; rr <= l; ++rr) A[rr][i] = A[rr][i] * f;
+        HQ_ROLLED for (int cc = k; cc < N; ++cc) A[i][cc] = A[i][cc] * g;
+        HQ_ROLLED for (int rr = 0; rr <= l; ++rr) A[rr][i] = A[rr][i] * f;
       }
     }
   }
   const int ilo = k, ihi = l;
-  for (int i = 0; i < ilo; ++i) { wr[i] = A[i][i]; wi[i] = 0.0; }
-  for (int i = ihi + 1; i < N; ++i) { wr[i] = A[i][i]; wi[i] = 0.0; }
+  HQ_ROLLED for (int i = 0; i < ilo; ++i) { wr[i] = A[i][i]; wi[i] = 0.0; }
+  HQ_ROLLED for (int i = ihi + 1; i < N; ++i) { wr[i] = A[i][i]; wi[i] = 0.0; }
   if (ilo > ihi) return 0;
   if (ilo == ihi) { wr[ilo] = A[ilo][ilo]; wi[ilo] = 0.0; return 0; }
-  for (int i = ilo; i < ihi; ++i) {
+  HQ_ROLLED for (int i = ilo; i < ihi; ++i) {
     const int nr = ihi - i;
     double v[N];
     double alpha = A[i + 1][i];
-    for (int r = 0; r < nr - 1; ++r) v[r + 1] = A[i + 2 + r][i];
+    HQ_ROLLED for (int r = 0; r < nr - 1; ++r) v[r + 1] = A[i + 2 + r][i];
     const double tau = dlarfg(nr, alpha, &v[1], 1);
     v[0] = 1.0;
     if (tau != 0.0) {
-      for (int r = 0; r <= ihi; ++r) {
+      HQ_ROLLED for (int r = 0; r <= ihi; ++r) {
         double w = 0.0;
-        for (int c = 0; c < nr; ++c) w = w + A[r][i + 1 + c] * v[c];
-        for (int c = 0; c < nr; ++c) A[r][i + 1 + c] = A[r][i + 1 + c] - tau * w * v[c];
+        HQ_ROLLED for (int c = 0; c < nr; ++c) w = w + A[r][i + 1 + c] * v[c];
+        HQ_ROLLED for (int c = 0; c < nr; ++c) A[r][i + 1 + c] = A[r][i + 1 + c] - tau * w * v[c];
       }
-      for (int c = i + 1; c < N; ++c) {
+      HQ_ROLLED for (int c = i + 1; c < N; ++c) {
         double w = 0.0;
-        for (int r = 0; r < nr; ++r) w = w + A[i + 1 + r][c] * v[r];
-        for (int r = 0; r < nr; ++r) A[i + 1 + r][c] = A[i + 1 + r][c] - tau * v[r] * w;
+        HQ_ROLLED for (int r = 0; r < nr; ++r) w = w + A[i + 1 + r][c] * v[r];
+        HQ_ROLLED for (int r = 0; r < nr; ++r) A[i + 1 + r][c] = A[i + 1 + r][c] - tau * v[r] * w;
       }
     }
     A[i + 1][i] = alpha;
-    for (int r = i + 2; r < N; ++r) A[r][i] = 0.0;
+    HQ_ROLLED for (int r = i + 2; r < N; ++r) A[r][i] = 0.0;
   }
   double (&H)[N][N] = A;
   const int nh = ihi - ilo + 1;
@@ -231,9 +243,9 @@ HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
   while (i >= ilo) {
     int lq = ilo;
     bool converged = false;
-    for (int its = 0; its <= itmax; ++its) {
+    HQ_ROLLED for (int its = 0; its <= itmax; ++its) {
       int kk;
-      for (kk = i; kk > lq; --kk) {
+      HQ_ROLLED for (kk = i; kk > lq; --kk) {
         if (fabs(H[kk][kk - 1]) <= smlnum) break;
         double tst = fabs(H[kk - 1][kk - 1]) + fabs(H[kk][kk]);
         if (tst == 0.0) {
@@ -282,7 +294,7 @@ HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
       }
       int m;
       double v[3];
-      for (m = i - 2; m >= lq; --m) {
+      HQ_ROLLED for (m = i - 2; m >= lq; --m) {
         double h21s = H[m + 1][m];
         double s2 = fabs(H[m][m] - rt2r) + fabs(rt2i) + fabs(h21s);
         h21s = H[m + 1][m] / s2;
@@ -296,9 +308,9 @@ HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
         const double h11b = fabs(v[0]) * (fabs(H[m - 1][m - 1]) + fabs(H[m][m]) + fabs(H[m + 1][m + 1]));
         if (h00 <= ulp * h11b) break;
       }
-      for (int kq = m; kq <= i - 1; ++kq) {
+      HQ_ROLLED for (int kq = m; kq <= i - 1; ++kq) {
         const int nr = (i - kq + 1) < 3 ? (i - kq + 1) : 3;
-        if (kq > m) for (int r = 0; r < nr; ++r) v[r] = H[kq + r][kq - 1];
+        if (kq > m) HQ_ROLLED for (int r = 0; r < nr; ++r) v[r] = H[kq + r][kq - 1];
         const double t1 = dlarfg(nr, v[0], &v[1], 1);
         if (kq > m) {
           H[kq][kq - 1] = v[0];
@@ -310,21 +322,21 @@ HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
         const double v2 = v[1], t2 = t1 * v2;
         if (nr == 3) {
           const double v3 = v[2], t3v = t1 * v3;
-          for (int j = kq; j <= i2; ++j) {
+          HQ_ROLLED for (int j = kq; j <= i2; ++j) {
             const double sum = H[kq][j] + v2 * H[kq + 1][j] + v3 * H[kq + 2][j];
             H[kq][j] = H[kq][j] - sum * t1; H[kq + 1][j] = H[kq + 1][j] - sum * t2; H[kq + 2][j] = H[kq + 2][j] - sum * t3v;
           }
           const int jm = (kq + 3 < i) ? kq + 3 : i;
-          for (int j = i1; j <= jm; ++j) {
+          HQ_ROLLED for (int j = i1; j <= jm; ++j) {
             const double sum = H[j][kq] + v2 * H[j][kq + 1] + v3 * H[j][kq + 2];
             H[j][kq] = H[j][kq] - sum * t1; H[j][kq + 1] = H[j][kq + 1] - sum * t2; H[j][kq + 2] = H[j][kq + 2] - sum * t3v;
           }
         } else if (nr == 2) {
-          for (int j = kq; j <= i2; ++j) {
+          HQ_ROLLED for (int j = kq; j <= i2; ++j) {
             const double sum = H[kq][j] + v2 * H[kq + 1][j];
             H[kq][j] = H[kq][j] - sum * t1; H[kq + 1][j] = H[kq + 1][j] - sum * t2;
           }
-          for (int j = i1; j <= i; ++j) {
+          HQ_ROLLED for (int j = i1; j <= i; ++j) {
             const double sum = H[j][kq] + v2 * H[j][kq + 1];
             H[j][kq] = H[j][kq] - sum * t1; H[j][kq + 1] = H[j][kq + 1] - sum * t2;
           }
@@ -378,12 +390,19 @@ HQD bool eig_real_jac_p1(double (&h)[36], double (&wr)[6], double (&wi)[6]) {
   return true;
 }
 
+// Which eigen-solve code jac_eigs_t and the functions above it run:
+// JAC_ANY the register path for pattern-1 Jacobians and the general code for
+// the rest; JAC_P1 pattern-1 Jacobians only (any other defers the cell);
+// JAC_GEN the general code for every Jacobian (one compact code path for a
+// pass over cells most of whose Jacobians need it).  Identical results.
+enum JacMode { JAC_ANY = 0, JAC_P1 = 1, JAC_GEN = 2 };
+
 // compute_jacobian_eigenvalues for one 15-moment slice: extreme real parts
 // and max |imag|.  A non-finite Jacobian gives NaN (the reference's guard).
-// FAST: pattern-1 Jacobians only; any other sets `deferred` and leaves the
+// Under JAC_P1 a Jacobian of another pattern sets `deferred` and leaves the
 // rest unset.
 struct EigOut { double vmin, vmax, imax; bool deferred; };
-template <bool FAST> HQN EigOut jac_eigs_t(const double* ma) {
+template <int MODE> HQN EigOut jac_eigs_t(const double* ma) {
   double r3[6], r5[6], r6[6];
   jacobian6_rows(ma, r3, r5, r6);
   double h[36];  // the Jacobian, row-major, held in registers
@@ -400,8 +419,15 @@ template <bool FAST> HQN EigOut jac_eigs_t(const double* ma) {
   o.deferred = false;
   if (!fin) { o.vmin = qnan(); o.vmax = qnan(); o.imax = qnan(); return o; }
   double wr[6], wi[6];
-  if (FAST) {
+  if (MODE == JAC_P1) {
     if (!eig_real_jac_p1(h, wr, wi)) { o.deferred = true; return o; }
+  } else if (MODE == JAC_GEN) {
+    double J[6][6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) J[r][c] = h[r * 6 + c];
+    eig_real<6>(J, wr, wi);
   } else {
     eig_real_jac(h, wr, wi);
   }
@@ -422,7 +448,7 @@ template <bool FAST> HQN EigOut jac_eigs_t(const double* ma) {
   o.imax = im;
   return o;
 }
-HQD EigOut jac_eigs(const double* ma) { return jac_eigs_t<false>(ma); }
+HQD EigOut jac_eigs(const double* ma) { return jac_eigs_t<JAC_ANY>(ma); }
 
 // axis_moment_slice (src/utils/axis_moment_slice.jl:31-54), 0-based
 __device__ constexpr int SLICE[4][15] = {{0, 5, 9, 12, 14, 1, 6, 10, 13, 2, 7, 11, 3, 8, 4},
@@ -477,16 +503,17 @@ HQN void correct_for_real(const double* M, int pa_i, int pa_j, int pb_i, int pb_
 // eigenvalues6_hyperbolic_3D for axis 1 (x) or 2 (y).
 // Moment n is read from M[n * ist] and written to Mr[n * ost] (the step
 // kernels pass the cell's entry of the moment-major fields, stride N); M and
-// Mr must not overlap.  FAST: returns true, with vmin, vmax and Mr not (or not
-// all) written, when a Jacobian needs the code outside the pattern-1 path.
-template <bool FAST>
+// Mr must not overlap.  MODE as jac_eigs_t; under JAC_P1 returns true, with
+// vmin, vmax and Mr not (or not all) written, when a Jacobian needs the code
+// outside the pattern-1 path.
+template <int MODE>
 HQN bool eigenvalues6_t(const double* M, int axis, int flag2D, double Ma, double& vmin, double& vmax, double* Mr, long long ist,
                         long long ost) {
   const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
   double a[15], b[15];
   for (int n = 0; n < 15; ++n) { a[n] = M[SLICE[sa][n] * ist]; b[n] = M[SLICE[sb][n] * ist]; }
-  EigOut ea = jac_eigs_t<FAST>(a), eb = jac_eigs_t<FAST>(b);
-  if (FAST && (ea.deferred || eb.deferred)) return true;
+  EigOut ea = jac_eigs_t<MODE>(a), eb = jac_eigs_t<MODE>(b);
+  if (MODE == JAC_P1 && (ea.deferred || eb.deferred)) return true;
   auto combine = [&]() {
     vmin = ea.vmin; vmax = ea.vmax;
     if (eb.vmin == eb.vmin || eb.vmax == eb.vmax) { vmin = jmin(vmin, eb.vmin); vmax = jmax(vmax, eb.vmax); }
@@ -502,8 +529,8 @@ HQN bool eigenvalues6_t(const double* M, int axis, int flag2D, double Ma, double
     // pair a is always the UV plane; pair b is UW (x) or VW (y)
     correct_for_real(Ml, 0, 1, axis == 1 ? 0 : 1, 2, (ca ? 1 : 0) | (cb ? 2 : 0), flag2D, Ma, Mc);
     for (int n = 0; n < 15; ++n) { a[n] = Mc[SLICE[sa][n]]; b[n] = Mc[SLICE[sb][n]]; }
-    ea = jac_eigs_t<FAST>(a); eb = jac_eigs_t<FAST>(b);
-    if (FAST && (ea.deferred || eb.deferred)) return true;
+    ea = jac_eigs_t<MODE>(a); eb = jac_eigs_t<MODE>(b);
+    if (MODE == JAC_P1 && (ea.deferred || eb.deferred)) return true;
     combine();
     for (int n = 0; n < 35; ++n) Mr[n * ost] = Mc[n];
   }
@@ -511,26 +538,26 @@ HQN bool eigenvalues6_t(const double* M, int axis, int flag2D, double Ma, double
 }
 HQD void eigenvalues6(const double* M, int axis, int flag2D, double Ma, double& vmin, double& vmax, double* Mr, long long ist = 1,
                       long long ost = 1) {
-  eigenvalues6_t<false>(M, axis, flag2D, Ma, vmin, vmax, Mr, ist, ost);
+  eigenvalues6_t<JAC_ANY>(M, axis, flag2D, Ma, vmin, vmax, Mr, ist, ost);
 }
 
 // Which of eigenvalues6's two planes need the complex-eigenvalue correction
 // (bit 0: first slice, bit 1: second), from the same Jacobians and the same
 // test; phase E only needs the corrected moments, so its kernels decide here
 // and leave the corrections to a separate pass over the flagged cells.
-// FAST: -1 when a Jacobian needs the code outside the pattern-1 path.
-template <bool FAST> HQN int eigenvalues6_flags_t(const double* M, int axis, long long ist) {
+// Under JAC_P1: -1 when a Jacobian needs the code outside the pattern-1 path.
+template <int MODE> HQN int eigenvalues6_flags_t(const double* M, int axis, long long ist) {
   const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
   double a[15], b[15];
   for (int n = 0; n < 15; ++n) { a[n] = M[SLICE[sa][n] * ist]; b[n] = M[SLICE[sb][n] * ist]; }
-  const EigOut ea = jac_eigs_t<FAST>(a), eb = jac_eigs_t<FAST>(b);
-  if (FAST && (ea.deferred || eb.deferred)) return -1;
+  const EigOut ea = jac_eigs_t<MODE>(a), eb = jac_eigs_t<MODE>(b);
+  if (MODE == JAC_P1 && (ea.deferred || eb.deferred)) return -1;
   const double thr = 1000.0 * EPS;
   return (ea.imax > thr ? 1 : 0) | (eb.imax > thr ? 2 : 0);
 }
 
-// eigenvalues6z_hyperbolic_3D (strides and FAST as eigenvalues6_t)
-template <bool FAST>
+// eigenvalues6z_hyperbolic_3D (strides and MODE as eigenvalues6_t)
+template <int MODE>
 HQN bool eigenvalues6z_t(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr, long long ist,
                          long long ost) {
   double Mw[35];
@@ -551,8 +578,8 @@ HQN bool eigenvalues6z_t(const double* M, int flag2D, double Ma, int positivity,
   for (int n = 0; n < 35; ++n) Mr[n * ost] = Mw[n];
   double a[15], b[15];
   for (int n = 0; n < 15; ++n) { a[n] = Mw[WUI[n]]; b[n] = Mw[SLICE[3][n]]; }
-  EigOut ea = jac_eigs_t<FAST>(a), eb = jac_eigs_t<FAST>(b);
-  if (FAST && (ea.deferred || eb.deferred)) return true;
+  EigOut ea = jac_eigs_t<MODE>(a), eb = jac_eigs_t<MODE>(b);
+  if (MODE == JAC_P1 && (ea.deferred || eb.deferred)) return true;
   vmin = jmin(ea.vmin, eb.vmin);
   vmax = jmax(ea.vmax, eb.vmax);
   const double thr = 1000.0 * EPS;
@@ -562,8 +589,8 @@ HQN bool eigenvalues6z_t(const double* M, int flag2D, double Ma, int positivity,
     for (int n = 0; n < 35; ++n) Ml[n] = M[n * ist];
     correct_for_real(Ml, 0, 2, 1, 2, (ca ? 1 : 0) | (cb ? 2 : 0), flag2D, Ma, Mc);
     for (int n = 0; n < 15; ++n) { a[n] = Mc[WUI[n]]; b[n] = Mc[SLICE[3][n]]; }
-    ea = jac_eigs_t<FAST>(a); eb = jac_eigs_t<FAST>(b);
-    if (FAST && (ea.deferred || eb.deferred)) return true;
+    ea = jac_eigs_t<MODE>(a); eb = jac_eigs_t<MODE>(b);
+    if (MODE == JAC_P1 && (ea.deferred || eb.deferred)) return true;
     vmin = jmin(ea.vmin, eb.vmin);
     vmax = jmax(ea.vmax, eb.vmax);
     for (int n = 0; n < 35; ++n) Mr[n * ost] = Mc[n];
@@ -572,7 +599,7 @@ HQN bool eigenvalues6z_t(const double* M, int flag2D, double Ma, int positivity,
 }
 HQD void eigenvalues6z(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr, long long ist = 1,
                        long long ost = 1) {
-  eigenvalues6z_t<false>(M, flag2D, Ma, positivity, vmin, vmax, Mr, ist, ost);
+  eigenvalues6z_t<JAC_ANY>(M, flag2D, Ma, positivity, vmin, vmax, Mr, ist, ost);
 }
 
 // closure_and_eigenvalues with N = 2: extreme eigenvalues of the 3x3 Jacobi

@@ -45,6 +45,11 @@ constexpr int MINB_CLOSURE = HQ_MINB_CLOSURE;
 constexpr int MINB_EIG = HQ_MINB_EIG;
 constexpr int MINB_FIX = HQ_MINB_FIX;
 constexpr int FIX_BLOCKS = HQ_FIX_BLOCKS;
+// Eigen-solve code of those passes (hyq::JacMode; 2 = the general code only)
+#ifndef HQ_FIX_MODE
+#define HQ_FIX_MODE 2
+#endif
+constexpr int FIX_MODE = HQ_FIX_MODE;
 
 constexpr int BS_A = 128;
 constexpr int BS_EF = 128;

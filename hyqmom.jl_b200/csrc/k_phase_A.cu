@@ -67,8 +67,8 @@ __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* __restri
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
   if (c >= c1) return;
   double lo, hi;
-  const bool deferred = axis == 3 ? eigenvalues6z_t<true>(in + c, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out + c, N, N)
-                                  : eigenvalues6_t<true>(in + c, axis, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
+  const bool deferred = axis == 3 ? eigenvalues6z_t<JAC_P1>(in + c, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out + c, N, N)
+                                  : eigenvalues6_t<JAC_P1>(in + c, axis, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
   if (deferred) {
     unsigned int* list = defer_list(vp, N);
     list[atomicAdd(list + N + (axis - 1), 1u)] = (unsigned int)c;
@@ -89,8 +89,8 @@ __global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* __restri
   for (unsigned int e = blockIdx.x * BS_A + threadIdx.x; e < count; e += gridDim.x * BS_A) {
     const long long c = list[e];
     double lo, hi;
-    if (axis == 3) eigenvalues6z_t<false>(in + c, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out + c, N, N);
-    else eigenvalues6_t<false>(in + c, axis, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
+    if (axis == 3) eigenvalues6z_t<FIX_MODE>(in + c, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out + c, N, N);
+    else eigenvalues6_t<FIX_MODE>(in + c, axis, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
     v[c] = lo; v[c + N] = hi;
   }
 }

@@ -38,7 +38,7 @@ __global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* __restr
   if (!clk->active) return;
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
   if (c >= c1) return;
-  const int planes = eigenvalues6_flags_t<true>(in + c, axis, N);
+  const int planes = eigenvalues6_flags_t<JAC_P1>(in + c, axis, N);
 #pragma unroll
   for (int n = 0; n < 35; ++n) out[c + N * n] = in[c + N * n];
   if (planes) {
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(BS_EF, MINB_FIX) k_E_fix(const double* __restr
     const unsigned long long v = list[e];
     const long long c = (long long)(v >> 2);
     int planes = int(v & 3ull);
-    if (planes == 0) planes = eigenvalues6_flags_t<false>(in + c, axis, N);
+    if (planes == 0) planes = eigenvalues6_flags_t<FIX_MODE>(in + c, axis, N);
     if (planes == 0) continue;
     double Ml[35], Mc[35];
     for (int n = 0; n < 35; ++n) Ml[n] = in[c + N * n];

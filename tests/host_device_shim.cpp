@@ -20,11 +20,11 @@ void sh_eig(const double* m, int axis, int flag2D, double Ma, int pos, double* v
 // the pattern-1-only variant the step kernels run first: 1 when it left the
 // cell to the complete function (outputs then not meaningful)
 int sh_eig_fast(const double* m, int axis, int flag2D, double Ma, int pos, double* v, double* Mr) {
-  if (axis == 3) return eigenvalues6z_t<true>(m, flag2D, Ma, pos, v[0], v[1], Mr, 1, 1) ? 1 : 0;
-  return eigenvalues6_t<true>(m, axis, flag2D, Ma, v[0], v[1], Mr, 1, 1) ? 1 : 0;
+  if (axis == 3) return eigenvalues6z_t<JAC_P1>(m, flag2D, Ma, pos, v[0], v[1], Mr, 1, 1) ? 1 : 0;
+  return eigenvalues6_t<JAC_P1>(m, axis, flag2D, Ma, v[0], v[1], Mr, 1, 1) ? 1 : 0;
 }
 int sh_eig_flags(const double* m, int axis, int fast) {
-  return fast ? eigenvalues6_flags_t<true>(m, axis, 1) : eigenvalues6_flags_t<false>(m, axis, 1);
+  return fast ? eigenvalues6_flags_t<JAC_P1>(m, axis, 1) : eigenvalues6_flags_t<JAC_ANY>(m, axis, 1);
 }
 void sh_closure(const double* mom, double* v) { closure_eigs(mom[0], mom[1], mom[2], mom[3], mom[4], v[0], v[1]); }
 void sh_coll(double* m, double dt, double Kn, int pos) { collision35(m, dt, Kn, pos); }
