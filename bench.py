@@ -2,8 +2,11 @@
 
 A "step" is one time step of simulation_runner over the whole grid.  Default
 workload: crossing jets 160 x 160 x 80 (2,048,000 cells, 573 MB of FP64
-state), Ma=1, Kn=1, CFL=0.7, plain eigen-solve.  The state (573 MB) and the
-flux buffers exceed L2 (126 MB), so no L2 flush is needed between steps.
+state), Ma=1, Kn=1, plain eigen-solve, 200 steps from the initial condition
+(the timed steps always start from the IC: a step's cost grows ~7x over the
+run as the flow develops, so a window of early steps would not represent
+it).  The state (573 MB) and the flux buffers exceed L2 (126 MB), so no L2
+flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -29,17 +32,18 @@ METRIC = "cell-steps/s on 1 B200: plain eig vs learned warm-start, <=1e-8 rel vs
 UNIT = "cell-steps/s"
 
 # FP64 operations per cell-step of the plain path (oracle op counter, +,-,*,/
-# and sqrt/cbrt/exp counted 1 each), crossing jets 160x160x80 Ma=1 Kn=1, first
-# step, averaged over a 160x160x8 slab through the jets; recomputed by
-# `python bench.py --count-ops`.
-F_ALG = 43772.6
+# and sqrt/cbrt/exp counted 1 each), crossing jets 160x160x80 Ma=1 Kn=1,
+# averaged over the 200-step run: counted on a 160x160x4 slab through the
+# jets of the state at steps 0, 25, ..., 175; recomputed by
+# `python bench.py --count-ops` (needs the GPU for the states).
+F_ALG = 92682.1
 B_ALG = 2 * 35 * 8  # bytes per cell-step: state read once, written once
 
 # The step's kernels in launch order (hyq_advance_timed slots) and their FP64
 # operations per cell from the same count (CFL: one max per cell; HLL: three
 # sweeps of 18 ops per moment plus the 4-op combination).
 E2E_SLABS = 4
-LAUNCHES_PER_STEP = 13  # the eleven timed kernels and the two correction passes of E2/E3
+LAUNCHES_PER_STEP = 21  # the eleven timed kernels and the two passes over listed cells of A2-A4, E2, E3
 KERNELS = ["A1_closure", "A2_eig_x", "A3_eig_y", "A4_eig_z", "A5_flux_speeds", "cfl", "hll",
            "E1_closure", "E2_eig_x", "E3_eig_y", "E4_closure_bgk"]
 # DRAM bytes (read + write) per cell of each kernel from one ncu capture of
@@ -48,8 +52,9 @@ KERNELS = ["A1_closure", "A2_eig_x", "A3_eig_y", "A4_eig_z", "A5_flux_speeds", "
 # depend on the grid size.
 TRAFFIC_PER_CELL = {"A1_closure": 3221.0, "A2_eig_x": 1720.0, "A3_eig_y": 1725.0, "A4_eig_z": 2326.0, "A5_flux_speeds": 4487.0,
                     "hll": 1609.0, "E1_closure": 3211.0, "E2_eig_x": 1443.0, "E3_eig_y": 1424.0, "E4_closure_bgk": 3951.0}
-F_KERNEL = {"A1_closure": 7583.0, "A2_eig_x": 1696.2, "A3_eig_y": 1696.2, "A4_eig_z": 1708.2, "A5_flux_speeds": 9709.4,
-            "cfl": 1.0, "hll": 2030.0, "E1_closure": 7583.0, "E2_eig_x": 1696.3, "E3_eig_y": 1696.3, "E4_closure_bgk": 8374.0}
+TRAFFIC_SOURCE = "ncu dram__bytes_read+write per cell on 96x96x48, first step, scaled to this launch's cells"
+F_KERNEL = {"A1_closure": 11800.8, "A2_eig_x": 8014.9, "A3_eig_y": 8022.6, "A4_eig_z": 8494.7, "A5_flux_speeds": 13804.2,
+            "cfl": 1.0, "hll": 2030.0, "E1_closure": 11811.2, "E2_eig_x": 8050.8, "E3_eig_y": 8050.3, "E4_closure_bgk": 12602.6}
 
 
 def workload(name="c2"):
@@ -143,32 +148,46 @@ def fp64_peak_tflops(torch):
     return best
 
 
-def cpu_baseline(p, seconds=15.0):
-    """The oracle (CPU restatement, OpenMP, all host threads) on a slab sample."""
+def slab_of(M, nz):
+    """An nz-layer z-slab through the middle (the jets) of a state."""
+    z0 = M.shape[2] // 2 - nz // 2
+    return np.array(M[:, :, z0:z0 + nz, :], order="F")
+
+
+def cpu_baseline(p, slabs, what=None):
+    """The oracle (CPU restatement, OpenMP, all host threads): one step on each
+    of `slabs` [(step, state)], slabs of the run's states at spread-out steps
+    (the same array listed again is stepped again)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as ol
     from hyqmom import ic
-    M = sample_slab(p, nz=8)
-    q = dict(p, Nz=M.shape[2], **ic.grid_spacing(p))
-    cells = M.shape[0] * M.shape[1] * M.shape[2]
-    t0 = time.perf_counter()
-    steps, t = 0, 0.0
-    while True:
-        _, t, _ = ol.step(M, q, t)
-        steps += 1
-        if time.perf_counter() - t0 > seconds or steps >= 3:
-            break
-    el = time.perf_counter() - t0
-    return {"value": cells * steps / el, "unit": UNIT, "cores": int(ol.load().hyqo_num_threads()), "kind": "port",
-            "sample": f"{steps} step(s) of a {M.shape[0]}x{M.shape[1]}x{M.shape[2]} z-slab through the jets of the "
-                      f"same IC ({cells} cells), oracle C++ restatement, OpenMP"}
+    cells = el = 0.0
+    for _, M in slabs:
+        q = dict(p, Nz=M.shape[2], **ic.grid_spacing(p))
+        t0 = time.perf_counter()
+        ol.step(M, q, 0.0)
+        el += time.perf_counter() - t0
+        cells += M.shape[0] * M.shape[1] * M.shape[2]
+    M = slabs[0][1]
+    return {"value": cells / el, "unit": UNIT, "cores": int(ol.load().hyqo_num_threads()), "kind": "port",
+            "sample": f"{what or 'one step of a z-slab through the jets of the run state at each of steps %s' % [k for k, _ in slabs]}"
+                      f" ({M.shape[0]}x{M.shape[1]}x{M.shape[2]} cells, {int(cells)} cell-steps, {el:.1f} s), "
+                      f"oracle C++ restatement, OpenMP"}
 
 
 def run_reference(args, rank, world):
+    """The oracle on the host cores: each step one oracle step of a z-slab
+    of the workload's initial condition (the reference arm has no GPU run to
+    draw later states from; the IC's steps are the cheapest of the run, so
+    this rate is optimistic for the CPU)."""
     if rank != 0:
         return
     p = workload(args.config)
-    base = cpu_baseline(p, seconds=20.0)
+    from hyqmom import ic
+    M0 = ic.initial_state(p)
+    n = max(1, min(args.steps, 3))
+    slab = slab_of(M0, 8)
+    base = cpu_baseline(p, [(k, slab) for k in range(n)], f"steps 1-{n} of a z-slab through the jets of the initial condition")
     line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (reference crossing-jets IC generator)",
@@ -176,7 +195,7 @@ def run_reference(args, rank, world):
                        "sample": base["sample"]},
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "reference Julia CPU path unavailable (no julia in the image); timed: the oracle restatement"}
+            "note": "reference Julia CPU path unavailable (no julia in the image); timed: the oracle restatement on IC slabs"}
     print(json.dumps(line), flush=True)
 
 
@@ -218,6 +237,8 @@ def run_gpu(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
+    # the timed steps: 1..K from the initial condition (set_state resets t, nn)
+    s.set_state(M0)
     barrier()
     sampler = ClockSampler(local_rank)
     with sampler:
@@ -229,33 +250,36 @@ def run_gpu(args, rank, world, local_rank):
         barrier()
     ms = e0.elapsed_time(e1)
     st = s.stats()
-    assert st["status"] == 0 and st["nn"] == args.warmup + args.steps, f"steps did not all run: {st}"
+    assert st["status"] == 0 and st["nn"] == args.steps, f"steps did not all run: {st}"
     ms = max_over_ranks(ms, dist, "cuda")
     value = replica_throughput(world, cells, args.steps, ms)
 
-    # per-kernel device time (individual launches, same stream)
-    s.set_state(M0)
-    s.advance(args.warmup)
+    # per-kernel device time over the same steps (individual launches, CUDA
+    # events on the context stream)
     import ctypes
-    kms = (ctypes.c_float * len(KERNELS))()
-    ksteps = max(1, min(args.steps, 3))
-    s._chk(s._lib.hyq_advance_timed(s._h, ksteps, kms))
-    kern = {k: kms[i] / ksteps for i, k in enumerate(KERNELS)}
-
-    # end to end through the public API: each step uploads the host state
-    # (pinned) and downloads the result (hyq_step_host, the copies overlapped
-    # slab by slab with the per-cell phases), on the same steps as the
-    # device-timed run (warm-up steps first, on the device)
     s.set_state(M0)
-    s.advance(args.warmup)
+    kms = (ctypes.c_float * len(KERNELS))()
+    s._chk(s._lib.hyq_advance_timed(s._h, args.steps, kms))
+    kern = {k: kms[i] / args.steps for i, k in enumerate(KERNELS)}
+
+    # end to end through the public API over the same steps: each step uploads
+    # the host state (pinned) and downloads the result (hyq_step_host, the
+    # copies overlapped slab by slab with the per-cell phases).  Slabs of the
+    # state at four points of the run are kept (outside the timing) for the
+    # CPU baseline.
+    s.set_state(M0)
     Mh_flat = torch.empty(35 * cells, dtype=torch.float64).pin_memory()
     Mh = Mh_flat.numpy().reshape(M0.shape, order="F")
-    s._chk(s._lib.hyq_get_state(s._h, ctypes.c_void_p(Mh_flat.data_ptr())))
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
+    Mh[...] = M0
+    marks = sorted({(args.steps * q) // 4 for q in range(4)})
+    slabs = []
+    e2e_s = 0.0
+    for k in range(args.steps):
+        if k in marks:
+            slabs.append((k, slab_of(Mh, 8)))
+        t0 = time.perf_counter()
         s.step_host(Mh, nslabs=E2E_SLABS)
-    e2e_s = time.perf_counter() - t0
+        e2e_s += time.perf_counter() - t0
     e2e = {"value": world * cells * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": Mh_flat.numel() * 8,
            "d2h_bytes_per_step": Mh_flat.numel() * 8, "api": f"hyq_step_host, {E2E_SLABS} slabs, pinned host state"}
     s.close()
@@ -273,7 +297,7 @@ def run_gpu(args, rank, world, local_rank):
     step_tflops = F_ALG * cells / (ms / args.steps * 1e-3) / 1e12
     traffic = TRAFFIC_PER_CELL[dom] * cells if dom in TRAFFIC_PER_CELL else None
     roof = {"bound": "fp64", "achieved": ach, "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64, "traffic": traffic,
-            "traffic_source": "ncu dram__bytes_read+write per cell on 96x96x48, scaled to this launch's cells",
+            "traffic_source": TRAFFIC_SOURCE,
             "peak_source": "measured in this run: FP64 DGEMM 8192^3 (cuBLAS via torch), best of 3",
             "dominant_kernel": "k_" + dom, "f_alg_per_cell": F_KERNEL[dom],
             "note": "built with -fmad=false: every counted op is one FP64 pipe instruction, so an FMA-free kernel tops out at peak/2",
@@ -284,12 +308,12 @@ def run_gpu(args, rank, world, local_rank):
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (reference crossing-jets IC generator)",
             "config": {"workload": f"crossing jets {p['Nx']}x{p['Ny']}x{p['Nz']} Ma={p['Ma']} Kn={p['Kn']} CFL={p['CFL']}, plain eig",
-                       "cells": cells, "parallelism": f"replicas x{world}",
+                       "cells": cells, "parallelism": f"replicas x{world}", "timed_steps": f"1-{args.steps} from the initial condition",
                        "l2": f"state {cells * 35 * 8 / 1e6:.0f} MB > L2 (126 MB), no flush needed",
                        "steps_done": st["nn"]},
             "gpu_launches": LAUNCHES_PER_STEP * args.steps, "e2e": e2e, "roofline": roof, "clocks": sampler.summary()}
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(p, seconds=15.0)
+        line["cpu_baseline"] = cpu_baseline(p, slabs)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -376,28 +400,40 @@ def run_batch(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
-def count_ops():
+def count_ops(args):
+    """F_ALG and F_KERNEL: the oracle's FP64 op counter on a 160x160x4 z-slab
+    through the jets of the workload's state at steps 0, 25, ..., 175 of the
+    run (states from the GPU step, which is bit-identical to the oracle's),
+    averaged over the samples."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as ol
     from hyqmom import ic
+    from hyqmom.runner import Solver
     p = workload("c2")
-    M = sample_slab(p, nz=8)
-    q = dict(p, Nz=M.shape[2], **ic.grid_spacing(p))
-    cells = M.shape[0] * M.shape[1] * M.shape[2]
-    dt = 1e-3
-    out = ol.count_ops(M, q, dt)
-    st = ol.count_ops_stages(M, q, dt) / cells
-    per = (out[0] + out[1]) / cells + out[2]
+    s = Solver(p)
+    s.set_state(ic.initial_state(p))
     names = [k for k in KERNELS if k not in ("cfl", "hll")]
-    print(json.dumps({"cells": cells, "phase_A_ops_per_cell": out[0] / cells, "phase_EF_ops_per_cell": out[1] / cells,
-                      "hll_ops_per_cell": out[2], "F_alg": per,
-                      "per_kernel": {k: round(float(v), 1) for k, v in zip(names, st)}}))
+    tot, stages, samples = np.zeros(3), np.zeros(len(names)), []
+    for k in range(0, args.steps, 25):
+        s.advance(k - s.stats()["nn"])
+        M = slab_of(s.get_state(), 4)
+        q = dict(p, Nz=M.shape[2], **ic.grid_spacing(p))
+        cells = M.shape[0] * M.shape[1] * M.shape[2]
+        out = ol.count_ops(M, q, 1e-3) / np.array([cells, cells, 1.0])
+        st = ol.count_ops_stages(M, q, 1e-3)[:len(names)] / cells
+        tot, stages = tot + out, stages + st
+        samples.append({"step": k, "F": round(float(out[0] + out[1] + out[2]), 1)})
+        print(json.dumps(samples[-1]), flush=True)
+    s.close()
+    n = len(samples)
+    print(json.dumps({"samples": n, "F_alg": round(float(tot.sum() / n), 1), "hll_ops_per_cell": float(tot[2] / n),
+                      "per_kernel": {k: round(float(v / n), 1) for k, v in zip(names, stages)}}))
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c2s", "c4", "c5"])
@@ -405,7 +441,7 @@ def main():
     ap.add_argument("--count-ops", action="store_true")
     args = ap.parse_args()
     if args.count_ops:
-        return count_ops()
+        return count_ops(args)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

@@ -500,20 +500,30 @@ HQN void correct_for_real(const double* M, int pa_i, int pa_j, int pb_i, int pb_
   flux_closure35(C, flag2D, Ma, nullptr, nullptr, nullptr, Mout);
 }
 
+// Outcome of the eigenvalue functions below when run in parts.
+enum EigStatus { EIG_DONE = 0, EIG_DEFERRED = 1, EIG_NEEDS_FIX = 2 };
+
 // eigenvalues6_hyperbolic_3D for axis 1 (x) or 2 (y).
 // Moment n is read from M[n * ist] and written to Mr[n * ost] (the step
 // kernels pass the cell's entry of the moment-major fields, stride N); M and
-// Mr must not overlap.  MODE as jac_eigs_t; under JAC_P1 returns true, with
-// vmin, vmax and Mr not (or not all) written, when a Jacobian needs the code
-// outside the pattern-1 path.
-template <int MODE>
-HQN bool eigenvalues6_t(const double* M, int axis, int flag2D, double Ma, double& vmin, double& vmax, double* Mr, long long ist,
-                        long long ost) {
+// Mr must not overlap.  MODE as jac_eigs_t.  With CORR the whole function
+// runs (EIG_DONE, or EIG_DEFERRED under JAC_P1); without it, a cell whose
+// Jacobians have complex eigenvalues returns EIG_NEEDS_FIX before the
+// correction, whose code (a closure with its realizability) is then not part
+// of the caller.  vmin, vmax and Mr are complete only with EIG_DONE.
+template <int MODE, bool CORR>
+HQN int eigenvalues6_s(const double* M, int axis, int flag2D, double Ma, double& vmin, double& vmax, double* Mr, long long ist,
+                       long long ost) {
   const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
   double a[15], b[15];
   for (int n = 0; n < 15; ++n) { a[n] = M[SLICE[sa][n] * ist]; b[n] = M[SLICE[sb][n] * ist]; }
-  EigOut ea = jac_eigs_t<MODE>(a), eb = jac_eigs_t<MODE>(b);
-  if (MODE == JAC_P1 && (ea.deferred || eb.deferred)) return true;
+  EigOut ea = jac_eigs_t<MODE>(a);
+  if (ea.deferred) return EIG_DEFERRED;
+  EigOut eb = jac_eigs_t<MODE>(b);
+  if (eb.deferred) return EIG_DEFERRED;
+  const double thr = 1000.0 * EPS;
+  const bool ca = ea.imax > thr, cb = eb.imax > thr;
+  if (!CORR && (ca || cb)) return EIG_NEEDS_FIX;
   auto combine = [&]() {
     vmin = ea.vmin; vmax = ea.vmax;
     if (eb.vmin == eb.vmin || eb.vmax == eb.vmax) { vmin = jmin(vmin, eb.vmin); vmax = jmax(vmax, eb.vmax); }
@@ -521,45 +531,51 @@ HQN bool eigenvalues6_t(const double* M, int axis, int flag2D, double Ma, double
   combine();
 #pragma unroll
   for (int n = 0; n < 35; ++n) Mr[n * ost] = M[n * ist];
-  const double thr = 1000.0 * EPS;
-  const bool ca = ea.imax > thr, cb = eb.imax > thr;
-  if (ca || cb) {
-    double Ml[35], Mc[35];
-    for (int n = 0; n < 35; ++n) Ml[n] = M[n * ist];
-    // pair a is always the UV plane; pair b is UW (x) or VW (y)
-    correct_for_real(Ml, 0, 1, axis == 1 ? 0 : 1, 2, (ca ? 1 : 0) | (cb ? 2 : 0), flag2D, Ma, Mc);
-    for (int n = 0; n < 15; ++n) { a[n] = Mc[SLICE[sa][n]]; b[n] = Mc[SLICE[sb][n]]; }
-    ea = jac_eigs_t<MODE>(a); eb = jac_eigs_t<MODE>(b);
-    if (MODE == JAC_P1 && (ea.deferred || eb.deferred)) return true;
-    combine();
-    for (int n = 0; n < 35; ++n) Mr[n * ost] = Mc[n];
+  if constexpr (CORR) {
+    if (ca || cb) {
+      double Ml[35], Mc[35];
+      for (int n = 0; n < 35; ++n) Ml[n] = M[n * ist];
+      // pair a is always the UV plane; pair b is UW (x) or VW (y)
+      correct_for_real(Ml, 0, 1, axis == 1 ? 0 : 1, 2, (ca ? 1 : 0) | (cb ? 2 : 0), flag2D, Ma, Mc);
+      for (int n = 0; n < 15; ++n) { a[n] = Mc[SLICE[sa][n]]; b[n] = Mc[SLICE[sb][n]]; }
+      ea = jac_eigs_t<MODE>(a);
+      if (ea.deferred) return EIG_DEFERRED;
+      eb = jac_eigs_t<MODE>(b);
+      if (eb.deferred) return EIG_DEFERRED;
+      combine();
+      for (int n = 0; n < 35; ++n) Mr[n * ost] = Mc[n];
+    }
   }
-  return false;
+  return EIG_DONE;
 }
 HQD void eigenvalues6(const double* M, int axis, int flag2D, double Ma, double& vmin, double& vmax, double* Mr, long long ist = 1,
                       long long ost = 1) {
-  eigenvalues6_t<JAC_ANY>(M, axis, flag2D, Ma, vmin, vmax, Mr, ist, ost);
+  eigenvalues6_s<JAC_ANY, true>(M, axis, flag2D, Ma, vmin, vmax, Mr, ist, ost);
 }
 
 // Which of eigenvalues6's two planes need the complex-eigenvalue correction
 // (bit 0: first slice, bit 1: second), from the same Jacobians and the same
 // test; phase E only needs the corrected moments, so its kernels decide here
 // and leave the corrections to a separate pass over the flagged cells.
-// Under JAC_P1: -1 when a Jacobian needs the code outside the pattern-1 path.
+// -1 when MODE defers a Jacobian (JAC_P1).
 template <int MODE> HQN int eigenvalues6_flags_t(const double* M, int axis, long long ist) {
   const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
   double a[15], b[15];
   for (int n = 0; n < 15; ++n) { a[n] = M[SLICE[sa][n] * ist]; b[n] = M[SLICE[sb][n] * ist]; }
-  const EigOut ea = jac_eigs_t<MODE>(a), eb = jac_eigs_t<MODE>(b);
-  if (MODE == JAC_P1 && (ea.deferred || eb.deferred)) return -1;
+  const EigOut ea = jac_eigs_t<MODE>(a);
+  if (ea.deferred) return -1;
+  const EigOut eb = jac_eigs_t<MODE>(b);
+  if (eb.deferred) return -1;
   const double thr = 1000.0 * EPS;
   return (ea.imax > thr ? 1 : 0) | (eb.imax > thr ? 2 : 0);
 }
 
-// eigenvalues6z_hyperbolic_3D (strides and MODE as eigenvalues6_t)
-template <int MODE>
-HQN bool eigenvalues6z_t(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr, long long ist,
-                         long long ost) {
+// eigenvalues6z_hyperbolic_3D (strides, MODE, CORR and the outcome as
+// eigenvalues6_s; without CORR the negative-variance re-realization also
+// returns EIG_NEEDS_FIX)
+template <int MODE, bool CORR>
+HQN int eigenvalues6z_s(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr, long long ist,
+                        long long ost) {
   double Mw[35];
 #pragma unroll
   for (int n = 0; n < 35; ++n) Mw[n] = M[n * ist];
@@ -569,37 +585,45 @@ HQN bool eigenvalues6z_t(const double* M, int flag2D, double Ma, int positivity,
     const double vx = M[2 * ist] / m000 - sq(M[1 * ist] / m000), vy = M[9 * ist] / m000 - sq(M[5 * ist] / m000),
                  vz = M[19 * ist] / m000 - sq(M[15 * ist] / m000);
     if (vx < 0.0 || vy < 0.0 || vz < 0.0) {
-      flux_closure35(M, flag2D, Ma, nullptr, nullptr, nullptr, Mw, ist, 1);
+      if constexpr (CORR) flux_closure35(M, flag2D, Ma, nullptr, nullptr, nullptr, Mw, ist, 1);
+      else return EIG_NEEDS_FIX;
     }
   }
+  double a[15], b[15];
+  for (int n = 0; n < 15; ++n) { a[n] = Mw[WUI[n]]; b[n] = Mw[SLICE[3][n]]; }
+  EigOut ea = jac_eigs_t<MODE>(a);
+  if (ea.deferred) return EIG_DEFERRED;
+  EigOut eb = jac_eigs_t<MODE>(b);
+  if (eb.deferred) return EIG_DEFERRED;
+  const double thr = 1000.0 * EPS;
+  const bool ca = ea.imax > thr, cb = eb.imax > thr;
+  if (!CORR && (ca || cb)) return EIG_NEEDS_FIX;
   // Mr: the input with its density floored or, after the negative-variance
   // re-realization, that closure -- Mw in both cases
 #pragma unroll
   for (int n = 0; n < 35; ++n) Mr[n * ost] = Mw[n];
-  double a[15], b[15];
-  for (int n = 0; n < 15; ++n) { a[n] = Mw[WUI[n]]; b[n] = Mw[SLICE[3][n]]; }
-  EigOut ea = jac_eigs_t<MODE>(a), eb = jac_eigs_t<MODE>(b);
-  if (MODE == JAC_P1 && (ea.deferred || eb.deferred)) return true;
   vmin = jmin(ea.vmin, eb.vmin);
   vmax = jmax(ea.vmax, eb.vmax);
-  const double thr = 1000.0 * EPS;
-  const bool ca = ea.imax > thr, cb = eb.imax > thr;
-  if (ca || cb) {
-    double Ml[35], Mc[35];
-    for (int n = 0; n < 35; ++n) Ml[n] = M[n * ist];
-    correct_for_real(Ml, 0, 2, 1, 2, (ca ? 1 : 0) | (cb ? 2 : 0), flag2D, Ma, Mc);
-    for (int n = 0; n < 15; ++n) { a[n] = Mc[WUI[n]]; b[n] = Mc[SLICE[3][n]]; }
-    ea = jac_eigs_t<MODE>(a); eb = jac_eigs_t<MODE>(b);
-    if (MODE == JAC_P1 && (ea.deferred || eb.deferred)) return true;
-    vmin = jmin(ea.vmin, eb.vmin);
-    vmax = jmax(ea.vmax, eb.vmax);
-    for (int n = 0; n < 35; ++n) Mr[n * ost] = Mc[n];
+  if constexpr (CORR) {
+    if (ca || cb) {
+      double Ml[35], Mc[35];
+      for (int n = 0; n < 35; ++n) Ml[n] = M[n * ist];
+      correct_for_real(Ml, 0, 2, 1, 2, (ca ? 1 : 0) | (cb ? 2 : 0), flag2D, Ma, Mc);
+      for (int n = 0; n < 15; ++n) { a[n] = Mc[WUI[n]]; b[n] = Mc[SLICE[3][n]]; }
+      ea = jac_eigs_t<MODE>(a);
+      if (ea.deferred) return EIG_DEFERRED;
+      eb = jac_eigs_t<MODE>(b);
+      if (eb.deferred) return EIG_DEFERRED;
+      vmin = jmin(ea.vmin, eb.vmin);
+      vmax = jmax(ea.vmax, eb.vmax);
+      for (int n = 0; n < 35; ++n) Mr[n * ost] = Mc[n];
+    }
   }
-  return false;
+  return EIG_DONE;
 }
 HQD void eigenvalues6z(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr, long long ist = 1,
                        long long ost = 1) {
-  eigenvalues6z_t<JAC_ANY>(M, flag2D, Ma, positivity, vmin, vmax, Mr, ist, ost);
+  eigenvalues6z_s<JAC_ANY, true>(M, flag2D, Ma, positivity, vmin, vmax, Mr, ist, ost);
 }
 
 // closure_and_eigenvalues with N = 2: extreme eigenvalues of the 3x3 Jacobi

@@ -34,22 +34,26 @@ struct StepConst {
 #endif
 // The passes over listed cells (complete eigen-solve, corrections) run at the
 // eigenvalue kernels' occupancy (fewer resident blocks with more registers
-// were slower), a grid of FIX_BLOCKS blocks striding over the list.
+// were slower), one thread per possible entry of the list, so that the block
+// scheduler balances the uneven per-cell cost (a persistent grid striding
+// over a long list was 1.5x slower).
 #ifndef HQ_MINB_FIX
 #define HQ_MINB_FIX 8
-#endif
-#ifndef HQ_FIX_BLOCKS
-#define HQ_FIX_BLOCKS (148 * 8)
 #endif
 constexpr int MINB_CLOSURE = HQ_MINB_CLOSURE;
 constexpr int MINB_EIG = HQ_MINB_EIG;
 constexpr int MINB_FIX = HQ_MINB_FIX;
-constexpr int FIX_BLOCKS = HQ_FIX_BLOCKS;
 // Eigen-solve code of those passes (hyq::JacMode; 2 = the general code only)
 #ifndef HQ_FIX_MODE
 #define HQ_FIX_MODE 2
 #endif
 constexpr int FIX_MODE = HQ_FIX_MODE;
+// Eigen-solve code of the eigenvalue kernels themselves (hyq::JacMode; 1 =
+// the pattern-1 register path, the rest left to the passes above)
+#ifndef HQ_EIG_MODE
+#define HQ_EIG_MODE 1
+#endif
+constexpr int EIG_MODE = HQ_EIG_MODE;
 
 constexpr int BS_A = 128;
 constexpr int BS_EF = 128;
@@ -62,8 +66,9 @@ inline int grid_of(long long n, int bs) { return int((n + bs - 1) / bs); }
 // Phase [A] in place on M; Mtmp, Fx, Fy, Fz carry its intermediate states,
 // and on completion Fx, Fy, Fz hold the fluxes (Mtmp is left as scratch).
 // vp: 7N + 2 doubles, the six wave-speed arrays and the list of cells left
-// to the complete eigen-solve.  ev (optional): five events recorded after
-// A1, A2, A3, A4 (each with its pass over listed cells) and A5.  [c0, c1):
+// to the later parts of the eigenvalue stages.  ev (optional): five events
+// recorded after A1, A2, A3, A4 (each with its passes over listed cells) and
+// A5.  [c0, c1):
 // the cells to process (default all; c0 a multiple of BS_A).
 void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, double* Fy, double* Fz, double* vp, double* blockmax,
                     const DevClock* clk, cudaStream_t s, cudaEvent_t* ev = nullptr, long long c0 = 0, long long c1 = -1);

@@ -36,20 +36,20 @@ __device__ __noinline__ void cell_phase_A(const double* m, int flag2D, double Ma
 // instruction fetch); the intermediate states go through buffers that are
 // dead during phase A:  M -A1-> Fx -A2-> Fy -A3-> Fz -A4-> Mtmp -A5-> M, with
 // the Jacobian speeds of A2-A4 parked in vp and combined in A5.
-// The eigenvalue kernels A2-A4 solve only Jacobians of the usual permutation
-// (pattern 1) in their 64-register code and list the cells with any other
-// Jacobian; k_A_fix then runs the complete eigenvalue function on the listed
-// cells, densely packed into warps and with the registers the full 6 x 6
-// eigen-solve needs.  The list lives in vp[6N..7N) (cell indices as unsigned
-// ints, three counters after the first N of them), one list per kernel in
-// turn.
+// Each eigenvalue stage A2-A4 runs in three parts, each with small code: the
+// kernel itself solves pattern-1 Jacobians on its 64-register path and lists
+// every other cell; k_A_fix runs the general eigen-solve on the listed cells
+// (packed densely into warps) and marks those that need the correction of
+// complex eigenvalues; k_A_corr runs the complete function on the marked
+// cells (rare).  The list lives in vp[6N..7N) (entries (cell << 1) | marked,
+// three counters after the first N of them), one list per stage in turn.
 __device__ __forceinline__ bool phase_A_active(const StepConst& sc, const DevClock* clk) {
   return (clk->t < sc.tmax) && (clk->nn < sc.nnmax);
 }
 __device__ __forceinline__ unsigned int* defer_list(double* vp, long long N) { return reinterpret_cast<unsigned int*>(vp + 6 * N); }
 
 // A1: Flux_closure35_and_realizable_3D (realized moments only); also resets
-// the three deferral counters
+// the three list counters
 __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure(const double* __restrict__ M, double* __restrict__ out, double* vp,
                                                               const StepConst sc, const DevClock* clk, long long c0, long long c1) {
   if (!phase_A_active(sc, clk)) return;
@@ -59,38 +59,66 @@ __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure(const double*
   flux_closure35(M + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
 }
 
-// A2/A3: eigenvalues6_hyperbolic_3D along x (axis 1) or y (axis 2); A4
-// (axis 3): eigenvalues6z_hyperbolic_3D.  Deferred cells go to list `axis - 1`.
+// eigenvalues6_hyperbolic_3D along x (axis 1) or y (axis 2), and
+// eigenvalues6z_hyperbolic_3D (axis 3), as a part (MODE, CORR)
+template <int MODE, bool CORR>
+__device__ __forceinline__ int eig_stage(const double* in, double* out, int axis, const StepConst& sc, double& lo, double& hi) {
+  const long long N = sc.N;
+  return axis == 3 ? eigenvalues6z_s<MODE, CORR>(in, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out, N, N)
+                   : eigenvalues6_s<MODE, CORR>(in, axis, sc.flag2D, sc.Ma, lo, hi, out, N, N);
+}
+
+// A2/A3/A4: the pattern-1 part; cells left go to the list, marked when they
+// need the correction
 __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* __restrict__ in, double* __restrict__ out, double* vp,
                                                          int axis, const StepConst sc, const DevClock* clk, long long c0, long long c1) {
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
   if (c >= c1) return;
   double lo, hi;
-  const bool deferred = axis == 3 ? eigenvalues6z_t<JAC_P1>(in + c, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out + c, N, N)
-                                  : eigenvalues6_t<JAC_P1>(in + c, axis, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
-  if (deferred) {
-    unsigned int* list = defer_list(vp, N);
-    list[atomicAdd(list + N + (axis - 1), 1u)] = (unsigned int)c;
-  } else {
+  const int st = eig_stage<EIG_MODE, false>(in + c, out + c, axis, sc, lo, hi);
+  if (st == EIG_DONE) {
     double* v = vp + 2 * (axis - 1) * N;
     v[c] = lo; v[c + N] = hi;
+  } else {
+    unsigned int* list = defer_list(vp, N);
+    list[atomicAdd(list + N + (axis - 1), 1u)] = ((unsigned int)c << 1) | (st == EIG_NEEDS_FIX ? 1u : 0u);
   }
 }
 
-// The listed cells of k_A_eig, grid-stride over the list
+// The general eigen-solve on the unmarked listed cells; marks the ones that
+// need the correction.  One thread per possible entry.
 __global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* __restrict__ in, double* __restrict__ out, double* vp, int axis,
                                                          const StepConst sc, const DevClock* clk) {
+  if (!phase_A_active(sc, clk)) return;
+  const long long N = sc.N;
+  unsigned int* list = defer_list(vp, N);
+  const unsigned int count = list[N + (axis - 1)];
+  double* v = vp + 2 * (axis - 1) * N;
+  for (unsigned int e = blockIdx.x * BS_A + threadIdx.x; e < count; e += gridDim.x * BS_A) {
+    const unsigned int entry = list[e];
+    if (entry & 1u) continue;
+    const long long c = entry >> 1;
+    double lo, hi;
+    if (eig_stage<FIX_MODE, false>(in + c, out + c, axis, sc, lo, hi) == EIG_DONE) { v[c] = lo; v[c + N] = hi; }
+    else list[e] = entry | 1u;
+  }
+}
+
+// The complete function on the marked listed cells
+__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A_corr(const double* __restrict__ in, double* __restrict__ out, double* vp,
+                                                              int axis, const StepConst sc, const DevClock* clk) {
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N;
   const unsigned int* list = defer_list(vp, N);
   const unsigned int count = list[N + (axis - 1)];
   double* v = vp + 2 * (axis - 1) * N;
   for (unsigned int e = blockIdx.x * BS_A + threadIdx.x; e < count; e += gridDim.x * BS_A) {
-    const long long c = list[e];
+    const unsigned int entry = list[e];
+    if (!(entry & 1u)) continue;
+    const long long c = entry >> 1;
     double lo, hi;
-    if (axis == 3) eigenvalues6z_t<FIX_MODE>(in + c, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out + c, N, N);
-    else eigenvalues6_t<FIX_MODE>(in + c, axis, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
+    eig_stage<FIX_MODE, true>(in + c, out + c, axis, sc, lo, hi);
     v[c] = lo; v[c + N] = hi;
   }
 }
@@ -141,18 +169,17 @@ void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, do
   const long long N = sc.N;
   if (c1 < 0) c1 = N;
   const int g = grid_of(c1 - c0, BS_A);
-  const int gfix = g < FIX_BLOCKS ? g : FIX_BLOCKS;
+  const int gfix = g;  // one thread per possible list entry: blocks past the count exit at once
   k_A1_closure<<<g, BS_A, 0, s>>>(M, Fx, vp, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
-  k_A_eig<<<g, BS_A, 0, s>>>(Fx, Fy, vp, 1, sc, clk, c0, c1);
-  k_A_fix<<<gfix, BS_A, 0, s>>>(Fx, Fy, vp, 1, sc, clk);
-  if (ev) cudaEventRecord(ev[1], s);
-  k_A_eig<<<g, BS_A, 0, s>>>(Fy, Fz, vp, 2, sc, clk, c0, c1);
-  k_A_fix<<<gfix, BS_A, 0, s>>>(Fy, Fz, vp, 2, sc, clk);
-  if (ev) cudaEventRecord(ev[2], s);
-  k_A_eig<<<g, BS_A, 0, s>>>(Fz, Mtmp, vp, 3, sc, clk, c0, c1);
-  k_A_fix<<<gfix, BS_A, 0, s>>>(Fz, Mtmp, vp, 3, sc, clk);
-  if (ev) cudaEventRecord(ev[3], s);
+  double* const ins[3] = {Fx, Fy, Fz};
+  double* const outs[3] = {Fy, Fz, Mtmp};
+  for (int axis = 1; axis <= 3; ++axis) {
+    k_A_eig<<<g, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
+    k_A_fix<<<gfix, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk);
+    k_A_corr<<<gfix, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk);
+    if (ev) cudaEventRecord(ev[axis], s);
+  }
   k_A5_flux<<<g, BS_A, 0, s>>>(Mtmp, M, Fx, Fy, Fz, vp, blockmax, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[4], s);
 }

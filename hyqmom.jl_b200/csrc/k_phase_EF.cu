@@ -13,12 +13,13 @@ namespace {
 // intermediate states go through the flux buffers, dead after the HLL sweep:
 //   Mtmp -E1-> Fx -E2-> Fy -E3-> Fz -E4-> M.
 // E2/E3 copy the moments and list the cells whose Jacobians have complex
-// eigenvalues, and the cells with a Jacobian outside the usual permutation
-// (pattern 1, the only one their 64-register code solves); k_E_fix then
-// decides and corrects only those cells, so that a few such cells no longer
-// hold every lane of their warps.  The lists live in the wave-speed buffer
-// vp, dead after the HLL sweep (vp[0..N): entries (cell << 2) | planes,
-// planes = 0 for a cell still to be decided; two counters after them).
+// eigenvalues and the cells with a Jacobian outside the usual permutation
+// (pattern 1, the only one their 64-register code solves); k_E_fix decides
+// the latter with the general eigen-solve and k_E_corr corrects the cells
+// that need it, so that each kernel keeps small code and a few such cells no
+// longer hold every lane of their warps.  The lists live in the wave-speed
+// buffer vp, dead after the HLL sweep (vp[0..N): entries (cell << 2) |
+// planes, planes = 0 for a cell still to be decided; two counters after them).
 __device__ __forceinline__ unsigned int* fix_counters(double* vp, long long N) { return reinterpret_cast<unsigned int*>(vp + N); }
 
 // E1: Flux_closure35_and_realizable_3D; also resets the two fix counters
@@ -38,7 +39,7 @@ __global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* __restr
   if (!clk->active) return;
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
   if (c >= c1) return;
-  const int planes = eigenvalues6_flags_t<JAC_P1>(in + c, axis, N);
+  const int planes = eigenvalues6_flags_t<EIG_MODE>(in + c, axis, N);
 #pragma unroll
   for (int n = 0; n < 35; ++n) out[c + N * n] = in[c + N * n];
   if (planes) {
@@ -47,22 +48,36 @@ __global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* __restr
   }
 }
 
-// The listed cells: the planes from the complete eigen-solve where k_E_eig
-// left them undecided, then the correction
-// (correct_moments_for_real_eigenvalues, as in eigenvalues6); grid-stride
-// over the list
-__global__ void __launch_bounds__(BS_EF, MINB_FIX) k_E_fix(const double* __restrict__ in, double* __restrict__ out, const double* vp,
-                                                           int axis, int which, const StepConst sc, const DevClock* clk) {
+// The undecided listed cells: their planes from the general eigen-solve,
+// written back into the entry.  One thread per possible entry.
+__global__ void __launch_bounds__(BS_EF, MINB_FIX) k_E_fix(const double* __restrict__ in, double* vp, int axis, int which,
+                                                           const StepConst sc, const DevClock* clk) {
+  if (!clk->active) return;
+  const long long N = sc.N;
+  const unsigned int count = reinterpret_cast<const unsigned int*>(vp + N)[which];
+  unsigned long long* list = reinterpret_cast<unsigned long long*>(vp);
+  for (unsigned int e = blockIdx.x * BS_EF + threadIdx.x; e < count; e += gridDim.x * BS_EF) {
+    const unsigned long long v = list[e];
+    if (v & 3ull) continue;
+    const long long c = (long long)(v >> 2);
+    const int planes = eigenvalues6_flags_t<FIX_MODE>(in + c, axis, N);
+    if (planes) list[e] = v | (unsigned long long)planes;
+  }
+}
+
+// The correction of the listed cells that need it
+// (correct_moments_for_real_eigenvalues, as in eigenvalues6)
+__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E_corr(const double* __restrict__ in, double* __restrict__ out, const double* vp,
+                                                                int axis, int which, const StepConst sc, const DevClock* clk) {
   if (!clk->active) return;
   const long long N = sc.N;
   const unsigned int count = reinterpret_cast<const unsigned int*>(vp + N)[which];
   const unsigned long long* list = reinterpret_cast<const unsigned long long*>(vp);
   for (unsigned int e = blockIdx.x * BS_EF + threadIdx.x; e < count; e += gridDim.x * BS_EF) {
     const unsigned long long v = list[e];
+    const int planes = int(v & 3ull);
+    if (!planes) continue;
     const long long c = (long long)(v >> 2);
-    int planes = int(v & 3ull);
-    if (planes == 0) planes = eigenvalues6_flags_t<FIX_MODE>(in + c, axis, N);
-    if (planes == 0) continue;
     double Ml[35], Mc[35];
     for (int n = 0; n < 35; ++n) Ml[n] = in[c + N * n];
     correct_for_real(Ml, 0, 1, axis == 1 ? 0 : 1, 2, planes, sc.flag2D, sc.Ma, Mc);
@@ -89,14 +104,16 @@ void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, doubl
                      const DevClock* clk, cudaStream_t s, cudaEvent_t* ev, long long c0, long long c1) {
   if (c1 < 0) c1 = sc.N;
   const int g = grid_of(c1 - c0, BS_EF);
-  const int gfix = g < FIX_BLOCKS ? g : FIX_BLOCKS;
+  const int gfix = g;  // one thread per possible list entry: blocks past the count exit at once
   k_E1_closure<<<g, BS_EF, 0, s>>>(Min, Fx, vp, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
   k_E_eig<<<g, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk, c0, c1);
-  k_E_fix<<<gfix, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk);
+  k_E_fix<<<gfix, BS_EF, 0, s>>>(Fx, vp, 1, 0, sc, clk);
+  k_E_corr<<<gfix, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk);
   if (ev) cudaEventRecord(ev[1], s);
   k_E_eig<<<g, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk, c0, c1);
-  k_E_fix<<<gfix, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk);
+  k_E_fix<<<gfix, BS_EF, 0, s>>>(Fy, vp, 2, 1, sc, clk);
+  k_E_corr<<<gfix, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk);
   if (ev) cudaEventRecord(ev[2], s);
   k_E4_closure_bgk<<<g, BS_EF, 0, s>>>(Fz, Mout, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[3], s);

@@ -17,14 +17,21 @@ void sh_flux(const double* m, int flag2D, double Ma, double* Fx, double* Fy, dou
 void sh_eig(const double* m, int axis, int flag2D, double Ma, int pos, double* v, double* Mr) {
   if (axis == 3) eigenvalues6z(m, flag2D, Ma, pos, v[0], v[1], Mr); else eigenvalues6(m, axis, flag2D, Ma, v[0], v[1], Mr);
 }
-// the pattern-1-only variant the step kernels run first: 1 when it left the
-// cell to the complete function (outputs then not meaningful)
-int sh_eig_fast(const double* m, int axis, int flag2D, double Ma, int pos, double* v, double* Mr) {
-  if (axis == 3) return eigenvalues6z_t<JAC_P1>(m, flag2D, Ma, pos, v[0], v[1], Mr, 1, 1) ? 1 : 0;
-  return eigenvalues6_t<JAC_P1>(m, axis, flag2D, Ma, v[0], v[1], Mr, 1, 1) ? 1 : 0;
+// the parts the step kernels run before the correction pass: gen = 0 the
+// pattern-1-only variant, 1 the general code; 0 done, 1 deferred, 2
+// correction needed (outputs then incomplete)
+int sh_eig_part(const double* m, int axis, int flag2D, double Ma, int pos, int gen, double* v, double* Mr) {
+  if (gen) {
+    if (axis == 3) return eigenvalues6z_s<JAC_GEN, false>(m, flag2D, Ma, pos, v[0], v[1], Mr, 1, 1);
+    return eigenvalues6_s<JAC_GEN, false>(m, axis, flag2D, Ma, v[0], v[1], Mr, 1, 1);
+  }
+  if (axis == 3) return eigenvalues6z_s<JAC_P1, false>(m, flag2D, Ma, pos, v[0], v[1], Mr, 1, 1);
+  return eigenvalues6_s<JAC_P1, false>(m, axis, flag2D, Ma, v[0], v[1], Mr, 1, 1);
 }
-int sh_eig_flags(const double* m, int axis, int fast) {
-  return fast ? eigenvalues6_flags_t<JAC_P1>(m, axis, 1) : eigenvalues6_flags_t<JAC_ANY>(m, axis, 1);
+int sh_eig_flags(const double* m, int axis, int mode) {
+  if (mode == 1) return eigenvalues6_flags_t<JAC_P1>(m, axis, 1);
+  if (mode == 2) return eigenvalues6_flags_t<JAC_GEN>(m, axis, 1);
+  return eigenvalues6_flags_t<JAC_ANY>(m, axis, 1);
 }
 void sh_closure(const double* mom, double* v) { closure_eigs(mom[0], mom[1], mom[2], mom[3], mom[4], v[0], v[1]); }
 void sh_coll(double* m, double dt, double Kn, int pos) { collision35(m, dt, Kn, pos); }

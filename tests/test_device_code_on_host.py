@@ -112,33 +112,39 @@ def test_fast_eigen_path_is_bitwise_general(shim, states):
     assert seen[1] > 100 and seen[0] > 300, seen
 
 
-def test_pattern1_only_variant_defers_or_agrees(shim, states):
-    """The step kernels' first pass solves only pattern-1 Jacobians: on every
-    cell (the evolved states and copies whose first Jacobian column carries
-    round-off-sized entries) it either leaves the cell to the complete function
-    or gives its results bit for bit; the flag variant likewise."""
+def test_kernel_parts_defer_or_agree(shim, states):
+    """The step kernels run the eigenvalue functions in parts: the pattern-1
+    register path first, the general code on the cells it left, and the
+    correction last.  On every cell (the evolved states and copies whose first
+    Jacobian column carries round-off-sized entries) each part either leaves
+    the cell to a later one or gives the complete function's results bit for
+    bit; the flag variants likewise."""
     rng = np.random.default_rng(11)
     cells = [np.ascontiguousarray(m) for m in states]
     for m in states[rng.choice(len(states), 200, replace=False)]:
         k = m.copy()
         k[rng.choice([16, 25, 26, 27, 28, 29, 30, 31, 32, 33, 34], 2, replace=False)] *= 1.0 + 1e-15
         cells.append(np.ascontiguousarray(k))
-    shim.sh_eig_fast.restype = ctypes.c_int
+    shim.sh_eig_part.restype = ctypes.c_int
     shim.sh_eig_flags.restype = ctypes.c_int
-    deferred = kept = 0
+    seen = {(g, st): 0 for g in (0, 1) for st in (0, 1, 2)}
     for m in cells:
         for ax in (1, 2, 3):
-            v, Mr, v2, Mr2 = np.zeros(2), np.zeros(35), np.zeros(2), np.zeros(35)
+            v, Mr = np.zeros(2), np.zeros(35)
             shim.sh_eig(P(m), ax, 0, ctypes.c_double(0.0), 1, P(v), P(Mr))
-            if shim.sh_eig_fast(P(m), ax, 0, ctypes.c_double(0.0), 1, P(v2), P(Mr2)):
-                deferred += 1
-            else:
-                kept += 1
-                assert np.array_equal(v, v2, equal_nan=True) and np.array_equal(Mr, Mr2, equal_nan=True), ax
+            for gen in (0, 1):
+                v2, Mr2 = np.zeros(2), np.zeros(35)
+                st = shim.sh_eig_part(P(m), ax, 0, ctypes.c_double(0.0), 1, gen, P(v2), P(Mr2))
+                seen[(gen, st)] += 1
+                assert st in (0, 1, 2) and not (gen and st == 1)
+                if st == 0:
+                    assert np.array_equal(v, v2, equal_nan=True) and np.array_equal(Mr, Mr2, equal_nan=True), (ax, gen)
             if ax < 3:
+                full = shim.sh_eig_flags(P(m), ax, 0)
                 f = shim.sh_eig_flags(P(m), ax, 1)
-                assert f == -1 or f == shim.sh_eig_flags(P(m), ax, 0)
-    assert kept > 100 and deferred > 100, (kept, deferred)
+                assert f == -1 or f == full
+                assert shim.sh_eig_flags(P(m), ax, 2) == full
+    assert seen[(0, 0)] > 100 and seen[(0, 1)] > 100 and seen[(1, 0)] > 100 and seen[(1, 2)] > 0, seen
 
 
 def test_reciprocal_division_is_ieee_division(shim):
