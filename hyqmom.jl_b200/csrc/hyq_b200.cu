@@ -173,6 +173,7 @@ __global__ void __launch_bounds__(BS_HLL, HQ_MINB_HLL) k_hll(const double* __res
 
 __global__ void k_set_clock(DevClock* clk, double t, long long nn) {
   clk->t = t; clk->nn = nn; clk->dt = 0.0; clk->vmax = 0.0; clk->active = 0; clk->status = 0;
+  for (int q = 0; q < 5; ++q) clk->dense[q] = 0;
 }
 
 

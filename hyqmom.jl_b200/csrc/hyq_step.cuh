@@ -11,6 +11,10 @@ struct DevClock {
   long long nn;
   int active;  // 1 while the current step runs
   int status;
+  // per eigenvalue stage (A x, y, z, E x, y): runs left in which the general
+  // eigen-solve takes every cell directly (set when a stage listed most of its
+  // cells; 0: the pattern-1 kernel first)
+  int dense[5];
 };
 
 // Per-context constants of the step.
@@ -54,6 +58,9 @@ constexpr int FIX_MODE = HQ_FIX_MODE;
 #define HQ_EIG_MODE 1
 #endif
 constexpr int EIG_MODE = HQ_EIG_MODE;
+// A stage that listed more than 3/4 of its cells runs dense for the next
+// DENSE_RUNS runs, then tries the pattern-1 kernel again.
+constexpr int DENSE_RUNS = 16;
 
 constexpr int BS_A = 128;
 constexpr int BS_EF = 128;
@@ -71,12 +78,12 @@ inline int grid_of(long long n, int bs) { return int((n + bs - 1) / bs); }
 // A5.  [c0, c1):
 // the cells to process (default all; c0 a multiple of BS_A).
 void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, double* Fy, double* Fz, double* vp, double* blockmax,
-                    const DevClock* clk, cudaStream_t s, cudaEvent_t* ev = nullptr, long long c0 = 0, long long c1 = -1);
+                    DevClock* clk, cudaStream_t s, cudaEvent_t* ev = nullptr, long long c0 = 0, long long c1 = -1);
 // Phases [E]+[F] from Min to Mout; Fx, Fy, Fz are overwritten and vp (6N
 // doubles, dead after the HLL sweep) holds the correction lists.
 // ev (optional): four events recorded after E1, E2, E3 and E4.
 void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, double* Fx, double* Fy, double* Fz, double* vp,
-                     const DevClock* clk, cudaStream_t s, cudaEvent_t* ev = nullptr, long long c0 = 0, long long c1 = -1);
+                     DevClock* clk, cudaStream_t s, cudaEvent_t* ev = nullptr, long long c0 = 0, long long c1 = -1);
 void launch_cells_phase_A(const double* M, long long n, int flag2D, double Ma, int positivity, double* Fx, double* Fy, double* Fz,
                           double* Mr, double* vp, cudaStream_t s);
 void launch_cells_flux(const double* M, long long n, int flag2D, double Ma, double* Fx, double* Fy, double* Fz, double* Mr, cudaStream_t s);

@@ -43,6 +43,9 @@ __device__ __noinline__ void cell_phase_A(const double* m, int flag2D, double Ma
 // complex eigenvalues; k_A_corr runs the complete function on the marked
 // cells (rare).  The list lives in vp[6N..7N) (entries (cell << 1) | marked,
 // three counters after the first N of them), one list per stage in turn.
+// Late in a developed flow nearly every cell is listed; a stage then runs
+// dense for a while (DevClock::dense): k_A_eig returns at once and k_A_fix
+// takes every cell of the range, listing only those to correct.
 __device__ __forceinline__ bool phase_A_active(const StepConst& sc, const DevClock* clk) {
   return (clk->t < sc.tmax) && (clk->nn < sc.nnmax);
 }
@@ -72,7 +75,7 @@ __device__ __forceinline__ int eig_stage(const double* in, double* out, int axis
 // need the correction
 __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* __restrict__ in, double* __restrict__ out, double* vp,
                                                          int axis, const StepConst sc, const DevClock* clk, long long c0, long long c1) {
-  if (!phase_A_active(sc, clk)) return;
+  if (!phase_A_active(sc, clk) || clk->dense[axis - 1]) return;
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
   if (c >= c1) return;
   double lo, hi;
@@ -86,33 +89,47 @@ __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* __restri
   }
 }
 
-// The general eigen-solve on the unmarked listed cells; marks the ones that
-// need the correction.  One thread per possible entry.
+// The general eigen-solve on the unmarked listed cells (dense: on every cell
+// of the range); marks (lists) the ones that need the correction.  One thread
+// per possible entry.
 __global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* __restrict__ in, double* __restrict__ out, double* vp, int axis,
-                                                         const StepConst sc, const DevClock* clk) {
+                                                         const StepConst sc, const DevClock* clk, long long c0, long long c1) {
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N;
   unsigned int* list = defer_list(vp, N);
-  const unsigned int count = list[N + (axis - 1)];
   double* v = vp + 2 * (axis - 1) * N;
+  double lo, hi;
+  if (clk->dense[axis - 1]) {
+    const long long c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
+    if (c >= c1) return;
+    if (eig_stage<FIX_MODE, false>(in + c, out + c, axis, sc, lo, hi) == EIG_DONE) { v[c] = lo; v[c + N] = hi; }
+    else list[atomicAdd(list + N + (axis - 1), 1u)] = ((unsigned int)c << 1) | 1u;
+    return;
+  }
+  const unsigned int count = list[N + (axis - 1)];
   for (unsigned int e = blockIdx.x * BS_A + threadIdx.x; e < count; e += gridDim.x * BS_A) {
     const unsigned int entry = list[e];
     if (entry & 1u) continue;
     const long long c = entry >> 1;
-    double lo, hi;
     if (eig_stage<FIX_MODE, false>(in + c, out + c, axis, sc, lo, hi) == EIG_DONE) { v[c] = lo; v[c + N] = hi; }
     else list[e] = entry | 1u;
   }
 }
 
-// The complete function on the marked listed cells
+// The complete function on the marked listed cells; the first thread then
+// decides whether the stage runs dense next time
 __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A_corr(const double* __restrict__ in, double* __restrict__ out, double* vp,
-                                                              int axis, const StepConst sc, const DevClock* clk) {
+                                                              int axis, const StepConst sc, DevClock* clk, long long c0, long long c1) {
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N;
   const unsigned int* list = defer_list(vp, N);
   const unsigned int count = list[N + (axis - 1)];
   double* v = vp + 2 * (axis - 1) * N;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int& d = clk->dense[axis - 1];
+    if (d > 0) d = d - 1;
+    else if ((long long)count * 4 > (c1 - c0) * 3) d = DENSE_RUNS;
+  }
   for (unsigned int e = blockIdx.x * BS_A + threadIdx.x; e < count; e += gridDim.x * BS_A) {
     const unsigned int entry = list[e];
     if (!(entry & 1u)) continue;
@@ -165,7 +182,7 @@ __global__ void __launch_bounds__(BS_CELLS) k_cells_phase_A(const double* __rest
 }  // namespace
 
 void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, double* Fy, double* Fz, double* vp, double* blockmax,
-                    const DevClock* clk, cudaStream_t s, cudaEvent_t* ev, long long c0, long long c1) {
+                    DevClock* clk, cudaStream_t s, cudaEvent_t* ev, long long c0, long long c1) {
   const long long N = sc.N;
   if (c1 < 0) c1 = N;
   const int g = grid_of(c1 - c0, BS_A);
@@ -176,8 +193,8 @@ void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, do
   double* const outs[3] = {Fy, Fz, Mtmp};
   for (int axis = 1; axis <= 3; ++axis) {
     k_A_eig<<<g, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
-    k_A_fix<<<gfix, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk);
-    k_A_corr<<<gfix, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk);
+    k_A_fix<<<gfix, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
+    k_A_corr<<<gfix, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
     if (ev) cudaEventRecord(ev[axis], s);
   }
   k_A5_flux<<<g, BS_A, 0, s>>>(Mtmp, M, Fx, Fy, Fz, vp, blockmax, sc, clk, c0, c1);

@@ -20,6 +20,9 @@ namespace {
 // longer hold every lane of their warps.  The lists live in the wave-speed
 // buffer vp, dead after the HLL sweep (vp[0..N): entries (cell << 2) |
 // planes, planes = 0 for a cell still to be decided; two counters after them).
+// A stage that listed most of its cells runs dense for a while
+// (DevClock::dense): k_E_eig only copies and k_E_fix decides every cell,
+// listing those to correct.
 __device__ __forceinline__ unsigned int* fix_counters(double* vp, long long N) { return reinterpret_cast<unsigned int*>(vp + N); }
 
 // E1: Flux_closure35_and_realizable_3D; also resets the two fix counters
@@ -39,7 +42,8 @@ __global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* __restr
   if (!clk->active) return;
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
   if (c >= c1) return;
-  const int planes = eigenvalues6_flags_t<EIG_MODE>(in + c, axis, N);
+  const bool dense = clk->dense[3 + which] != 0;
+  const int planes = dense ? 0 : eigenvalues6_flags_t<EIG_MODE>(in + c, axis, N);
 #pragma unroll
   for (int n = 0; n < 35; ++n) out[c + N * n] = in[c + N * n];
   if (planes) {
@@ -48,14 +52,22 @@ __global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* __restr
   }
 }
 
-// The undecided listed cells: their planes from the general eigen-solve,
-// written back into the entry.  One thread per possible entry.
+// The undecided listed cells (dense: every cell of the range): their planes
+// from the general eigen-solve, written back into the entry (dense: listed).
+// One thread per possible entry.
 __global__ void __launch_bounds__(BS_EF, MINB_FIX) k_E_fix(const double* __restrict__ in, double* vp, int axis, int which,
-                                                           const StepConst sc, const DevClock* clk) {
+                                                           const StepConst sc, const DevClock* clk, long long c0, long long c1) {
   if (!clk->active) return;
   const long long N = sc.N;
-  const unsigned int count = reinterpret_cast<const unsigned int*>(vp + N)[which];
   unsigned long long* list = reinterpret_cast<unsigned long long*>(vp);
+  if (clk->dense[3 + which]) {
+    const long long c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
+    if (c >= c1) return;
+    const int planes = eigenvalues6_flags_t<FIX_MODE>(in + c, axis, N);
+    if (planes) list[atomicAdd(fix_counters(vp, N) + which, 1u)] = ((unsigned long long)c << 2) | (unsigned long long)planes;
+    return;
+  }
+  const unsigned int count = reinterpret_cast<const unsigned int*>(vp + N)[which];
   for (unsigned int e = blockIdx.x * BS_EF + threadIdx.x; e < count; e += gridDim.x * BS_EF) {
     const unsigned long long v = list[e];
     if (v & 3ull) continue;
@@ -66,13 +78,20 @@ __global__ void __launch_bounds__(BS_EF, MINB_FIX) k_E_fix(const double* __restr
 }
 
 // The correction of the listed cells that need it
-// (correct_moments_for_real_eigenvalues, as in eigenvalues6)
+// (correct_moments_for_real_eigenvalues, as in eigenvalues6); the first thread
+// then decides whether the stage runs dense next time
 __global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E_corr(const double* __restrict__ in, double* __restrict__ out, const double* vp,
-                                                                int axis, int which, const StepConst sc, const DevClock* clk) {
+                                                                int axis, int which, const StepConst sc, DevClock* clk, long long c0,
+                                                                long long c1) {
   if (!clk->active) return;
   const long long N = sc.N;
   const unsigned int count = reinterpret_cast<const unsigned int*>(vp + N)[which];
   const unsigned long long* list = reinterpret_cast<const unsigned long long*>(vp);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int& d = clk->dense[3 + which];
+    if (d > 0) d = d - 1;
+    else if ((long long)count * 4 > (c1 - c0) * 3) d = DENSE_RUNS;
+  }
   for (unsigned int e = blockIdx.x * BS_EF + threadIdx.x; e < count; e += gridDim.x * BS_EF) {
     const unsigned long long v = list[e];
     const int planes = int(v & 3ull);
@@ -101,19 +120,19 @@ __global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E4_closure_bgk(const do
 }  // namespace
 
 void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, double* Fx, double* Fy, double* Fz, double* vp,
-                     const DevClock* clk, cudaStream_t s, cudaEvent_t* ev, long long c0, long long c1) {
+                     DevClock* clk, cudaStream_t s, cudaEvent_t* ev, long long c0, long long c1) {
   if (c1 < 0) c1 = sc.N;
   const int g = grid_of(c1 - c0, BS_EF);
   const int gfix = g;  // one thread per possible list entry: blocks past the count exit at once
   k_E1_closure<<<g, BS_EF, 0, s>>>(Min, Fx, vp, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
   k_E_eig<<<g, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk, c0, c1);
-  k_E_fix<<<gfix, BS_EF, 0, s>>>(Fx, vp, 1, 0, sc, clk);
-  k_E_corr<<<gfix, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk);
+  k_E_fix<<<gfix, BS_EF, 0, s>>>(Fx, vp, 1, 0, sc, clk, c0, c1);
+  k_E_corr<<<gfix, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[1], s);
   k_E_eig<<<g, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk, c0, c1);
-  k_E_fix<<<gfix, BS_EF, 0, s>>>(Fy, vp, 2, 1, sc, clk);
-  k_E_corr<<<gfix, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk);
+  k_E_fix<<<gfix, BS_EF, 0, s>>>(Fy, vp, 2, 1, sc, clk, c0, c1);
+  k_E_corr<<<gfix, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[2], s);
   k_E4_closure_bgk<<<g, BS_EF, 0, s>>>(Fz, Mout, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[3], s);
