@@ -8,7 +8,7 @@ run as the flow develops, so a window of early steps would not represent
 it).  The state (573 MB) and the flux buffers exceed L2 (126 MB), so no L2
 flush is needed between steps.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--from-step S] [--impl reference]
 
 Multi-GPU: independent replicas (one domain per rank, no data-path
 collective); value = all ranks' cell-steps / max-over-ranks time.
@@ -237,8 +237,14 @@ def run_gpu(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # the timed steps: 1..K from the initial condition (set_state resets t, nn)
-    s.set_state(M0)
+    # the timed steps: S+1..S+K of the run from the initial condition
+    # (set_state resets t and nn; S = --from-step, 0 by default)
+    def restart():
+        s.set_state(M0)
+        if args.from_step:
+            s.advance(args.from_step)
+
+    restart()
     barrier()
     sampler = ClockSampler(local_rank)
     with sampler:
@@ -250,14 +256,14 @@ def run_gpu(args, rank, world, local_rank):
         barrier()
     ms = e0.elapsed_time(e1)
     st = s.stats()
-    assert st["status"] == 0 and st["nn"] == args.steps, f"steps did not all run: {st}"
+    assert st["status"] == 0 and st["nn"] == args.from_step + args.steps, f"steps did not all run: {st}"
     ms = max_over_ranks(ms, dist, "cuda")
     value = replica_throughput(world, cells, args.steps, ms)
 
     # per-kernel device time over the same steps (individual launches, CUDA
     # events on the context stream)
     import ctypes
-    s.set_state(M0)
+    restart()
     kms = (ctypes.c_float * len(KERNELS))()
     s._chk(s._lib.hyq_advance_timed(s._h, args.steps, kms))
     kern = {k: kms[i] / args.steps for i, k in enumerate(KERNELS)}
@@ -267,16 +273,16 @@ def run_gpu(args, rank, world, local_rank):
     # copies overlapped slab by slab with the per-cell phases).  Slabs of the
     # state at four points of the run are kept (outside the timing) for the
     # CPU baseline.
-    s.set_state(M0)
+    restart()
     Mh_flat = torch.empty(35 * cells, dtype=torch.float64).pin_memory()
     Mh = Mh_flat.numpy().reshape(M0.shape, order="F")
-    Mh[...] = M0
-    marks = sorted({(args.steps * q) // 4 for q in range(4)})
+    s._chk(s._lib.hyq_get_state(s._h, ctypes.c_void_p(Mh_flat.data_ptr())))
+    marks = sorted({(args.steps * q) // 4 for q in range(4)})  # offsets into the timed steps
     slabs = []
     e2e_s = 0.0
     for k in range(args.steps):
         if k in marks:
-            slabs.append((k, slab_of(Mh, 8)))
+            slabs.append((args.from_step + k, slab_of(Mh, 8)))
         t0 = time.perf_counter()
         s.step_host(Mh, nslabs=E2E_SLABS)
         e2e_s += time.perf_counter() - t0
@@ -308,7 +314,8 @@ def run_gpu(args, rank, world, local_rank):
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (reference crossing-jets IC generator)",
             "config": {"workload": f"crossing jets {p['Nx']}x{p['Ny']}x{p['Nz']} Ma={p['Ma']} Kn={p['Kn']} CFL={p['CFL']}, plain eig",
-                       "cells": cells, "parallelism": f"replicas x{world}", "timed_steps": f"1-{args.steps} from the initial condition",
+                       "cells": cells, "parallelism": f"replicas x{world}",
+                       "timed_steps": f"{args.from_step + 1}-{args.from_step + args.steps} from the initial condition",
                        "l2": f"state {cells * 35 * 8 / 1e6:.0f} MB > L2 (126 MB), no flush needed",
                        "steps_done": st["nn"]},
             "gpu_launches": LAUNCHES_PER_STEP * args.steps, "e2e": e2e, "roofline": roof, "clocks": sampler.summary()}
@@ -435,6 +442,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--from-step", type=int, default=0, help="untimed steps from the initial condition before the timed ones")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c2s", "c4", "c5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

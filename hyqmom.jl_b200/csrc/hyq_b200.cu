@@ -249,8 +249,8 @@ int hyq_create(const hyq_params* p, hyq_ctx** out) {
     return fail(nullptr, HYQ_EINVAL, "grid must have Nx >= 2, Ny >= 2, Nz >= 1 (pas_HLL needs two cells per row)");
   if (!(p->CFL > 0) || !(p->Kn > 0) || !(p->dtmax > 0))
     return fail(nullptr, HYQ_EINVAL, "CFL, Kn and dtmax must be positive");
-  if ((long long)p->Nx * p->Ny * p->Nz >= (1LL << 31))
-    return fail(nullptr, HYQ_EINVAL, "grid must have fewer than 2^31 cells (in-line offsets are 32-bit)");
+  if ((long long)p->Nx * p->Ny * p->Nz >= (1LL << 29))
+    return fail(nullptr, HYQ_EINVAL, "grid must have fewer than 2^29 cells (the step's cell lists hold 32-bit entries)");
   hyq_ctx* ctx = new hyq_ctx();
   ctx->p = *p;
   ctx->device = p->device;

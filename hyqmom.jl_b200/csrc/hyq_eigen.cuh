@@ -513,7 +513,7 @@ enum EigStatus { EIG_DONE = 0, EIG_DEFERRED = 1, EIG_NEEDS_FIX = 2 };
 // of the caller.  vmin, vmax and Mr are complete only with EIG_DONE.
 template <int MODE, bool CORR>
 HQN int eigenvalues6_s(const double* M, int axis, int flag2D, double Ma, double& vmin, double& vmax, double* Mr, long long ist,
-                       long long ost) {
+                       long long ost, int* planes = nullptr) {
   const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
   double a[15], b[15];
   for (int n = 0; n < 15; ++n) { a[n] = M[SLICE[sa][n] * ist]; b[n] = M[SLICE[sb][n] * ist]; }
@@ -523,7 +523,10 @@ HQN int eigenvalues6_s(const double* M, int axis, int flag2D, double Ma, double&
   if (eb.deferred) return EIG_DEFERRED;
   const double thr = 1000.0 * EPS;
   const bool ca = ea.imax > thr, cb = eb.imax > thr;
-  if (!CORR && (ca || cb)) return EIG_NEEDS_FIX;
+  if (!CORR && (ca || cb)) {
+    if (planes) *planes = (ca ? 1 : 0) | (cb ? 2 : 0);
+    return EIG_NEEDS_FIX;
+  }
   auto combine = [&]() {
     vmin = ea.vmin; vmax = ea.vmax;
     if (eb.vmin == eb.vmin || eb.vmax == eb.vmax) { vmin = jmin(vmin, eb.vmin); vmax = jmax(vmax, eb.vmax); }
@@ -553,6 +556,23 @@ HQD void eigenvalues6(const double* M, int axis, int flag2D, double Ma, double& 
   eigenvalues6_s<JAC_ANY, true>(M, axis, flag2D, Ma, vmin, vmax, Mr, ist, ost);
 }
 
+// The end of eigenvalues6 for a cell whose planes need the correction
+// (planes as eigenvalues6_s reported them): the corrected moments and their
+// speeds, the same results as the complete function.
+template <int MODE>
+HQN void eigenvalues6_corrected(const double* M, int axis, int planes, int flag2D, double Ma, double& vmin, double& vmax, double* Mr,
+                                long long ist, long long ost) {
+  const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
+  double Ml[35], Mc[35], a[15], b[15];
+  for (int n = 0; n < 35; ++n) Ml[n] = M[n * ist];
+  correct_for_real(Ml, 0, 1, axis == 1 ? 0 : 1, 2, planes, flag2D, Ma, Mc);
+  for (int n = 0; n < 15; ++n) { a[n] = Mc[SLICE[sa][n]]; b[n] = Mc[SLICE[sb][n]]; }
+  const EigOut ea = jac_eigs_t<MODE>(a), eb = jac_eigs_t<MODE>(b);
+  vmin = ea.vmin; vmax = ea.vmax;
+  if (eb.vmin == eb.vmin || eb.vmax == eb.vmax) { vmin = jmin(vmin, eb.vmin); vmax = jmax(vmax, eb.vmax); }
+  for (int n = 0; n < 35; ++n) Mr[n * ost] = Mc[n];
+}
+
 // Which of eigenvalues6's two planes need the complex-eigenvalue correction
 // (bit 0: first slice, bit 1: second), from the same Jacobians and the same
 // test; phase E only needs the corrected moments, so its kernels decide here
@@ -575,7 +595,7 @@ template <int MODE> HQN int eigenvalues6_flags_t(const double* M, int axis, long
 // returns EIG_NEEDS_FIX)
 template <int MODE, bool CORR>
 HQN int eigenvalues6z_s(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr, long long ist,
-                        long long ost) {
+                        long long ost, int* planes = nullptr) {
   double Mw[35];
 #pragma unroll
   for (int n = 0; n < 35; ++n) Mw[n] = M[n * ist];
@@ -586,7 +606,10 @@ HQN int eigenvalues6z_s(const double* M, int flag2D, double Ma, int positivity, 
                  vz = M[19 * ist] / m000 - sq(M[15 * ist] / m000);
     if (vx < 0.0 || vy < 0.0 || vz < 0.0) {
       if constexpr (CORR) flux_closure35(M, flag2D, Ma, nullptr, nullptr, nullptr, Mw, ist, 1);
-      else return EIG_NEEDS_FIX;
+      else {
+        if (planes) *planes = 0;  // the re-realization: only the complete function
+        return EIG_NEEDS_FIX;
+      }
     }
   }
   double a[15], b[15];
@@ -597,7 +620,10 @@ HQN int eigenvalues6z_s(const double* M, int flag2D, double Ma, int positivity, 
   if (eb.deferred) return EIG_DEFERRED;
   const double thr = 1000.0 * EPS;
   const bool ca = ea.imax > thr, cb = eb.imax > thr;
-  if (!CORR && (ca || cb)) return EIG_NEEDS_FIX;
+  if (!CORR && (ca || cb)) {
+    if (planes) *planes = (ca ? 1 : 0) | (cb ? 2 : 0);
+    return EIG_NEEDS_FIX;
+  }
   // Mr: the input with its density floored or, after the negative-variance
   // re-realization, that closure -- Mw in both cases
 #pragma unroll
@@ -624,6 +650,21 @@ HQN int eigenvalues6z_s(const double* M, int flag2D, double Ma, int positivity, 
 HQD void eigenvalues6z(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr, long long ist = 1,
                        long long ost = 1) {
   eigenvalues6z_s<JAC_ANY, true>(M, flag2D, Ma, positivity, vmin, vmax, Mr, ist, ost);
+}
+
+// The end of eigenvalues6z for a cell whose planes need the correction
+// (the correction starts from the input moments, not the floored ones)
+template <int MODE>
+HQN void eigenvalues6z_corrected(const double* M, int planes, int flag2D, double Ma, double& vmin, double& vmax, double* Mr,
+                                 long long ist, long long ost) {
+  double Ml[35], Mc[35], a[15], b[15];
+  for (int n = 0; n < 35; ++n) Ml[n] = M[n * ist];
+  correct_for_real(Ml, 0, 2, 1, 2, planes, flag2D, Ma, Mc);
+  for (int n = 0; n < 15; ++n) { a[n] = Mc[WUI[n]]; b[n] = Mc[SLICE[3][n]]; }
+  const EigOut ea = jac_eigs_t<MODE>(a), eb = jac_eigs_t<MODE>(b);
+  vmin = jmin(ea.vmin, eb.vmin);
+  vmax = jmax(ea.vmax, eb.vmax);
+  for (int n = 0; n < 35; ++n) Mr[n * ost] = Mc[n];
 }
 
 // closure_and_eigenvalues with N = 2: extreme eigenvalues of the 3x3 Jacobi

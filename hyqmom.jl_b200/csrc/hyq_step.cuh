@@ -61,6 +61,9 @@ constexpr int EIG_MODE = HQ_EIG_MODE;
 // A stage that listed more than 3/4 of its cells runs dense for the next
 // DENSE_RUNS runs, then tries the pattern-1 kernel again.
 constexpr int DENSE_RUNS = 16;
+// The correction passes (few cells, or none) stride over their list with at
+// most one wave of blocks.
+constexpr int CORR_BLOCKS = 148 * 4;
 
 constexpr int BS_A = 128;
 constexpr int BS_EF = 128;

@@ -40,9 +40,11 @@ __device__ __noinline__ void cell_phase_A(const double* m, int flag2D, double Ma
 // kernel itself solves pattern-1 Jacobians on its 64-register path and lists
 // every other cell; k_A_fix runs the general eigen-solve on the listed cells
 // (packed densely into warps) and marks those that need the correction of
-// complex eigenvalues; k_A_corr runs the complete function on the marked
-// cells (rare).  The list lives in vp[6N..7N) (entries (cell << 1) | marked,
-// three counters after the first N of them), one list per stage in turn.
+// complex eigenvalues; k_A_corr finishes the marked cells (rare) from the
+// planes to correct.  The list lives in vp[6N..7N) (entries (cell << 3) |
+// code, code 0 = to solve, 1-3 = the planes to correct, 4 = the complete
+// function; three counters after the first N entries), one list per stage in
+// turn.
 // Late in a developed flow nearly every cell is listed; a stage then runs
 // dense for a while (DevClock::dense): k_A_eig returns at once and k_A_fix
 // takes every cell of the range, listing only those to correct.
@@ -63,12 +65,17 @@ __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure(const double*
 }
 
 // eigenvalues6_hyperbolic_3D along x (axis 1) or y (axis 2), and
-// eigenvalues6z_hyperbolic_3D (axis 3), as a part (MODE, CORR)
+// eigenvalues6z_hyperbolic_3D (axis 3), as a part (MODE, CORR); a cell left
+// for the correction gets its list code in *code
 template <int MODE, bool CORR>
-__device__ __forceinline__ int eig_stage(const double* in, double* out, int axis, const StepConst& sc, double& lo, double& hi) {
+__device__ __forceinline__ int eig_stage(const double* in, double* out, int axis, const StepConst& sc, double& lo, double& hi,
+                                         unsigned int* code = nullptr) {
   const long long N = sc.N;
-  return axis == 3 ? eigenvalues6z_s<MODE, CORR>(in, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out, N, N)
-                   : eigenvalues6_s<MODE, CORR>(in, axis, sc.flag2D, sc.Ma, lo, hi, out, N, N);
+  int planes = 0;
+  const int st = axis == 3 ? eigenvalues6z_s<MODE, CORR>(in, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out, N, N, &planes)
+                           : eigenvalues6_s<MODE, CORR>(in, axis, sc.flag2D, sc.Ma, lo, hi, out, N, N, &planes);
+  if (code) *code = st == EIG_NEEDS_FIX ? (planes ? (unsigned int)planes : 4u) : 0u;
+  return st;
 }
 
 // A2/A3/A4: the pattern-1 part; cells left go to the list, marked when they
@@ -79,13 +86,13 @@ __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* __restri
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
   if (c >= c1) return;
   double lo, hi;
-  const int st = eig_stage<EIG_MODE, false>(in + c, out + c, axis, sc, lo, hi);
-  if (st == EIG_DONE) {
+  unsigned int code;
+  if (eig_stage<EIG_MODE, false>(in + c, out + c, axis, sc, lo, hi, &code) == EIG_DONE) {
     double* v = vp + 2 * (axis - 1) * N;
     v[c] = lo; v[c + N] = hi;
   } else {
     unsigned int* list = defer_list(vp, N);
-    list[atomicAdd(list + N + (axis - 1), 1u)] = ((unsigned int)c << 1) | (st == EIG_NEEDS_FIX ? 1u : 0u);
+    list[atomicAdd(list + N + (axis - 1), 1u)] = ((unsigned int)c << 3) | code;
   }
 }
 
@@ -99,20 +106,21 @@ __global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* __restri
   unsigned int* list = defer_list(vp, N);
   double* v = vp + 2 * (axis - 1) * N;
   double lo, hi;
+  unsigned int code;
   if (clk->dense[axis - 1]) {
     const long long c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
     if (c >= c1) return;
-    if (eig_stage<FIX_MODE, false>(in + c, out + c, axis, sc, lo, hi) == EIG_DONE) { v[c] = lo; v[c + N] = hi; }
-    else list[atomicAdd(list + N + (axis - 1), 1u)] = ((unsigned int)c << 1) | 1u;
+    if (eig_stage<FIX_MODE, false>(in + c, out + c, axis, sc, lo, hi, &code) == EIG_DONE) { v[c] = lo; v[c + N] = hi; }
+    else list[atomicAdd(list + N + (axis - 1), 1u)] = ((unsigned int)c << 3) | code;
     return;
   }
   const unsigned int count = list[N + (axis - 1)];
   for (unsigned int e = blockIdx.x * BS_A + threadIdx.x; e < count; e += gridDim.x * BS_A) {
     const unsigned int entry = list[e];
-    if (entry & 1u) continue;
-    const long long c = entry >> 1;
-    if (eig_stage<FIX_MODE, false>(in + c, out + c, axis, sc, lo, hi) == EIG_DONE) { v[c] = lo; v[c + N] = hi; }
-    else list[e] = entry | 1u;
+    if (entry & 7u) continue;
+    const long long c = entry >> 3;
+    if (eig_stage<FIX_MODE, false>(in + c, out + c, axis, sc, lo, hi, &code) == EIG_DONE) { v[c] = lo; v[c + N] = hi; }
+    else list[e] = entry | code;
   }
 }
 
@@ -132,10 +140,13 @@ __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A_corr(const double* __r
   }
   for (unsigned int e = blockIdx.x * BS_A + threadIdx.x; e < count; e += gridDim.x * BS_A) {
     const unsigned int entry = list[e];
-    if (!(entry & 1u)) continue;
-    const long long c = entry >> 1;
+    const int code = int(entry & 7u);
+    if (!code) continue;
+    const long long c = entry >> 3;
     double lo, hi;
-    eig_stage<FIX_MODE, true>(in + c, out + c, axis, sc, lo, hi);
+    if (code == 4) eig_stage<FIX_MODE, true>(in + c, out + c, axis, sc, lo, hi);
+    else if (axis == 3) eigenvalues6z_corrected<FIX_MODE>(in + c, code, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
+    else eigenvalues6_corrected<FIX_MODE>(in + c, axis, code, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
     v[c] = lo; v[c + N] = hi;
   }
 }
@@ -187,6 +198,7 @@ void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, do
   if (c1 < 0) c1 = N;
   const int g = grid_of(c1 - c0, BS_A);
   const int gfix = g;  // one thread per possible list entry: blocks past the count exit at once
+  const int gcorr = g < CORR_BLOCKS ? g : CORR_BLOCKS;
   k_A1_closure<<<g, BS_A, 0, s>>>(M, Fx, vp, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
   double* const ins[3] = {Fx, Fy, Fz};
@@ -194,7 +206,7 @@ void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, do
   for (int axis = 1; axis <= 3; ++axis) {
     k_A_eig<<<g, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
     k_A_fix<<<gfix, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
-    k_A_corr<<<gfix, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
+    k_A_corr<<<gcorr, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
     if (ev) cudaEventRecord(ev[axis], s);
   }
   k_A5_flux<<<g, BS_A, 0, s>>>(Mtmp, M, Fx, Fy, Fz, vp, blockmax, sc, clk, c0, c1);

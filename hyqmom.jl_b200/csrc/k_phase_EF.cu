@@ -124,15 +124,16 @@ void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, doubl
   if (c1 < 0) c1 = sc.N;
   const int g = grid_of(c1 - c0, BS_EF);
   const int gfix = g;  // one thread per possible list entry: blocks past the count exit at once
+  const int gcorr = g < CORR_BLOCKS ? g : CORR_BLOCKS;
   k_E1_closure<<<g, BS_EF, 0, s>>>(Min, Fx, vp, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
   k_E_eig<<<g, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk, c0, c1);
   k_E_fix<<<gfix, BS_EF, 0, s>>>(Fx, vp, 1, 0, sc, clk, c0, c1);
-  k_E_corr<<<gfix, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk, c0, c1);
+  k_E_corr<<<gcorr, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[1], s);
   k_E_eig<<<g, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk, c0, c1);
   k_E_fix<<<gfix, BS_EF, 0, s>>>(Fy, vp, 2, 1, sc, clk, c0, c1);
-  k_E_corr<<<gfix, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk, c0, c1);
+  k_E_corr<<<gcorr, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[2], s);
   k_E4_closure_bgk<<<g, BS_EF, 0, s>>>(Fz, Mout, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[3], s);

@@ -19,14 +19,20 @@ void sh_eig(const double* m, int axis, int flag2D, double Ma, int pos, double* v
 }
 // the parts the step kernels run before the correction pass: gen = 0 the
 // pattern-1-only variant, 1 the general code; 0 done, 1 deferred, 2
-// correction needed (outputs then incomplete)
-int sh_eig_part(const double* m, int axis, int flag2D, double Ma, int pos, int gen, double* v, double* Mr) {
+// correction needed (outputs then incomplete; *planes: the planes to
+// correct, 0 = only the complete function)
+int sh_eig_part(const double* m, int axis, int flag2D, double Ma, int pos, int gen, double* v, double* Mr, int* planes) {
   if (gen) {
-    if (axis == 3) return eigenvalues6z_s<JAC_GEN, false>(m, flag2D, Ma, pos, v[0], v[1], Mr, 1, 1);
-    return eigenvalues6_s<JAC_GEN, false>(m, axis, flag2D, Ma, v[0], v[1], Mr, 1, 1);
+    if (axis == 3) return eigenvalues6z_s<JAC_GEN, false>(m, flag2D, Ma, pos, v[0], v[1], Mr, 1, 1, planes);
+    return eigenvalues6_s<JAC_GEN, false>(m, axis, flag2D, Ma, v[0], v[1], Mr, 1, 1, planes);
   }
-  if (axis == 3) return eigenvalues6z_s<JAC_P1, false>(m, flag2D, Ma, pos, v[0], v[1], Mr, 1, 1);
-  return eigenvalues6_s<JAC_P1, false>(m, axis, flag2D, Ma, v[0], v[1], Mr, 1, 1);
+  if (axis == 3) return eigenvalues6z_s<JAC_P1, false>(m, flag2D, Ma, pos, v[0], v[1], Mr, 1, 1, planes);
+  return eigenvalues6_s<JAC_P1, false>(m, axis, flag2D, Ma, v[0], v[1], Mr, 1, 1, planes);
+}
+// the correction pass from the reported planes
+void sh_eig_corrected(const double* m, int axis, int planes, int flag2D, double Ma, double* v, double* Mr) {
+  if (axis == 3) eigenvalues6z_corrected<JAC_GEN>(m, planes, flag2D, Ma, v[0], v[1], Mr, 1, 1);
+  else eigenvalues6_corrected<JAC_GEN>(m, axis, planes, flag2D, Ma, v[0], v[1], Mr, 1, 1);
 }
 int sh_eig_flags(const double* m, int axis, int mode) {
   if (mode == 1) return eigenvalues6_flags_t<JAC_P1>(m, axis, 1);

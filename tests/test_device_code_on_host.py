@@ -115,7 +115,7 @@ def test_fast_eigen_path_is_bitwise_general(shim, states):
 def test_kernel_parts_defer_or_agree(shim, states):
     """The step kernels run the eigenvalue functions in parts: the pattern-1
     register path first, the general code on the cells it left, and the
-    correction last.  On every cell (the evolved states and copies whose first
+    correction last, from the planes the earlier part reported.  On every cell (the evolved states and copies whose first
     Jacobian column carries round-off-sized entries) each part either leaves
     the cell to a later one or gives the complete function's results bit for
     bit; the flag variants likewise."""
@@ -133,10 +133,14 @@ def test_kernel_parts_defer_or_agree(shim, states):
             v, Mr = np.zeros(2), np.zeros(35)
             shim.sh_eig(P(m), ax, 0, ctypes.c_double(0.0), 1, P(v), P(Mr))
             for gen in (0, 1):
-                v2, Mr2 = np.zeros(2), np.zeros(35)
-                st = shim.sh_eig_part(P(m), ax, 0, ctypes.c_double(0.0), 1, gen, P(v2), P(Mr2))
+                v2, Mr2, planes = np.zeros(2), np.zeros(35), ctypes.c_int(-1)
+                st = shim.sh_eig_part(P(m), ax, 0, ctypes.c_double(0.0), 1, gen, P(v2), P(Mr2), ctypes.byref(planes))
                 seen[(gen, st)] += 1
                 assert st in (0, 1, 2) and not (gen and st == 1)
+                if st == 2 and planes.value:
+                    v2, Mr2 = np.zeros(2), np.zeros(35)
+                    shim.sh_eig_corrected(P(m), ax, planes.value, 0, ctypes.c_double(0.0), P(v2), P(Mr2))
+                    st = 0
                 if st == 0:
                     assert np.array_equal(v, v2, equal_nan=True) and np.array_equal(Mr, Mr2, equal_nan=True), (ax, gen)
             if ax < 3:
