@@ -44,15 +44,21 @@ B_ALG = 2 * 35 * 8  # bytes per cell-step: state read once, written once
 # sweeps of 18 ops per moment plus the 4-op combination).
 E2E_SLABS = 4
 LAUNCHES_PER_STEP = 21  # the eleven timed kernels and the two passes over listed cells of A2-A4, E2, E3
+# the launches of an eigenvalue stage (one hyq_advance_timed slot)
+STAGE_KERNELS = {k: f"k_{p}_eig+k_{p}_fix+k_{p}_corr ({k[-1]})" for k, p in
+                 (("A2_eig_x", "A"), ("A3_eig_y", "A"), ("A4_eig_z", "A"), ("E2_eig_x", "E"), ("E3_eig_y", "E"))}
 KERNELS = ["A1_closure", "A2_eig_x", "A3_eig_y", "A4_eig_z", "A5_flux_speeds", "cfl", "hll",
            "E1_closure", "E2_eig_x", "E3_eig_y", "E4_closure_bgk"]
-# DRAM bytes (read + write) per cell of each kernel from one ncu capture of
-# the 96x96x48 case of the same workload (profiles/step_kernels_crossing96x96x48.md),
-# scaled to a launch by its cells: the local-memory traffic per cell does not
-# depend on the grid size.
-TRAFFIC_PER_CELL = {"A1_closure": 3221.0, "A2_eig_x": 1720.0, "A3_eig_y": 1725.0, "A4_eig_z": 2326.0, "A5_flux_speeds": 4487.0,
-                    "hll": 1609.0, "E1_closure": 3211.0, "E2_eig_x": 1443.0, "E3_eig_y": 1424.0, "E4_closure_bgk": 3951.0}
-TRAFFIC_SOURCE = "ncu dram__bytes_read+write per cell on 96x96x48, first step, scaled to this launch's cells"
+# DRAM bytes (read + write) per cell from ncu captures on the 96x96x48 case of
+# the same workload (profiles/step_kernels_crossing96x96x48.md), scaled to a
+# launch by its cells (the local-memory traffic per cell does not depend on
+# the grid size): the eigenvalue stages A2-A4 from step 151 (dense mode, the
+# late part of the run that dominates it), the closure and HLL kernels from
+# the first step.
+TRAFFIC_PER_CELL = {"A1_closure": 3221.0, "A2_eig_x": 3531.0, "A3_eig_y": 3546.0, "A4_eig_z": 4028.0, "A5_flux_speeds": 4487.0,
+                    "hll": 1609.0, "E1_closure": 3211.0, "E4_closure_bgk": 3951.0}
+TRAFFIC_SOURCE = ("ncu dram__bytes_read+write per cell on 96x96x48 (eigenvalue stages: all three kernels at step 151; "
+                  "closures: first step), scaled to this launch's cells")
 F_KERNEL = {"A1_closure": 11800.8, "A2_eig_x": 8014.9, "A3_eig_y": 8022.6, "A4_eig_z": 8494.7, "A5_flux_speeds": 13804.2,
             "cfl": 1.0, "hll": 2030.0, "E1_closure": 11811.2, "E2_eig_x": 8050.8, "E3_eig_y": 8050.3, "E4_closure_bgk": 12602.6}
 
@@ -305,7 +311,7 @@ def run_gpu(args, rank, world, local_rank):
     roof = {"bound": "fp64", "achieved": ach, "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64, "traffic": traffic,
             "traffic_source": TRAFFIC_SOURCE,
             "peak_source": "measured in this run: FP64 DGEMM 8192^3 (cuBLAS via torch), best of 3",
-            "dominant_kernel": "k_" + dom, "f_alg_per_cell": F_KERNEL[dom],
+            "dominant_kernel": STAGE_KERNELS.get(dom, "k_" + dom), "f_alg_per_cell": F_KERNEL[dom],
             "note": "built with -fmad=false: every counted op is one FP64 pipe instruction, so an FMA-free kernel tops out at peak/2",
             "step": {"f_alg_per_cell": F_ALG, "achieved": step_tflops, "frac": step_tflops / fp64,
                      "hbm_achieved_gbs": B_ALG * cells / (ms / args.steps * 1e-3) / 1e9},
