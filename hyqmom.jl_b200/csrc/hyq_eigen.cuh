@@ -280,7 +280,8 @@ HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
       double rt1r, rt1i, rt2r, rt2i;
       if (s == 0.0) { rt1r = rt1i = rt2r = rt2i = 0.0; }
       else {
-        h11 = h11 / s; h21 = h21 / s; h12 = h12 / s; h22 = h22 / s;
+        const double rs = 1.0 / s;  // four quotients through one reciprocal (div_by: bit-identical)
+        h11 = div_by(h11, s, rs); h21 = div_by(h21, s, rs); h12 = div_by(h12, s, rs); h22 = div_by(h22, s, rs);
         const double tr = (h11 + h22) / 2.0;
         const double det = (h11 - tr) * (h22 - tr) - h12 * h21;
         const double rtdisc = sqrt(fabs(det));
@@ -297,12 +298,14 @@ HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
       HQ_ROLLED for (m = i - 2; m >= lq; --m) {
         double h21s = H[m + 1][m];
         double s2 = fabs(H[m][m] - rt2r) + fabs(rt2i) + fabs(h21s);
-        h21s = H[m + 1][m] / s2;
-        v[0] = h21s * H[m][m + 1] + (H[m][m] - rt1r) * ((H[m][m] - rt2r) / s2) - rt1i * (rt2i / s2);
+        const double rs2 = 1.0 / s2;
+        h21s = div_by(H[m + 1][m], s2, rs2);
+        v[0] = h21s * H[m][m + 1] + (H[m][m] - rt1r) * div_by(H[m][m] - rt2r, s2, rs2) - rt1i * div_by(rt2i, s2, rs2);
         v[1] = h21s * (H[m][m] + H[m + 1][m + 1] - rt1r - rt2r);
         v[2] = h21s * H[m + 2][m + 1];
         s2 = fabs(v[0]) + fabs(v[1]) + fabs(v[2]);
-        v[0] = v[0] / s2; v[1] = v[1] / s2; v[2] = v[2] / s2;
+        const double rv = 1.0 / s2;
+        v[0] = div_by(v[0], s2, rv); v[1] = div_by(v[1], s2, rv); v[2] = div_by(v[2], s2, rv);
         if (m == lq) break;
         const double h00 = fabs(H[m][m - 1]) * (fabs(v[1]) + fabs(v[2]));
         const double h11b = fabs(v[0]) * (fabs(H[m - 1][m - 1]) + fabs(H[m][m]) + fabs(H[m + 1][m + 1]));
@@ -511,9 +514,14 @@ enum EigStatus { EIG_DONE = 0, EIG_DEFERRED = 1, EIG_NEEDS_FIX = 2 };
 // Jacobians have complex eigenvalues returns EIG_NEEDS_FIX before the
 // correction, whose code (a closure with its realizability) is then not part
 // of the caller.  vmin, vmax and Mr are complete only with EIG_DONE.
+//
+// park (optional): on EIG_DONE, the second Jacobian's (vmin, vmax) go to
+// park[0], park[pst] when the moments were not corrected, NaN otherwise.
+// Along y that Jacobian is the VW plane, which eigenvalues6z_s solves again
+// from the same moments when it neither floors nor re-realizes them.
 template <int MODE, bool CORR>
 HQN int eigenvalues6_s(const double* M, int axis, int flag2D, double Ma, double& vmin, double& vmax, double* Mr, long long ist,
-                       long long ost, int* planes = nullptr) {
+                       long long ost, int* planes = nullptr, double* park = nullptr, long long pst = 0) {
   const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
   double a[15], b[15];
   for (int n = 0; n < 15; ++n) { a[n] = M[SLICE[sa][n] * ist]; b[n] = M[SLICE[sb][n] * ist]; }
@@ -534,6 +542,11 @@ HQN int eigenvalues6_s(const double* M, int axis, int flag2D, double Ma, double&
   combine();
 #pragma unroll
   for (int n = 0; n < 35; ++n) Mr[n * ost] = M[n * ist];
+  if (park) {
+    const bool fixed = ca || cb;
+    park[0] = fixed ? qnan() : eb.vmin;
+    park[pst] = fixed ? qnan() : eb.vmax;
+  }
   if constexpr (CORR) {
     if (ca || cb) {
       double Ml[35], Mc[35];
@@ -561,7 +574,8 @@ HQD void eigenvalues6(const double* M, int axis, int flag2D, double Ma, double& 
 // speeds, the same results as the complete function.
 template <int MODE>
 HQN void eigenvalues6_corrected(const double* M, int axis, int planes, int flag2D, double Ma, double& vmin, double& vmax, double* Mr,
-                                long long ist, long long ost) {
+                                long long ist, long long ost, double* park = nullptr, long long pst = 0) {
+  if (park) { park[0] = qnan(); park[pst] = qnan(); }
   const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
   double Ml[35], Mc[35], a[15], b[15];
   for (int n = 0; n < 35; ++n) Ml[n] = M[n * ist];
@@ -592,19 +606,24 @@ template <int MODE> HQN int eigenvalues6_flags_t(const double* M, int axis, long
 
 // eigenvalues6z_hyperbolic_3D (strides, MODE, CORR and the outcome as
 // eigenvalues6_s; without CORR the negative-variance re-realization also
-// returns EIG_NEEDS_FIX)
+// returns EIG_NEEDS_FIX).  parked (optional): the VW-plane speeds that the y
+// stage parked for these moments (eigenvalues6_s park); used instead of
+// solving that Jacobian again when the moments go in unchanged and the pair
+// is not NaN, NaN (the same numbers either way).
 template <int MODE, bool CORR>
 HQN int eigenvalues6z_s(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr, long long ist,
-                        long long ost, int* planes = nullptr) {
+                        long long ost, int* planes = nullptr, const double* parked = nullptr, long long pst = 0) {
   double Mw[35];
 #pragma unroll
   for (int n = 0; n < 35; ++n) Mw[n] = M[n * ist];
-  if (positivity && Mw[0] <= 0.0) Mw[0] = jmax(Mw[0], 1e-14);
+  bool same = true;  // Mw equals the input moments
+  if (positivity && Mw[0] <= 0.0) { Mw[0] = jmax(Mw[0], 1e-14); same = false; }
   if (positivity && Mw[0] > 1e-15) {
     const double m000 = Mw[0];
     const double vx = M[2 * ist] / m000 - sq(M[1 * ist] / m000), vy = M[9 * ist] / m000 - sq(M[5 * ist] / m000),
                  vz = M[19 * ist] / m000 - sq(M[15 * ist] / m000);
     if (vx < 0.0 || vy < 0.0 || vz < 0.0) {
+      same = false;
       if constexpr (CORR) flux_closure35(M, flag2D, Ma, nullptr, nullptr, nullptr, Mw, ist, 1);
       else {
         if (planes) *planes = 0;  // the re-realization: only the complete function
@@ -616,8 +635,15 @@ HQN int eigenvalues6z_s(const double* M, int flag2D, double Ma, int positivity, 
   for (int n = 0; n < 15; ++n) { a[n] = Mw[WUI[n]]; b[n] = Mw[SLICE[3][n]]; }
   EigOut ea = jac_eigs_t<MODE>(a);
   if (ea.deferred) return EIG_DEFERRED;
-  EigOut eb = jac_eigs_t<MODE>(b);
-  if (eb.deferred) return EIG_DEFERRED;
+  EigOut eb;
+  if (parked && same && !(parked[0] != parked[0] && parked[pst] != parked[pst])) {
+    // the y stage did not correct these moments, so its VW Jacobian had no
+    // eigenvalue with |imag| above the threshold
+    eb.vmin = parked[0]; eb.vmax = parked[pst]; eb.imax = 0.0; eb.deferred = false;
+  } else {
+    eb = jac_eigs_t<MODE>(b);
+    if (eb.deferred) return EIG_DEFERRED;
+  }
   const double thr = 1000.0 * EPS;
   const bool ca = ea.imax > thr, cb = eb.imax > thr;
   if (!CORR && (ca || cb)) {

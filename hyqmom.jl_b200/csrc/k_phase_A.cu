@@ -65,15 +65,20 @@ __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure(const double*
 }
 
 // eigenvalues6_hyperbolic_3D along x (axis 1) or y (axis 2), and
-// eigenvalues6z_hyperbolic_3D (axis 3), as a part (MODE, CORR); a cell left
-// for the correction gets its list code in *code
+// eigenvalues6z_hyperbolic_3D (axis 3), as a part (MODE, CORR) for cell c; a
+// cell left for the correction gets its list code in *code.  The y stage
+// parks its VW-plane speeds in the z stage's speed slots (vp[4N + c],
+// vp[5N + c], which the z stage reads and then overwrites); every part of the
+// y stage that finishes a cell parks, so no stale pair survives.
 template <int MODE, bool CORR>
-__device__ __forceinline__ int eig_stage(const double* in, double* out, int axis, const StepConst& sc, double& lo, double& hi,
-                                         unsigned int* code = nullptr) {
+__device__ __forceinline__ int eig_stage(const double* in, double* out, double* vp, long long c, int axis, const StepConst& sc,
+                                         double& lo, double& hi, unsigned int* code = nullptr) {
   const long long N = sc.N;
   int planes = 0;
-  const int st = axis == 3 ? eigenvalues6z_s<MODE, CORR>(in, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out, N, N, &planes)
-                           : eigenvalues6_s<MODE, CORR>(in, axis, sc.flag2D, sc.Ma, lo, hi, out, N, N, &planes);
+  double* park = vp + 4 * N + c;
+  const int st = axis == 3 ? eigenvalues6z_s<MODE, CORR>(in + c, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out + c, N, N, &planes, park, N)
+                           : eigenvalues6_s<MODE, CORR>(in + c, axis, sc.flag2D, sc.Ma, lo, hi, out + c, N, N, &planes,
+                                                        axis == 2 ? park : nullptr, N);
   if (code) *code = st == EIG_NEEDS_FIX ? (planes ? (unsigned int)planes : 4u) : 0u;
   return st;
 }
@@ -87,7 +92,7 @@ __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* __restri
   if (c >= c1) return;
   double lo, hi;
   unsigned int code;
-  if (eig_stage<EIG_MODE, false>(in + c, out + c, axis, sc, lo, hi, &code) == EIG_DONE) {
+  if (eig_stage<EIG_MODE, false>(in, out, vp, c, axis, sc, lo, hi, &code) == EIG_DONE) {
     double* v = vp + 2 * (axis - 1) * N;
     v[c] = lo; v[c + N] = hi;
   } else {
@@ -110,7 +115,7 @@ __global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* __restri
   if (clk->dense[axis - 1]) {
     const long long c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
     if (c >= c1) return;
-    if (eig_stage<FIX_MODE, false>(in + c, out + c, axis, sc, lo, hi, &code) == EIG_DONE) { v[c] = lo; v[c + N] = hi; }
+    if (eig_stage<FIX_MODE, false>(in, out, vp, c, axis, sc, lo, hi, &code) == EIG_DONE) { v[c] = lo; v[c + N] = hi; }
     else list[atomicAdd(list + N + (axis - 1), 1u)] = ((unsigned int)c << 3) | code;
     return;
   }
@@ -119,7 +124,7 @@ __global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* __restri
     const unsigned int entry = list[e];
     if (entry & 7u) continue;
     const long long c = entry >> 3;
-    if (eig_stage<FIX_MODE, false>(in + c, out + c, axis, sc, lo, hi, &code) == EIG_DONE) { v[c] = lo; v[c + N] = hi; }
+    if (eig_stage<FIX_MODE, false>(in, out, vp, c, axis, sc, lo, hi, &code) == EIG_DONE) { v[c] = lo; v[c + N] = hi; }
     else list[e] = entry | code;
   }
 }
@@ -144,9 +149,10 @@ __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A_corr(const double* __r
     if (!code) continue;
     const long long c = entry >> 3;
     double lo, hi;
-    if (code == 4) eig_stage<FIX_MODE, true>(in + c, out + c, axis, sc, lo, hi);
+    if (code == 4) eig_stage<FIX_MODE, true>(in, out, vp, c, axis, sc, lo, hi);
     else if (axis == 3) eigenvalues6z_corrected<FIX_MODE>(in + c, code, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
-    else eigenvalues6_corrected<FIX_MODE>(in + c, axis, code, sc.flag2D, sc.Ma, lo, hi, out + c, N, N);
+    else eigenvalues6_corrected<FIX_MODE>(in + c, axis, code, sc.flag2D, sc.Ma, lo, hi, out + c, N, N,
+                                          axis == 2 ? vp + 4 * N + c : nullptr, N);
     v[c] = lo; v[c + N] = hi;
   }
 }

@@ -29,6 +29,17 @@ int sh_eig_part(const double* m, int axis, int flag2D, double Ma, int pos, int g
   if (axis == 3) return eigenvalues6z_s<JAC_P1, false>(m, flag2D, Ma, pos, v[0], v[1], Mr, 1, 1, planes);
   return eigenvalues6_s<JAC_P1, false>(m, axis, flag2D, Ma, v[0], v[1], Mr, 1, 1, planes);
 }
+// the y stage parking its VW-plane speeds and the z stage reusing them, on
+// the y stage's output, against the z stage solving everything (out[0..1]
+// and out[2..1+35]: with reuse; out[37..38], out[39..73]: without); returns
+// 1 when the parked pair was usable (not NaN, NaN)
+int sh_yz_park(const double* m, int pos, double* out) {
+  double My[35], park[2], lo, hi;
+  eigenvalues6_s<JAC_ANY, true>(m, 2, 0, 0.0, lo, hi, My, 1, 1, nullptr, park, 1);
+  eigenvalues6z_s<JAC_ANY, true>(My, 0, 0.0, pos, out[0], out[1], out + 2, 1, 1, nullptr, park, 1);
+  eigenvalues6z_s<JAC_ANY, true>(My, 0, 0.0, pos, out[37], out[38], out + 39, 1, 1);
+  return (park[0] != park[0] && park[1] != park[1]) ? 0 : 1;
+}
 // the correction pass from the reported planes
 void sh_eig_corrected(const double* m, int axis, int planes, int flag2D, double Ma, double* v, double* Mr) {
   if (axis == 3) eigenvalues6z_corrected<JAC_GEN>(m, planes, flag2D, Ma, v[0], v[1], Mr, 1, 1);

@@ -151,6 +151,20 @@ def test_kernel_parts_defer_or_agree(shim, states):
     assert seen[(0, 0)] > 100 and seen[(0, 1)] > 100 and seen[(1, 0)] > 100 and seen[(1, 2)] > 0, seen
 
 
+def test_z_stage_reuses_the_y_stage_vw_speeds(shim, states):
+    """The y stage parks the speeds of its VW-plane Jacobian; the z stage,
+    given the y stage's output, uses them instead of solving that Jacobian
+    again and gets the same bits as solving it (or ignores a NaN pair)."""
+    shim.sh_yz_park.restype = ctypes.c_int
+    used = 0
+    for m in states:
+        m = np.ascontiguousarray(m)
+        out = np.zeros(74)
+        used += shim.sh_yz_park(P(m), 1, P(out))
+        assert np.array_equal(out[:37], out[37:], equal_nan=True)
+    assert used > len(states) // 2, used
+
+
 def test_reciprocal_division_is_ieee_division(shim):
     """div_by (the HLL star state's division through a shared reciprocal,
     with Markstein's correction) equals the IEEE quotient bit for bit."""
