@@ -280,8 +280,7 @@ HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
       double rt1r, rt1i, rt2r, rt2i;
       if (s == 0.0) { rt1r = rt1i = rt2r = rt2i = 0.0; }
       else {
-        const double rs = 1.0 / s;  // four quotients through one reciprocal (div_by: bit-identical)
-        h11 = div_by(h11, s, rs); h21 = div_by(h21, s, rs); h12 = div_by(h12, s, rs); h22 = div_by(h22, s, rs);
+        h11 = h11 / s; h21 = h21 / s; h12 = h12 / s; h22 = h22 / s;
         const double tr = (h11 + h22) / 2.0;
         const double det = (h11 - tr) * (h22 - tr) - h12 * h21;
         const double rtdisc = sqrt(fabs(det));
@@ -298,14 +297,12 @@ HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
       HQ_ROLLED for (m = i - 2; m >= lq; --m) {
         double h21s = H[m + 1][m];
         double s2 = fabs(H[m][m] - rt2r) + fabs(rt2i) + fabs(h21s);
-        const double rs2 = 1.0 / s2;
-        h21s = div_by(H[m + 1][m], s2, rs2);
-        v[0] = h21s * H[m][m + 1] + (H[m][m] - rt1r) * div_by(H[m][m] - rt2r, s2, rs2) - rt1i * div_by(rt2i, s2, rs2);
+        h21s = H[m + 1][m] / s2;
+        v[0] = h21s * H[m][m + 1] + (H[m][m] - rt1r) * ((H[m][m] - rt2r) / s2) - rt1i * (rt2i / s2);
         v[1] = h21s * (H[m][m] + H[m + 1][m + 1] - rt1r - rt2r);
         v[2] = h21s * H[m + 2][m + 1];
         s2 = fabs(v[0]) + fabs(v[1]) + fabs(v[2]);
-        const double rv = 1.0 / s2;
-        v[0] = div_by(v[0], s2, rv); v[1] = div_by(v[1], s2, rv); v[2] = div_by(v[2], s2, rv);
+        v[0] = v[0] / s2; v[1] = v[1] / s2; v[2] = v[2] / s2;
         if (m == lq) break;
         const double h00 = fabs(H[m][m - 1]) * (fabs(v[1]) + fabs(v[2]));
         const double h11b = fabs(v[0]) * (fabs(H[m - 1][m - 1]) + fabs(H[m][m]) + fabs(H[m + 1][m + 1]));
