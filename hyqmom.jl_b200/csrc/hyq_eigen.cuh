@@ -506,7 +506,8 @@ enum EigStatus { EIG_DONE = 0, EIG_DEFERRED = 1, EIG_NEEDS_FIX = 2 };
 // eigenvalues6_hyperbolic_3D for axis 1 (x) or 2 (y).
 // Moment n is read from M[n * ist] and written to Mr[n * ost] (the step
 // kernels pass the cell's entry of the moment-major fields, stride N); M and
-// Mr must not overlap.  MODE as jac_eigs_t.  With CORR the whole function
+// Mr either do not overlap or are the same array with the same strides (in
+// place: only corrected moments are written).  MODE as jac_eigs_t.  With CORR the whole function
 // runs (EIG_DONE, or EIG_DEFERRED under JAC_P1); without it, a cell whose
 // Jacobians have complex eigenvalues returns EIG_NEEDS_FIX before the
 // correction, whose code (a closure with its realizability) is then not part
@@ -537,8 +538,10 @@ HQN int eigenvalues6_s(const double* M, int axis, int flag2D, double Ma, double&
     if (eb.vmin == eb.vmin || eb.vmax == eb.vmax) { vmin = jmin(vmin, eb.vmin); vmax = jmax(vmax, eb.vmax); }
   };
   combine();
+  if (Mr != M) {  // in place (Mr == M, same strides) the moments are already there
 #pragma unroll
-  for (int n = 0; n < 35; ++n) Mr[n * ost] = M[n * ist];
+    for (int n = 0; n < 35; ++n) Mr[n * ost] = M[n * ist];
+  }
   if (park) {
     const bool fixed = ca || cb;
     park[0] = fixed ? qnan() : eb.vmin;

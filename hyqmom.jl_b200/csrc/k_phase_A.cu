@@ -34,8 +34,9 @@ __device__ __noinline__ void cell_phase_A(const double* m, int flag2D, double Ma
 // Phase [A] runs as five kernels, one per-cell function each, so that every
 // kernel's code stays small (the fused cell_phase_A kernel was bound by
 // instruction fetch); the intermediate states go through buffers that are
-// dead during phase A:  M -A1-> Fx -A2-> Fy -A3-> Fz -A4-> Mtmp -A5-> M, with
-// the Jacobian speeds of A2-A4 parked in vp and combined in A5.
+// dead during phase A:  M -A1-> Fx -A2, A3 (in place)-> Fx -A4-> Mtmp -A5-> M,
+// with the Jacobian speeds of A2-A4 parked in vp and combined in A5 (A2 and A3
+// write only the moments they correct).
 // Each eigenvalue stage A2-A4 runs in three parts, each with small code: the
 // kernel itself solves pattern-1 Jacobians on its 64-register path and lists
 // every other cell; k_A_fix runs the general eigen-solve on the listed cells
@@ -85,7 +86,7 @@ __device__ __forceinline__ int eig_stage(const double* in, double* out, double* 
 
 // A2/A3/A4: the pattern-1 part; cells left go to the list, marked when they
 // need the correction
-__global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* __restrict__ in, double* __restrict__ out, double* vp,
+__global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* in, double* out, double* vp,
                                                          int axis, const StepConst sc, const DevClock* clk, long long c0, long long c1) {
   if (!phase_A_active(sc, clk) || clk->dense[axis - 1]) return;
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
@@ -104,7 +105,7 @@ __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* __restri
 // The general eigen-solve on the unmarked listed cells (dense: on every cell
 // of the range); marks (lists) the ones that need the correction.  One thread
 // per possible entry.
-__global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* __restrict__ in, double* __restrict__ out, double* vp, int axis,
+__global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* in, double* out, double* vp, int axis,
                                                          const StepConst sc, const DevClock* clk, long long c0, long long c1) {
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N;
@@ -131,7 +132,7 @@ __global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* __restri
 
 // The complete function on the marked listed cells; the first thread then
 // decides whether the stage runs dense next time
-__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A_corr(const double* __restrict__ in, double* __restrict__ out, double* vp,
+__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A_corr(const double* in, double* out, double* vp,
                                                               int axis, const StepConst sc, DevClock* clk, long long c0, long long c1) {
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N;
@@ -207,8 +208,8 @@ void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, do
   const int gcorr = g < CORR_BLOCKS ? g : CORR_BLOCKS;
   k_A1_closure<<<g, BS_A, 0, s>>>(M, Fx, vp, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
-  double* const ins[3] = {Fx, Fy, Fz};
-  double* const outs[3] = {Fy, Fz, Mtmp};
+  double* const ins[3] = {Fx, Fx, Fx};
+  double* const outs[3] = {Fx, Fx, Mtmp};  // x and y in place
   for (int axis = 1; axis <= 3; ++axis) {
     k_A_eig<<<g, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
     k_A_fix<<<gfix, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);

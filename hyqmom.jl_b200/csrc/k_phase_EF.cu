@@ -10,8 +10,8 @@ namespace {
 
 
 // Phases [E]+[F] run as per-function kernels (small code per kernel);
-// intermediate states go through the flux buffers, dead after the HLL sweep:
-//   Mtmp -E1-> Fx -E2-> Fy -E3-> Fz -E4-> M.
+// intermediate states go through a flux buffer, dead after the HLL sweep:
+//   Mtmp -E1-> Fx -E2, E3 (in place: only corrected moments are written)-> Fx -E4-> M.
 // E2/E3 copy the moments and list the cells whose Jacobians have complex
 // eigenvalues and the cells with a Jacobian outside the usual permutation
 // (pattern 1, the only one their 64-register code solves); k_E_fix decides
@@ -37,15 +37,17 @@ __global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E1_closure(const double
 
 // E2/E3: eigenvalues6_hyperbolic_3D along x or y: copy, and list the cells
 // that need the correction or the complete eigen-solve (counter `which`)
-__global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* __restrict__ in, double* __restrict__ out, double* vp, int axis,
+__global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* in, double* out, double* vp, int axis,
                                                            int which, const StepConst sc, const DevClock* clk, long long c0, long long c1) {
   if (!clk->active) return;
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
   if (c >= c1) return;
   const bool dense = clk->dense[3 + which] != 0;
   const int planes = dense ? 0 : eigenvalues6_flags_t<EIG_MODE>(in + c, axis, N);
+  if (out != in) {
 #pragma unroll
-  for (int n = 0; n < 35; ++n) out[c + N * n] = in[c + N * n];
+    for (int n = 0; n < 35; ++n) out[c + N * n] = in[c + N * n];
+  }
   if (planes) {
     const unsigned int slot = atomicAdd(fix_counters(vp, N) + which, 1u);
     reinterpret_cast<unsigned long long*>(vp)[slot] = ((unsigned long long)c << 2) | (unsigned long long)(planes < 0 ? 0 : planes);
@@ -80,7 +82,7 @@ __global__ void __launch_bounds__(BS_EF, MINB_FIX) k_E_fix(const double* __restr
 // The correction of the listed cells that need it
 // (correct_moments_for_real_eigenvalues, as in eigenvalues6); the first thread
 // then decides whether the stage runs dense next time
-__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E_corr(const double* __restrict__ in, double* __restrict__ out, const double* vp,
+__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E_corr(const double* in, double* out, const double* vp,
                                                                 int axis, int which, const StepConst sc, DevClock* clk, long long c0,
                                                                 long long c1) {
   if (!clk->active) return;
@@ -127,15 +129,15 @@ void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, doubl
   const int gcorr = g < CORR_BLOCKS ? g : CORR_BLOCKS;
   k_E1_closure<<<g, BS_EF, 0, s>>>(Min, Fx, vp, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
-  k_E_eig<<<g, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk, c0, c1);
+  k_E_eig<<<g, BS_EF, 0, s>>>(Fx, Fx, vp, 1, 0, sc, clk, c0, c1);
   k_E_fix<<<gfix, BS_EF, 0, s>>>(Fx, vp, 1, 0, sc, clk, c0, c1);
-  k_E_corr<<<gcorr, BS_EF, 0, s>>>(Fx, Fy, vp, 1, 0, sc, clk, c0, c1);
+  k_E_corr<<<gcorr, BS_EF, 0, s>>>(Fx, Fx, vp, 1, 0, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[1], s);
-  k_E_eig<<<g, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk, c0, c1);
-  k_E_fix<<<gfix, BS_EF, 0, s>>>(Fy, vp, 2, 1, sc, clk, c0, c1);
-  k_E_corr<<<gcorr, BS_EF, 0, s>>>(Fy, Fz, vp, 2, 1, sc, clk, c0, c1);
+  k_E_eig<<<g, BS_EF, 0, s>>>(Fx, Fx, vp, 2, 1, sc, clk, c0, c1);
+  k_E_fix<<<gfix, BS_EF, 0, s>>>(Fx, vp, 2, 1, sc, clk, c0, c1);
+  k_E_corr<<<gcorr, BS_EF, 0, s>>>(Fx, Fx, vp, 2, 1, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[2], s);
-  k_E4_closure_bgk<<<g, BS_EF, 0, s>>>(Fz, Mout, sc, clk, c0, c1);
+  k_E4_closure_bgk<<<g, BS_EF, 0, s>>>(Fx, Mout, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[3], s);
 }
 
