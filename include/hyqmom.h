@@ -56,6 +56,9 @@ typedef struct hyq_stats {
 typedef struct hyq_ctx hyq_ctx;
 
 int hyq_abi_version(void);
+/* Grids need Nx >= 2, Ny >= 2, Nz >= 1 and fewer than 2^29 cells (the step's
+ * cell lists hold 32-bit entries); anything else gets HYQ_EINVAL before any
+ * CUDA call. */
 int hyq_create(const hyq_params* p, hyq_ctx** out);
 void hyq_destroy(hyq_ctx* ctx);
 const char* hyq_last_error(const hyq_ctx* ctx);
@@ -103,7 +106,7 @@ void* hyq_stream(hyq_ctx* ctx);
  * with CUDA events around each on the context stream; ms[HYQ_TIMED_SLOTS]
  * receives the summed device time of each kernel, in launch order:
  * A1 closure, A2 x eigenvalues, A3 y eigenvalues, A4 z eigenvalues (each
- * with its pass over the cells it left to the complete eigen-solve),
+ * with its passes over the cells it listed: general eigen-solve, correction),
  * A5 closure with fluxes and speeds, CFL reduction, HLL sweep,
  * E1 closure, E2 x eigenvalues, E3 y eigenvalues (each with its pass that
  * decides and corrects the listed cells), E4 closure + BGK.

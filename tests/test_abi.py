@@ -35,3 +35,20 @@ def test_missing_library_fails_loudly(tmp_path):
             _lib.load(str(tmp_path / "nope.so"))
     finally:
         _lib._lib = saved
+
+
+@pytest.mark.skipif(not os.path.exists(_lib.LIB_PATH), reason="library not built")
+def test_create_rejects_grids_beyond_the_list_limit():
+    """hyq_create checks the grid on the host before any CUDA call, so this
+    runs without a GPU: 2^29 cells and more do not fit the 32-bit entries of
+    the step's cell lists."""
+    import ctypes
+    from hyqmom.runner import params_struct
+    from hyqmom import ic
+    lib = _lib.load()
+    p = ic.default_params(Nx=1024, Ny=1024, Nz=512)  # exactly 2^29 cells
+    h = ctypes.c_void_p()
+    assert lib.hyq_create(ctypes.byref(params_struct(p)), ctypes.byref(h)) == -1
+    assert "2^29" in lib.hyq_last_error(None).decode()
+    p = ic.default_params(Nx=1, Ny=4, Nz=4)
+    assert lib.hyq_create(ctypes.byref(params_struct(p)), ctypes.byref(h)) == -1
