@@ -130,8 +130,9 @@ __global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* in, doub
   }
 }
 
-// The complete function on the marked listed cells; the first thread then
-// decides whether the stage runs dense next time
+// The marked listed cells: the correction from the recorded planes (code
+// 1-3), or the complete function (code 4, a z-stage re-realization); the first
+// thread then decides whether the stage runs dense next time
 __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A_corr(const double* in, double* out, double* vp,
                                                               int axis, const StepConst sc, DevClock* clk, long long c0, long long c1) {
   if (!phase_A_active(sc, clk)) return;
