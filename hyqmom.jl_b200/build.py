@@ -8,8 +8,9 @@ import subprocess
 import sys
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-SOURCES = ["hyq_b200.cu", "k_phase_A.cu", "k_phase_EF.cu", "k_cells.cu", "hyq_noalloc.cu"]
-HEADERS = ["hyq_cell.cuh", "hyq_closure.cuh", "hyq_eigen.cuh", "hyq_eig6.cuh", "hyq_step.cuh", "gen_jacobian6.inc"]
+SOURCES = ["hyq_b200.cu", "k_phase_A.cu", "k_phase_EF.cu", "k_cells.cu", "hyq_noalloc.cu", "k_mlp.cu"]
+HEADERS = ["hyq_cell.cuh", "hyq_closure.cuh", "hyq_eigen.cuh", "hyq_eig6.cuh", "hyq_charpoly.cuh", "hyq_umma.cuh", "hyq_step.cuh",
+           "gen_jacobian6.inc"]
 OBJ_DIR = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libhyqmom_b200.so")
 INCLUDE = os.path.join(os.path.dirname(PKG), "include", "hyqmom.h")

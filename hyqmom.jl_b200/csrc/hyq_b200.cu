@@ -174,6 +174,7 @@ __global__ void __launch_bounds__(BS_HLL, HQ_MINB_HLL) k_hll(const double* __res
 __global__ void k_set_clock(DevClock* clk, double t, long long nn) {
   clk->t = t; clk->nn = nn; clk->dt = 0.0; clk->vmax = 0.0; clk->active = 0; clk->status = 0;
   for (int q = 0; q < 5; ++q) clk->dense[q] = 0;
+  clk->fb_cells = 0; clk->stage_cells = 0;
 }
 
 
@@ -193,6 +194,11 @@ struct hyq_ctx {
   // hyq_step_host: copy stream and per-slab events, made on first use
   cudaStream_t cstream = nullptr;
   std::vector<cudaEvent_t> up, down;
+  // learned mode: the network's seeds [6][N], its weight image and error word
+  float* seeds = nullptr;
+  WaveNet net{nullptr, nullptr};
+  float* net_w = nullptr;  // FP32 parameters (device), packed into net.image
+  bool net_loaded = false;
   std::string err;
 };
 
@@ -215,11 +221,34 @@ int cuda_fail(hyq_ctx* ctx, cudaError_t e, const char* what) {
 
 void enqueue_step(hyq_ctx* ctx, cudaStream_t s) {
   const long long N = ctx->N;
-  launch_phase_A(ctx->sc, ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s);
+  launch_phase_A(ctx->sc, ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s, nullptr, 0, -1, &ctx->net);
   k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
   k_hll<<<grid_of(N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
   launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->clk, s);
 }
+// Capture one step as the context's graph (replacing an earlier one).
+int capture_graph(hyq_ctx* ctx) {
+  cudaError_t e;
+  if (ctx->exec) { cudaGraphExecDestroy(ctx->exec); ctx->exec = nullptr; }
+  if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+  if ((e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+    return cuda_fail(ctx, e, "cudaStreamBeginCapture");
+  enqueue_step(ctx, ctx->stream);
+  if ((e = cudaStreamEndCapture(ctx->stream, &ctx->graph)) != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
+  if ((e = cudaGraphInstantiate(&ctx->exec, ctx->graph, 0)) != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
+  return HYQ_OK;
+}
+
+int net_status(hyq_ctx* ctx) {
+  if (ctx->sc.mode != MODE_LEARNED) return HYQ_OK;
+  int h = 0;
+  HQ_CHECK(ctx, cudaMemcpyAsync(&h, ctx->net.err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  HQ_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  if (h) return fail(ctx, HYQ_ETIMEOUT, "the wave-speed network kernel gave up waiting for its tensor-core operations");
+  return HYQ_OK;
+}
+
+__global__ void k_reset_counters(DevClock* clk) { clk->fb_cells = 0; clk->stage_cells = 0; }
 }  // namespace
 
 // Launch helpers for other translation units (same kernels and shapes as
@@ -251,6 +280,8 @@ int hyq_create(const hyq_params* p, hyq_ctx** out) {
     return fail(nullptr, HYQ_EINVAL, "CFL, Kn and dtmax must be positive");
   if ((long long)p->Nx * p->Ny * p->Nz >= (1LL << 29))
     return fail(nullptr, HYQ_EINVAL, "grid must have fewer than 2^29 cells (the step's cell lists hold 32-bit entries)");
+  if (p->mode != HYQ_MODE_PLAIN && p->mode != HYQ_MODE_LEARNED && p->mode != HYQ_MODE_CERTIFIED)
+    return fail(nullptr, HYQ_EINVAL, "mode must be HYQ_MODE_PLAIN, HYQ_MODE_LEARNED or HYQ_MODE_CERTIFIED");
   hyq_ctx* ctx = new hyq_ctx();
   ctx->p = *p;
   ctx->device = p->device;
@@ -263,6 +294,9 @@ int hyq_create(const hyq_params* p, hyq_ctx** out) {
   sc.nnmax = p->nnmax; sc.tmax = p->tmax; sc.Kn = p->Kn; sc.Ma = p->Ma; sc.CFL = p->CFL; sc.dtmax = p->dtmax;
   sc.dx = (p->xmax - p->xmin) / p->Nx; sc.dy = (p->ymax - p->ymin) / p->Ny; sc.dz = (p->zmax - p->zmin) / p->Nz;
   sc.nblocksA = grid_of(N, BS_A);
+  sc.mode = p->mode;
+  sc.seeds = nullptr;
+  sc.seed_margin = 0.0;
   const size_t b35 = sizeof(double) * 35 * (size_t)N;
   auto alloc = [&](double** ptr, size_t bytes) { return cudaMalloc((void**)ptr, bytes); };
   if (alloc(&ctx->M, b35) != cudaSuccess || alloc(&ctx->Mtmp, b35) != cudaSuccess || alloc(&ctx->Fx, b35) != cudaSuccess ||
@@ -274,6 +308,22 @@ int hyq_create(const hyq_params* p, hyq_ctx** out) {
     hyq_destroy(ctx);
     return fail(nullptr, HYQ_ENOMEM, "device allocation failed");
   }
+  if (p->mode == HYQ_MODE_LEARNED) {
+    if (cudaMalloc((void**)&ctx->seeds, sizeof(float) * 6 * (size_t)N) != cudaSuccess ||
+        cudaMalloc((void**)&ctx->net.image, (size_t)hyq_net_image_bytes()) != cudaSuccess ||
+        cudaMalloc((void**)&ctx->net.err, sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void**)&ctx->net_w, sizeof(float) * HYQ_NET_PARAMS) != cudaSuccess) {
+      cudaGetLastError();
+      hyq_destroy(ctx);
+      return fail(nullptr, HYQ_ENOMEM, "device allocation failed");
+    }
+    if ((e = net_set_smem()) != cudaSuccess || (e = cudaMemset(ctx->net.err, 0, sizeof(int))) != cudaSuccess) {
+      int r = cuda_fail(nullptr, e, "network set-up");
+      hyq_destroy(ctx);
+      return r;
+    }
+    sc.seeds = ctx->seeds;
+  }
   if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) {
     int r = cuda_fail(nullptr, e, "cudaStreamCreate");
     hyq_destroy(ctx);
@@ -281,15 +331,10 @@ int hyq_create(const hyq_params* p, hyq_ctx** out) {
   }
   k_set_clock<<<1, 1, 0, ctx->stream>>>(ctx->clk, 0.0, 0);
   // capture one step as a graph
-  if ((e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
-    int r = cuda_fail(nullptr, e, "cudaStreamBeginCapture"); hyq_destroy(ctx); return r;
-  }
-  enqueue_step(ctx, ctx->stream);
-  if ((e = cudaStreamEndCapture(ctx->stream, &ctx->graph)) != cudaSuccess) {
-    int r = cuda_fail(nullptr, e, "cudaStreamEndCapture"); hyq_destroy(ctx); return r;
-  }
-  if ((e = cudaGraphInstantiate(&ctx->exec, ctx->graph, 0)) != cudaSuccess) {
-    int r = cuda_fail(nullptr, e, "cudaGraphInstantiate"); hyq_destroy(ctx); return r;
+  if (capture_graph(ctx) != HYQ_OK) {
+    const std::string msg = ctx->err;
+    hyq_destroy(ctx);
+    return fail(nullptr, HYQ_ECUDA, msg);
   }
   if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) {
     int r = cuda_fail(nullptr, e, "create sync"); hyq_destroy(ctx); return r;
@@ -307,6 +352,10 @@ void hyq_destroy(hyq_ctx* ctx) {
   double* bufs[] = {ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax};
   for (double* b : bufs) if (b) cudaFree(b);
   if (ctx->clk) cudaFree(ctx->clk);
+  if (ctx->seeds) cudaFree(ctx->seeds);
+  if (ctx->net.image) cudaFree(ctx->net.image);
+  if (ctx->net.err) cudaFree(ctx->net.err);
+  if (ctx->net_w) cudaFree(ctx->net_w);
   if (ctx->cstream) cudaStreamSynchronize(ctx->cstream);
   for (cudaEvent_t e : ctx->up) cudaEventDestroy(e);
   for (cudaEvent_t e : ctx->down) cudaEventDestroy(e);
@@ -358,8 +407,36 @@ int hyq_get_state_device(hyq_ctx* ctx, double* dM) {
   return HYQ_OK;
 }
 
+int hyq_reset_counters(hyq_ctx* ctx) {
+  if (!ctx) return fail(nullptr, HYQ_EINVAL, "null ctx");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  k_reset_counters<<<1, 1, 0, ctx->stream>>>(ctx->clk);
+  HQ_CHECK(ctx, cudaGetLastError());
+  return HYQ_OK;
+}
+
+int hyq_set_wavespeed_net(hyq_ctx* ctx, const float* w, double margin) {
+  if (!ctx || !w) return fail(ctx, HYQ_EINVAL, "null argument");
+  if (ctx->sc.mode != MODE_LEARNED) return fail(ctx, HYQ_EINVAL, "the context was not created with HYQ_MODE_LEARNED");
+  if (!(margin >= 0.0) || !(margin < 8.0)) return fail(ctx, HYQ_EINVAL, "margin must be in [0, 8)");
+  for (int i = 0; i < HYQ_NET_PARAMS; ++i)
+    if (!std::isfinite(w[i])) return fail(ctx, HYQ_EINVAL, "network parameters must be finite");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  HQ_CHECK(ctx, cudaMemcpyAsync(ctx->net_w, w, sizeof(float) * HYQ_NET_PARAMS, cudaMemcpyHostToDevice, ctx->stream));
+  int r = hyq_net_pack(ctx->net_w, ctx->net.image, ctx->stream);
+  if (r != HYQ_OK) return fail(ctx, r, hyq_last_error(nullptr));
+  HQ_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->sc.seed_margin = margin;
+  // the margin is a kernel argument of the captured step
+  if ((r = capture_graph(ctx)) != HYQ_OK) return r;
+  ctx->net_loaded = true;
+  return HYQ_OK;
+}
+
 int hyq_advance_async(hyq_ctx* ctx, int64_t max_steps) {
   if (!ctx || max_steps < 0) return fail(ctx, HYQ_EINVAL, "bad argument");
+  if (ctx->sc.mode == MODE_LEARNED && !ctx->net_loaded)
+    return fail(ctx, HYQ_EINVAL, "HYQ_MODE_LEARNED needs the wave-speed network (hyq_set_wavespeed_net) before stepping");
   HQ_CHECK(ctx, cudaSetDevice(ctx->device));
   for (int64_t s = 0; s < max_steps; ++s) HQ_CHECK(ctx, cudaGraphLaunch(ctx->exec, ctx->stream));
   return HYQ_OK;
@@ -376,7 +453,7 @@ int hyq_advance_timed(hyq_ctx* ctx, int64_t steps, float* ms) {
   cudaStream_t s = ctx->stream;
   for (int64_t it = 0; it < steps; ++it) {
     cudaEventRecord(ev[0], s);
-    launch_phase_A(ctx->sc, ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s, ev + 1);
+    launch_phase_A(ctx->sc, ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s, ev + 1, 0, -1, &ctx->net);
     k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
     cudaEventRecord(ev[6], s);
     k_hll<<<grid_of(N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
@@ -408,12 +485,15 @@ int hyq_stats_get(hyq_ctx* ctx, hyq_stats* out) {
   HQ_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
   out->t = h.t; out->dt = h.dt; out->vmax = h.vmax; out->nn = h.nn; out->status = h.status;
   out->done = (h.t < ctx->p.tmax && h.nn < ctx->p.nnmax) ? 0 : 1;
+  out->stage_cells = (int64_t)h.stage_cells;
+  out->fallback_cells = (int64_t)h.fb_cells;
   return HYQ_OK;
 }
 
 int hyq_advance(hyq_ctx* ctx, int64_t max_steps, double* t, int64_t* nn, int32_t* done) {
   int r = hyq_advance_async(ctx, max_steps);
   if (r) return r;
+  if ((r = net_status(ctx)) != HYQ_OK) return r;
   hyq_stats st;
   r = hyq_stats_get(ctx, &st);
   if (r) return r;
@@ -452,7 +532,7 @@ int hyq_step_host(hyq_ctx* ctx, const double* M_in, double* M_out, int32_t nslab
     HQ_CHECK(ctx, cudaMemcpy2DAsync(ctx->M + c0, pitch, M_in + c0, pitch, sizeof(double) * (size_t)(c1 - c0), 35, cudaMemcpyHostToDevice, cs));
     HQ_CHECK(ctx, cudaEventRecord(ctx->up[k], cs));
     HQ_CHECK(ctx, cudaStreamWaitEvent(s, ctx->up[k], 0));
-    launch_phase_A(ctx->sc, ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s, nullptr, c0, c1);
+    launch_phase_A(ctx->sc, ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s, nullptr, c0, c1, &ctx->net);
   }
   // the CFL reduction and the HLL sweep need every cell
   k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
@@ -524,6 +604,12 @@ int hyq_cells_collision(const double* M, int64_t n, double dt, double Kn, int32_
   CELLS_LAUNCH_CHECK();
   return HYQ_OK;
 }
+int hyq_cells_wavespeed_targets(const double* M, int64_t n, int32_t flag2D, double Ma, int32_t positivity, float* T, double* Mr, void* stream) {
+  if (!M || !T || n <= 0) return fail(nullptr, HYQ_EINVAL, "bad argument");
+  launch_cells_targets(M, n, flag2D, Ma, positivity, T, Mr, (cudaStream_t)stream);
+  CELLS_LAUNCH_CHECK();
+  return HYQ_OK;
+}
 int hyq_cells_phase_A(const double* M, int64_t n, int32_t flag2D, double Ma, int32_t positivity, double* Fx, double* Fy, double* Fz, double* Mr,
                       double* vp, void* stream) {
   if (!M || !Fx || !Fy || !Fz || !Mr || !vp || n <= 0) return fail(nullptr, HYQ_EINVAL, "bad argument");
@@ -546,12 +632,14 @@ struct hyq_batch {
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  cudaEvent_t replayed = nullptr;  // recorded after each hyq_batch_advance_async
 };
 
 void hyq_batch_destroy(hyq_batch* b) {
   if (!b) return;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->replayed) cudaEventDestroy(b->replayed);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -578,6 +666,7 @@ int hyq_batch_create(const hyq_params* p, int32_t n, hyq_batch** out) {
   }
   cudaError_t e;
   if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&b->replayed, cudaEventDisableTiming)) != cudaSuccess ||
       (e = cudaGraphCreate(&b->graph, 0)) != cudaSuccess) {
     const int r = cuda_fail(nullptr, e, "batch graph");
     hyq_batch_destroy(b);
@@ -619,6 +708,9 @@ int hyq_batch_advance_async(hyq_batch* b, int64_t max_steps) {
   // members' own streams may still hold a state upload or clock reset
   for (hyq_ctx* c : b->sims) HQ_CHECK(nullptr, cudaStreamSynchronize(c->stream));
   for (int64_t s = 0; s < max_steps; ++s) HQ_CHECK(nullptr, cudaGraphLaunch(b->exec, b->stream));
+  // member calls run on the members' own streams: order them after the replays
+  HQ_CHECK(nullptr, cudaEventRecord(b->replayed, b->stream));
+  for (hyq_ctx* c : b->sims) HQ_CHECK(nullptr, cudaStreamWaitEvent(c->stream, b->replayed, 0));
   return HYQ_OK;
 }
 

@@ -354,6 +354,7 @@ HQN int eig_real(double (&A)[N][N], double (&wr)[N], double (&wi)[N]) {
 
 }  // namespace hyq
 #include "hyq_eig6.cuh"
+#include "hyq_charpoly.cuh"
 namespace hyq {
 
 // eig_real<6> of a flux Jacobian: the register-resident path (hyq_eig6.cuh)
@@ -395,14 +396,24 @@ HQD bool eig_real_jac_p1(double (&h)[36], double (&wr)[6], double (&wi)[6]) {
 // the rest; JAC_P1 pattern-1 Jacobians only (any other defers the cell);
 // JAC_GEN the general code for every Jacobian (one compact code path for a
 // pass over cells most of whose Jacobians need it).  Identical results.
-enum JacMode { JAC_ANY = 0, JAC_P1 = 1, JAC_GEN = 2 };
+// JAC_CP (the learned wave-speed path) the register path for pattern-1
+// Jacobians and, for the rest, the certified characteristic-polynomial solve
+// of hyq_charpoly.cuh seeded by the predicted speeds; a Jacobian it cannot
+// certify defers the cell, which then takes the general code (the LAPACK
+// path) in the pass over listed cells.
+enum JacMode { JAC_ANY = 0, JAC_P1 = 1, JAC_GEN = 2, JAC_CP = 3 };
+
+// Predicted extreme eigenvalues of a plane's Jacobian (NaN: none) and the
+// normalised margin by which the certified solve moves them outward.
+struct Seeds { double lo, hi, margin; };
+HQD Seeds no_seeds() { Seeds s; s.lo = qnan(); s.hi = qnan(); s.margin = 0.0; return s; }
 
 // compute_jacobian_eigenvalues for one 15-moment slice: extreme real parts
 // and max |imag|.  A non-finite Jacobian gives NaN (the reference's guard).
 // Under JAC_P1 a Jacobian of another pattern sets `deferred` and leaves the
 // rest unset.
 struct EigOut { double vmin, vmax, imax; bool deferred; };
-template <int MODE> HQN EigOut jac_eigs_t(const double* ma) {
+template <int MODE> HQN EigOut jac_eigs_t(const double* ma, const Seeds sd) {
   double r3[6], r5[6], r6[6];
   jacobian6_rows(ma, r3, r5, r6);
   double h[36];  // the Jacobian, row-major, held in registers
@@ -421,6 +432,15 @@ template <int MODE> HQN EigOut jac_eigs_t(const double* ma) {
   double wr[6], wi[6];
   if (MODE == JAC_P1) {
     if (!eig_real_jac_p1(h, wr, wi)) { o.deferred = true; return o; }
+  } else if (MODE == JAC_CP) {
+    if (!eig_real_jac_p1(h, wr, wi)) {
+      const cp::Extremes e = cp::extremes(r3, r5, r6, sd.lo, sd.hi, sd.margin);
+      if (!e.ok) { o.deferred = true; return o; }
+      o.vmin = e.vmin;
+      o.vmax = e.vmax;
+      o.imax = 0.0;
+      return o;
+    }
   } else if (MODE == JAC_GEN) {
     double J[6][6];
 #pragma unroll
@@ -448,6 +468,7 @@ template <int MODE> HQN EigOut jac_eigs_t(const double* ma) {
   o.imax = im;
   return o;
 }
+template <int MODE> HQD EigOut jac_eigs_t(const double* ma) { return jac_eigs_t<MODE>(ma, no_seeds()); }
 HQD EigOut jac_eigs(const double* ma) { return jac_eigs_t<JAC_ANY>(ma); }
 
 // axis_moment_slice (src/utils/axis_moment_slice.jl:31-54), 0-based
@@ -519,13 +540,13 @@ enum EigStatus { EIG_DONE = 0, EIG_DEFERRED = 1, EIG_NEEDS_FIX = 2 };
 // from the same moments when it neither floors nor re-realizes them.
 template <int MODE, bool CORR>
 HQN int eigenvalues6_s(const double* M, int axis, int flag2D, double Ma, double& vmin, double& vmax, double* Mr, long long ist,
-                       long long ost, int* planes = nullptr, double* park = nullptr, long long pst = 0) {
+                       long long ost, int* planes = nullptr, double* park = nullptr, long long pst = 0, const Seeds sd = no_seeds()) {
   const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
   double a[15], b[15];
   for (int n = 0; n < 15; ++n) { a[n] = M[SLICE[sa][n] * ist]; b[n] = M[SLICE[sb][n] * ist]; }
-  EigOut ea = jac_eigs_t<MODE>(a);
+  EigOut ea = jac_eigs_t<MODE>(a, sd);
   if (ea.deferred) return EIG_DEFERRED;
-  EigOut eb = jac_eigs_t<MODE>(b);
+  EigOut eb = jac_eigs_t<MODE>(b, sd);
   if (eb.deferred) return EIG_DEFERRED;
   const double thr = 1000.0 * EPS;
   const bool ca = ea.imax > thr, cb = eb.imax > thr;
@@ -612,7 +633,8 @@ template <int MODE> HQN int eigenvalues6_flags_t(const double* M, int axis, long
 // is not NaN, NaN (the same numbers either way).
 template <int MODE, bool CORR>
 HQN int eigenvalues6z_s(const double* M, int flag2D, double Ma, int positivity, double& vmin, double& vmax, double* Mr, long long ist,
-                        long long ost, int* planes = nullptr, const double* parked = nullptr, long long pst = 0) {
+                        long long ost, int* planes = nullptr, const double* parked = nullptr, long long pst = 0,
+                        const Seeds sd = no_seeds()) {
   double Mw[35];
 #pragma unroll
   for (int n = 0; n < 35; ++n) Mw[n] = M[n * ist];
@@ -633,7 +655,7 @@ HQN int eigenvalues6z_s(const double* M, int flag2D, double Ma, int positivity, 
   }
   double a[15], b[15];
   for (int n = 0; n < 15; ++n) { a[n] = Mw[WUI[n]]; b[n] = Mw[SLICE[3][n]]; }
-  EigOut ea = jac_eigs_t<MODE>(a);
+  EigOut ea = jac_eigs_t<MODE>(a, sd);
   if (ea.deferred) return EIG_DEFERRED;
   EigOut eb;
   if (parked && same && !(parked[0] != parked[0] && parked[pst] != parked[pst])) {
@@ -641,7 +663,7 @@ HQN int eigenvalues6z_s(const double* M, int flag2D, double Ma, int positivity, 
     // eigenvalue with |imag| above the threshold
     eb.vmin = parked[0]; eb.vmax = parked[pst]; eb.imax = 0.0; eb.deferred = false;
   } else {
-    eb = jac_eigs_t<MODE>(b);
+    eb = jac_eigs_t<MODE>(b, sd);
     if (eb.deferred) return EIG_DEFERRED;
   }
   const double thr = 1000.0 * EPS;

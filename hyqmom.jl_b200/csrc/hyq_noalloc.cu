@@ -19,9 +19,11 @@
 // first, and every other region is written in full before it is read within
 // the same step.
 //
-// The first call on each device looks up the scratch address with
+// The first call on each device (and the first after a device reset, which
+// replaces the context) looks up the scratch address with
 // cudaGetSymbolAddress (which may load this module); make that first call
 // before any stream capture on that device.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <mutex>
 #include <string>
@@ -50,18 +52,57 @@ static __device__ __align__(256) double g_noalloc_scratch[kTotal];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
-double* g_scratch[kMaxDevices] = {};
+// Per device: the scratch address and the id of the CUDA context it was
+// looked up in.  A device reset (cudaDeviceReset) or a new primary context
+// reloads this module, which moves the scratch, so the address is looked up
+// again whenever the current context's id differs from the cached one.
+struct ScratchAddr {
+  unsigned long long ctx_id = 0;
+  double* ptr = nullptr;
+};
+ScratchAddr g_scratch[kMaxDevices];
 
-// Device address of the scratch on `dev` (the current device), looked up once.
+// The driver's cuCtxGetCurrent and cuCtxGetId, fetched through the runtime
+// (the library does not link libcuda directly).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+
+cudaError_t current_ctx_id(unsigned long long* id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  if (!get_current || !get_id) {
+    void* a = nullptr;
+    void* b = nullptr;
+    cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault);
+    if (e == cudaSuccess) e = cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault);
+    if (e != cudaSuccess) return e;
+    if (!a || !b) return cudaErrorSymbolNotFound;
+    get_current = reinterpret_cast<CtxGetCurrentFn>(a);
+    get_id = reinterpret_cast<CtxGetIdFn>(b);
+  }
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, id) != CUDA_SUCCESS) return cudaErrorDeviceUninitialized;
+  return cudaSuccess;
+}
+
+// Device address of the scratch on `dev` (the current device, whose primary
+// context the caller's cudaSetDevice has made current), looked up once per
+// context.
 cudaError_t scratch_for(int dev, double** out) {
   std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (!g_scratch[dev]) {
+  unsigned long long id = 0;
+  // cudaSetDevice (called before) initialises the device's primary context
+  // and makes it current
+  cudaError_t e = current_ctx_id(&id);
+  if (e != cudaSuccess) return e;
+  ScratchAddr& s = g_scratch[dev];
+  if (!s.ptr || s.ctx_id != id) {
     void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_scratch[dev] = static_cast<double*>(p);
+    if ((e = cudaGetSymbolAddress(&p, g_noalloc_scratch)) != cudaSuccess) return e;
+    s.ptr = static_cast<double*>(p);
+    s.ctx_id = id;
   }
-  *out = g_scratch[dev];
+  *out = s.ptr;
   return cudaSuccess;
 }
 
@@ -77,6 +118,7 @@ extern "C" int hyq_step_noalloc(const hyq_params* p, double* M, hyq_stats* stats
     return report_error(HYQ_EINVAL, "grid must have Nx >= 2, Ny >= 2, Nz >= 1 (pas_HLL needs two cells per row)");
   if (!(p->CFL > 0) || !(p->Kn > 0) || !(p->dtmax > 0)) return report_error(HYQ_EINVAL, "CFL, Kn and dtmax must be positive");
   if (p->device < 0 || p->device >= kMaxDevices) return report_error(HYQ_EINVAL, "device index out of range");
+  if (p->mode != HYQ_MODE_PLAIN) return report_error(HYQ_EINVAL, "hyq_step_noalloc runs the plain eigenvalue path only (mode 0)");
   const long long N = (long long)p->Nx * p->Ny * p->Nz;
   if (N > kMax)
     return report_error(HYQ_EINVAL, ("grid has " + std::to_string(N) + " cells; hyq_step_noalloc supports at most " +
@@ -92,6 +134,9 @@ extern "C" int hyq_step_noalloc(const hyq_params* p, double* M, hyq_stats* stats
   sc.nnmax = p->nnmax; sc.tmax = p->tmax; sc.Kn = p->Kn; sc.Ma = p->Ma; sc.CFL = p->CFL; sc.dtmax = p->dtmax;
   sc.dx = (p->xmax - p->xmin) / p->Nx; sc.dy = (p->ymax - p->ymin) / p->Ny; sc.dz = (p->zmax - p->zmin) / p->Nz;
   sc.nblocksA = grid_of(N, BS_A);
+  sc.mode = MODE_PLAIN;
+  sc.seeds = nullptr;
+  sc.seed_margin = 0.0;
 
   DevClock* clk = reinterpret_cast<DevClock*>(base + kClock);
   double* blockmax = base + kBlockmax;

@@ -15,7 +15,14 @@ struct DevClock {
   // eigen-solve takes every cell directly (set when a stage listed most of its
   // cells; 0: the pattern-1 kernel first)
   int dense[5];
+  // learned wave-speed path: cells whose Jacobians the certified solve could
+  // not certify (they fell back to the LAPACK path), and cells the certified
+  // stages processed, summed over stages and steps since the last reset
+  unsigned long long fb_cells, stage_cells;
 };
+
+// Eigenvalue path of a context (hyq_params.mode).
+enum StepMode { MODE_PLAIN = 0, MODE_LEARNED = 1, MODE_CERTIFIED = 2 };
 
 // Per-context constants of the step.
 struct StepConst {
@@ -24,6 +31,17 @@ struct StepConst {
   long long nnmax;
   double tmax, Kn, Ma, CFL, dtmax, dx, dy, dz;
   int nblocksA;
+  // MODE_PLAIN: the LAPACK-path eigen-solve of the reference for every
+  // Jacobian.  MODE_CERTIFIED: the certified characteristic-polynomial solve
+  // (hyq_charpoly.cuh) for every Jacobian it can certify, from bound starts.
+  // MODE_LEARNED: the same, started from the wave-speed network's predicted
+  // speeds, which the network kernel writes to `seeds` after the first
+  // closure of each step.
+  int mode;
+  // predicted standardized extreme speeds, SoA [6][N] (x lo, x hi, y lo,
+  // y hi, z lo, z hi): lam = u + sqrt(C_aa) * s; NULL unless MODE_LEARNED
+  float* seeds;
+  double seed_margin;  // normalised outward shift of the seeds
 };
 
 // Minimum resident blocks per SM requested from ptxas for the per-cell
@@ -80,8 +98,17 @@ inline int grid_of(long long n, int bs) { return int((n + bs - 1) / bs); }
 // recorded after A1, A2, A3, A4 (each with its passes over listed cells) and
 // A5.  [c0, c1):
 // the cells to process (default all; c0 a multiple of BS_A).
+// The wave-speed network of MODE_LEARNED on the device: its BF16 weight
+// image (k_mlp.cu layout) and an error word set when a bounded wait of its
+// kernel ran out.
+struct WaveNet {
+  unsigned char* image;
+  int* err;
+};
+// net: the wave-speed network (MODE_LEARNED only).
 void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, double* Fy, double* Fz, double* vp, double* blockmax,
-                    DevClock* clk, cudaStream_t s, cudaEvent_t* ev = nullptr, long long c0 = 0, long long c1 = -1);
+                    DevClock* clk, cudaStream_t s, cudaEvent_t* ev = nullptr, long long c0 = 0, long long c1 = -1,
+                    const WaveNet* net = nullptr);
 // Phases [E]+[F] from Min to Mout; Fx, Fy, Fz are overwritten and vp (6N
 // doubles, dead after the HLL sweep) holds the correction lists.
 // ev (optional): four events recorded after E1, E2, E3 and E4.
@@ -94,6 +121,7 @@ void launch_cells_eig(const double* M, long long n, int axis, int flag2D, double
 void launch_cells_closure_eigs(const double* mom, long long n, double* v, cudaStream_t s);
 void launch_cells_collision(const double* M, long long n, double dt, double Kn, int positivity, double* out, cudaStream_t s);
 void launch_std_central(const double* M, long long n, double* S, double* C, cudaStream_t s);
+void launch_cells_targets(const double* M, long long n, int flag2D, double Ma, int positivity, float* T, double* Mr, cudaStream_t s);
 // (defined in hyq_b200.cu) the CFL, HLL and clock-reset launches of one step,
 // and the thread-local error text read by hyq_last_error(NULL)
 void launch_cfl(const double* blockmax, const StepConst& sc, DevClock* clk, cudaStream_t s);
@@ -101,6 +129,13 @@ void launch_hll(const double* M, const double* Fx, const double* Fy, const doubl
                 const DevClock* clk, cudaStream_t s);
 void launch_set_clock(DevClock* clk, double t, long long nn, cudaStream_t s);
 int report_error(int code, const char* msg);
+// (defined in k_mlp.cu) the wave-speed network on the realized moments of
+// phase [A]'s first closure (moment-major, stride N, cells [c0, c1)): writes
+// sc.seeds for those cells.  net_set_smem raises the kernels' shared-memory
+// limit (call before the first launch on a device).
+cudaError_t net_set_smem();
+void launch_wavespeed_seeds(const StepConst& sc, const double* Mr, const WaveNet* net, float* seeds, const DevClock* clk, cudaStream_t s,
+                            long long c0, long long c1);
 
 }  // namespace hyqk
 

@@ -9,6 +9,8 @@ using namespace hyq;
 namespace hyqk {
 namespace {
 
+__device__ __forceinline__ float qnan_f() { return __int_as_float(0x7fc00000); }
+
 __global__ void __launch_bounds__(BS_CELLS) k_cells_flux(const double* __restrict__ M, long long n, int flag2D, double Ma, double* Fx, double* Fy,
                                                           double* Fz, double* Mr) {
   const long long c = (long long)blockIdx.x * BS_CELLS + threadIdx.x;
@@ -70,7 +72,40 @@ __global__ void __launch_bounds__(BS_CELLS) k_std_central(const double* __restri
   }
 }
 
+// Training targets of the wave-speed network: phase [A]'s first closure,
+// then the x, y and z eigenvalue functions (the plain path, with their
+// corrections) as the step runs them; the six extreme speeds standardized by
+// the realized moments' mean velocity and variance along each axis.
+__global__ void __launch_bounds__(BS_CELLS) k_cells_targets(const double* __restrict__ M, long long n, int flag2D, double Ma, int positivity,
+                                                             float* __restrict__ T, double* __restrict__ Mr) {
+  const long long c = (long long)blockIdx.x * BS_CELLS + threadIdx.x;
+  if (c >= n) return;
+  double m[35], a[35], b[35];
+  for (int q = 0; q < 35; ++q) m[q] = M[c + n * q];
+  flux_closure35(m, flag2D, Ma, nullptr, nullptr, nullptr, a);
+  if (Mr) for (int q = 0; q < 35; ++q) Mr[c + n * q] = a[q];
+  double v[6];
+  eigenvalues6(a, 1, flag2D, Ma, v[0], v[1], b);
+  eigenvalues6(b, 2, flag2D, Ma, v[2], v[3], m);
+  eigenvalues6z(m, flag2D, Ma, positivity, v[4], v[5], b);
+  const int iu[3] = {1, 5, 15}, i2[3] = {2, 9, 19};
+  for (int d = 0; d < 3; ++d) {
+    const double mu = a[iu[d]] / a[0], var = a[i2[d]] / a[0] - mu * mu;
+    const double sd = sqrt(var);
+    for (int q = 0; q < 2; ++q) {
+      const double s = (v[2 * d + q] - mu) / sd;
+      T[c * 8 + 2 * d + q] = isfinite(s) ? (float)s : qnan_f();
+    }
+  }
+  T[c * 8 + 6] = 0.0f;
+  T[c * 8 + 7] = 0.0f;
+}
+
 }  // namespace
+
+void launch_cells_targets(const double* M, long long n, int flag2D, double Ma, int positivity, float* T, double* Mr, cudaStream_t s) {
+  k_cells_targets<<<grid_of(n, BS_CELLS), BS_CELLS, 0, s>>>(M, n, flag2D, Ma, positivity, T, Mr);
+}
 
 void launch_cells_flux(const double* M, long long n, int flag2D, double Ma, double* Fx, double* Fy, double* Fz, double* Mr, cudaStream_t s) {
   k_cells_flux<<<grid_of(n, BS_CELLS), BS_CELLS, 0, s>>>(M, n, flag2D, Ma, Fx, Fy, Fz, Mr);

@@ -65,6 +65,24 @@ __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure(const double*
   flux_closure35(M + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
 }
 
+// The learned path's seeds of plane Jacobians along `axis` for cell c: the
+// network's standardized extreme speeds mapped back with the stage input's
+// mean velocity and variance along the axis (NaN seeds when there are none).
+__device__ __forceinline__ Seeds stage_seeds(const double* in, long long c, int axis, const StepConst& sc) {
+  if (!sc.seeds) return no_seeds();
+  const long long N = sc.N;
+  const int iu = axis == 1 ? 1 : (axis == 2 ? 5 : 15), i2 = axis == 1 ? 2 : (axis == 2 ? 9 : 19);
+  const double m0 = in[c], mu = in[c + N * iu] / m0;
+  const double var = in[c + N * i2] / m0 - mu * mu;
+  const double sd = sqrt(var > 0.0 ? var : 0.0);
+  const float* sp = sc.seeds + 2 * (axis - 1) * N + c;
+  Seeds s;
+  s.lo = mu + sd * (double)sp[0];
+  s.hi = mu + sd * (double)sp[N];
+  s.margin = sc.seed_margin;
+  return s;
+}
+
 // eigenvalues6_hyperbolic_3D along x (axis 1) or y (axis 2), and
 // eigenvalues6z_hyperbolic_3D (axis 3), as a part (MODE, CORR) for cell c; a
 // cell left for the correction gets its list code in *code.  The y stage
@@ -77,23 +95,42 @@ __device__ __forceinline__ int eig_stage(const double* in, double* out, double* 
   const long long N = sc.N;
   int planes = 0;
   double* park = vp + 4 * N + c;
-  const int st = axis == 3 ? eigenvalues6z_s<MODE, CORR>(in + c, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out + c, N, N, &planes, park, N)
+  const Seeds sd = (MODE == JAC_CP) ? stage_seeds(in, c, axis, sc) : no_seeds();
+  const int st = axis == 3 ? eigenvalues6z_s<MODE, CORR>(in + c, sc.flag2D, sc.Ma, sc.positivity, lo, hi, out + c, N, N, &planes, park, N, sd)
                            : eigenvalues6_s<MODE, CORR>(in + c, axis, sc.flag2D, sc.Ma, lo, hi, out + c, N, N, &planes,
-                                                        axis == 2 ? park : nullptr, N);
+                                                        axis == 2 ? park : nullptr, N, sd);
   if (code) *code = st == EIG_NEEDS_FIX ? (planes ? (unsigned int)planes : 4u) : 0u;
   return st;
 }
 
-// A2/A3/A4: the pattern-1 part; cells left go to the list, marked when they
-// need the correction
+// Warp-aggregated count of the calling threads with `flag` set, added to *ctr.
+__device__ __forceinline__ void count_flag(bool flag, unsigned long long* ctr) {
+  const unsigned int act = __activemask();
+  const unsigned int m = __ballot_sync(act, flag);
+  if (m && (int)(threadIdx.x & 31) == __ffs(act) - 1) atomicAdd(ctr, (unsigned long long)__popc(m));
+}
+
+// A2/A3/A4: the pattern-1 part (JM = EIG_MODE) or, on the certified and
+// learned paths, the pattern-1 part and the certified solve (JM = JAC_CP);
+// cells left go to the list, marked when they need the correction.  JAC_CP
+// counts the cells it had to leave to the LAPACK path (list code 0).
+template <int JM>
 __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* in, double* out, double* vp,
-                                                         int axis, const StepConst sc, const DevClock* clk, long long c0, long long c1) {
-  if (!phase_A_active(sc, clk) || clk->dense[axis - 1]) return;
+                                                         int axis, const StepConst sc, DevClock* clk, long long c0, long long c1) {
+  if (!phase_A_active(sc, clk)) return;
+  const bool dense = clk->dense[axis - 1] != 0;
+  if (JM == JAC_CP && blockIdx.x == 0 && threadIdx.x == 0) {
+    atomicAdd(&clk->stage_cells, (unsigned long long)(c1 - c0));
+    if (dense) atomicAdd(&clk->fb_cells, (unsigned long long)(c1 - c0));  // every cell to the LAPACK path
+  }
+  if (dense) return;
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
   if (c >= c1) return;
   double lo, hi;
   unsigned int code;
-  if (eig_stage<EIG_MODE, false>(in, out, vp, c, axis, sc, lo, hi, &code) == EIG_DONE) {
+  const int st = eig_stage<JM, false>(in, out, vp, c, axis, sc, lo, hi, &code);
+  if (JM == JAC_CP) count_flag(st == EIG_DEFERRED, &clk->fb_cells);
+  if (st == EIG_DONE) {
     double* v = vp + 2 * (axis - 1) * N;
     v[c] = lo; v[c + N] = hi;
   } else {
@@ -201,18 +238,20 @@ __global__ void __launch_bounds__(BS_CELLS) k_cells_phase_A(const double* __rest
 }  // namespace
 
 void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, double* Fy, double* Fz, double* vp, double* blockmax,
-                    DevClock* clk, cudaStream_t s, cudaEvent_t* ev, long long c0, long long c1) {
+                    DevClock* clk, cudaStream_t s, cudaEvent_t* ev, long long c0, long long c1, const WaveNet* net) {
   const long long N = sc.N;
   if (c1 < 0) c1 = N;
   const int g = grid_of(c1 - c0, BS_A);
   const int gfix = g;  // one thread per possible list entry: blocks past the count exit at once
   const int gcorr = g < CORR_BLOCKS ? g : CORR_BLOCKS;
   k_A1_closure<<<g, BS_A, 0, s>>>(M, Fx, vp, sc, clk, c0, c1);
+  if (sc.mode == MODE_LEARNED) launch_wavespeed_seeds(sc, Fx, net, sc.seeds, clk, s, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
   double* const ins[3] = {Fx, Fx, Fx};
   double* const outs[3] = {Fx, Fx, Mtmp};  // x and y in place
   for (int axis = 1; axis <= 3; ++axis) {
-    k_A_eig<<<g, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
+    if (sc.mode == MODE_PLAIN) k_A_eig<EIG_MODE><<<g, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
+    else k_A_eig<JAC_CP><<<g, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
     k_A_fix<<<gfix, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
     k_A_corr<<<gcorr, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
     if (ev) cudaEventRecord(ev[axis], s);

@@ -35,15 +35,31 @@ __global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E1_closure(const double
   flux_closure35(in + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
 }
 
+// Warp-aggregated count of the calling threads with `flag` set, added to *ctr.
+__device__ __forceinline__ void count_flag_ef(bool flag, unsigned long long* ctr) {
+  const unsigned int act = __activemask();
+  const unsigned int m = __ballot_sync(act, flag);
+  if (m && (int)(threadIdx.x & 31) == __ffs(act) - 1) atomicAdd(ctr, (unsigned long long)__popc(m));
+}
+
 // E2/E3: eigenvalues6_hyperbolic_3D along x or y: copy, and list the cells
-// that need the correction or the complete eigen-solve (counter `which`)
+// that need the correction or the complete eigen-solve (counter `which`).
+// JM = EIG_MODE: the pattern-1 register path; JM = JAC_CP (certified and
+// learned paths): that path or the certified solve, which decides a Jacobian
+// without its eigenvalues; the cells it leaves to the LAPACK path are counted.
+template <int JM>
 __global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* in, double* out, double* vp, int axis,
-                                                           int which, const StepConst sc, const DevClock* clk, long long c0, long long c1) {
+                                                           int which, const StepConst sc, DevClock* clk, long long c0, long long c1) {
   if (!clk->active) return;
+  const bool dense = clk->dense[3 + which] != 0;
+  if (JM == JAC_CP && blockIdx.x == 0 && threadIdx.x == 0) {
+    atomicAdd(&clk->stage_cells, (unsigned long long)(c1 - c0));
+    if (dense) atomicAdd(&clk->fb_cells, (unsigned long long)(c1 - c0));
+  }
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
   if (c >= c1) return;
-  const bool dense = clk->dense[3 + which] != 0;
-  const int planes = dense ? 0 : eigenvalues6_flags_t<EIG_MODE>(in + c, axis, N);
+  const int planes = dense ? 0 : eigenvalues6_flags_t<JM>(in + c, axis, N);
+  if (JM == JAC_CP && !dense) count_flag_ef(planes < 0, &clk->fb_cells);
   if (out != in) {
 #pragma unroll
     for (int n = 0; n < 35; ++n) out[c + N * n] = in[c + N * n];
@@ -129,11 +145,13 @@ void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, doubl
   const int gcorr = g < CORR_BLOCKS ? g : CORR_BLOCKS;
   k_E1_closure<<<g, BS_EF, 0, s>>>(Min, Fx, vp, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
-  k_E_eig<<<g, BS_EF, 0, s>>>(Fx, Fx, vp, 1, 0, sc, clk, c0, c1);
+  if (sc.mode == MODE_PLAIN) k_E_eig<EIG_MODE><<<g, BS_EF, 0, s>>>(Fx, Fx, vp, 1, 0, sc, clk, c0, c1);
+  else k_E_eig<JAC_CP><<<g, BS_EF, 0, s>>>(Fx, Fx, vp, 1, 0, sc, clk, c0, c1);
   k_E_fix<<<gfix, BS_EF, 0, s>>>(Fx, vp, 1, 0, sc, clk, c0, c1);
   k_E_corr<<<gcorr, BS_EF, 0, s>>>(Fx, Fx, vp, 1, 0, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[1], s);
-  k_E_eig<<<g, BS_EF, 0, s>>>(Fx, Fx, vp, 2, 1, sc, clk, c0, c1);
+  if (sc.mode == MODE_PLAIN) k_E_eig<EIG_MODE><<<g, BS_EF, 0, s>>>(Fx, Fx, vp, 2, 1, sc, clk, c0, c1);
+  else k_E_eig<JAC_CP><<<g, BS_EF, 0, s>>>(Fx, Fx, vp, 2, 1, sc, clk, c0, c1);
   k_E_fix<<<gfix, BS_EF, 0, s>>>(Fx, vp, 2, 1, sc, clk, c0, c1);
   k_E_corr<<<gcorr, BS_EF, 0, s>>>(Fx, Fx, vp, 2, 1, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[2], s);

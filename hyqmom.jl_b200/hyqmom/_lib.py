@@ -19,12 +19,20 @@ class HyqParams(ctypes.Structure):
                 ("positivity", ctypes.c_int32), ("device", ctypes.c_int32), ("nnmax", ctypes.c_int64),
                 ("tmax", ctypes.c_double), ("Kn", ctypes.c_double), ("Ma", ctypes.c_double), ("CFL", ctypes.c_double),
                 ("dtmax", ctypes.c_double), ("xmin", ctypes.c_double), ("xmax", ctypes.c_double),
-                ("ymin", ctypes.c_double), ("ymax", ctypes.c_double), ("zmin", ctypes.c_double), ("zmax", ctypes.c_double)]
+                ("ymin", ctypes.c_double), ("ymax", ctypes.c_double), ("zmin", ctypes.c_double), ("zmax", ctypes.c_double),
+                ("mode", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+# hyq_params.mode
+MODE_PLAIN, MODE_LEARNED, MODE_CERTIFIED = 0, 1, 2
+MODES = {"plain": MODE_PLAIN, "learned": MODE_LEARNED, "certified": MODE_CERTIFIED}
+NET_PARAMS = 38406  # HYQ_NET_PARAMS
 
 
 class HyqStats(ctypes.Structure):
     _fields_ = [("t", ctypes.c_double), ("dt", ctypes.c_double), ("vmax", ctypes.c_double), ("nn", ctypes.c_int64),
-                ("done", ctypes.c_int32), ("status", ctypes.c_int32)]
+                ("done", ctypes.c_int32), ("status", ctypes.c_int32), ("stage_cells", ctypes.c_int64),
+                ("fallback_cells", ctypes.c_int64)]
 
 
 class HyqError(RuntimeError):
@@ -38,7 +46,9 @@ SYMBOLS = ["hyq_abi_version", "hyq_create", "hyq_destroy", "hyq_last_error", "hy
            "hyq_set_state_device", "hyq_get_state_device", "hyq_set_clock", "hyq_advance", "hyq_advance_async",
            "hyq_synchronize", "hyq_stats_get", "hyq_advance_timed", "hyq_step_host", "hyq_get_SC", "hyq_stream", "hyq_cells_flux_closure",
            "hyq_cells_eigenvalues", "hyq_cells_closure_eigs", "hyq_cells_collision", "hyq_cells_phase_A", "hyq_step_noalloc", "hyq_batch_create", "hyq_batch_destroy", "hyq_batch_size",
-           "hyq_batch_member", "hyq_batch_stream", "hyq_batch_advance_async", "hyq_batch_advance"]
+           "hyq_batch_member", "hyq_batch_stream", "hyq_batch_advance_async", "hyq_batch_advance", "hyq_reset_counters",
+           "hyq_set_wavespeed_net", "hyq_net_image_bytes", "hyq_net_tile_bytes", "hyq_net_scratch_bytes", "hyq_net_pack",
+           "hyq_net_features", "hyq_net_forward", "hyq_net_train_batch", "hyq_net_adam", "hyq_cells_wavespeed_targets"]
 NOALLOC_MAX_CELLS = 16384  # HYQ_NOALLOC_MAX_CELLS
 
 
@@ -87,6 +97,19 @@ def load(path=None):
     lib.hyq_batch_stream.restype = vp
     lib.hyq_batch_advance_async.argtypes = [vp, i64]
     lib.hyq_batch_advance.argtypes = [vp, i64, ctypes.POINTER(i32), ctypes.POINTER(i32)]
+    flt = ctypes.c_float
+    lib.hyq_reset_counters.argtypes = [vp]
+    lib.hyq_set_wavespeed_net.argtypes = [vp, vp, dbl]
+    for nm in ("hyq_net_image_bytes", "hyq_net_tile_bytes"):
+        getattr(lib, nm).restype = i64
+    lib.hyq_net_scratch_bytes.argtypes = [i32]
+    lib.hyq_net_scratch_bytes.restype = i64
+    lib.hyq_net_pack.argtypes = [vp, vp, vp]
+    lib.hyq_net_features.argtypes = [vp, i64, vp, vp]
+    lib.hyq_net_forward.argtypes = [vp, vp, i64, vp, vp, vp]
+    lib.hyq_net_train_batch.argtypes = [vp, vp, vp, i64, vp, i32, flt, vp, vp, i32, vp, vp, vp]
+    lib.hyq_net_adam.argtypes = [vp, vp, vp, vp, i32, flt, flt, flt, flt, flt, i32, vp, vp]
+    lib.hyq_cells_wavespeed_targets.argtypes = [vp, i64, i32, dbl, i32, vp, vp, vp]
     _lib = lib
     return lib
 

@@ -17,24 +17,32 @@ from . import ic as _ic
 from .snapshots import SnapshotWriter
 
 
-def params_struct(p, device=0):
-    """hyq_params of a reference-style parameter dict."""
+def params_struct(p, device=0, mode="plain"):
+    """hyq_params of a reference-style parameter dict; mode: "plain" (the
+    reference's eigenvalue path), "learned" or "certified"."""
     xmin, xmax, ymin, ymax, zmin, zmax = _ic.extents(p)
     return _lib.HyqParams(Nx=p["Nx"], Ny=p["Ny"], Nz=p["Nz"], flag2D=int(p["flag2D"]),
                           positivity=int(bool(p.get("positivity", True))), device=device, nnmax=int(p["nnmax"]),
                           tmax=float(p["tmax"]), Kn=float(p["Kn"]), Ma=float(p["Ma"]), CFL=float(p["CFL"]),
-                          dtmax=float(p["dtmax"]), xmin=xmin, xmax=xmax, ymin=ymin, ymax=ymax, zmin=zmin, zmax=zmax)
+                          dtmax=float(p["dtmax"]), xmin=xmin, xmax=xmax, ymin=ymin, ymax=ymax, zmin=zmin, zmax=zmax,
+                          mode=_lib.MODES[mode] if isinstance(mode, str) else int(mode))
 
 
 class Solver:
-    """One simulation domain on one GPU (a hyq_ctx)."""
+    """One simulation domain on one GPU (a hyq_ctx).
 
-    def __init__(self, params, device=0, _handle=None):
+    mode: "plain" (the reference's LAPACK-path eigen-solves), "learned" (the
+    wave-speed network seeds a certified characteristic-polynomial solve;
+    `net` is the network, a hyqmom.wavenet.WaveNet or None for the packaged
+    one) or "certified" (the certified solve without the network)."""
+
+    def __init__(self, params, device=0, _handle=None, mode="plain", net=None):
         lib = _lib.load()
         p = params
         self._owns = _handle is None
+        self.mode = mode
         if _handle is None:
-            hp = params_struct(p, device)
+            hp = params_struct(p, device, mode)
             h = ctypes.c_void_p()
             rc = lib.hyq_create(ctypes.byref(hp), ctypes.byref(h))
             if rc != 0:
@@ -43,6 +51,15 @@ class Solver:
             h = ctypes.c_void_p(_handle)
         self._lib, self._h, self.params = lib, h, dict(p)
         self.shape = (p["Nx"], p["Ny"], p["Nz"], 35)
+        if mode == "learned" and _handle is None:
+            from . import wavenet
+            self.set_wavespeed_net(net if net is not None else wavenet.load_default())
+
+    def set_wavespeed_net(self, net):
+        """Upload the wave-speed network (a hyqmom.wavenet.WaveNet)."""
+        w = np.ascontiguousarray(net.params, dtype=np.float32)
+        assert w.size == _lib.NET_PARAMS
+        self._chk(self._lib.hyq_set_wavespeed_net(self._h, w.ctypes.data, float(net.margin)))
 
     def close(self):
         if self._h:
@@ -117,7 +134,11 @@ class Solver:
     def stats(self):
         st = _lib.HyqStats()
         self._chk(self._lib.hyq_stats_get(self._h, ctypes.byref(st)))
-        return dict(t=st.t, dt=st.dt, vmax=st.vmax, nn=st.nn, done=bool(st.done), status=st.status)
+        return dict(t=st.t, dt=st.dt, vmax=st.vmax, nn=st.nn, done=bool(st.done), status=st.status,
+                    stage_cells=st.stage_cells, fallback_cells=st.fallback_cells)
+
+    def reset_counters(self):
+        self._chk(self._lib.hyq_reset_counters(self._h))
 
     @property
     def stream(self):
@@ -196,6 +217,8 @@ def simulation_runner(params, device=0, verbose=False, chunk=64):
         solver.set_state(M0)
         writer = None
         if interval > 0:
+            # the reference's default name (src/simulation_runner.jl:283-289);
+            # the writer stores it as .npz (see snapshots.py)
             fname = p.get("snapshot_filename") or "snapshots_Nx%d_Ny%d_Nz%d_Kn%.2f_Ma%.2f_tmax%.4f.jld2" % (
                 p["Nx"], p["Ny"], p["Nz"], p["Kn"], p["Ma"], p["tmax"])
             writer = SnapshotWriter(fname, p, interval)

@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define HYQ_ABI_VERSION 1
+#define HYQ_ABI_VERSION 2
 
 #define HYQ_OK 0
 #define HYQ_EINVAL -1      /* invalid argument or parameter */
@@ -34,6 +34,25 @@ extern "C" {
 #define HYQ_ENONFINITE -3  /* non-finite state found (opt-in check) */
 #define HYQ_ETIMEOUT -4    /* a bounded device wait ran out */
 #define HYQ_ENOMEM -5      /* device allocation failed */
+
+/* Eigenvalue path of a context (hyq_params.mode).
+ * HYQ_MODE_PLAIN: every flux-Jacobian eigen-solve follows the reference's
+ *   LAPACK path (eigvals), bit for bit.
+ * HYQ_MODE_LEARNED: the learned wave-speed path.  After the first closure of
+ *   each step a small network (35 standardized moments -> 6 standardized
+ *   extreme speeds, BF16 tensor-core kernels) predicts each cell's extreme
+ *   x/y/z wave speeds; they seed a certified solve of each Jacobian's
+ *   characteristic polynomial, which proves all six eigenvalues real and
+ *   distinct and converges the extremes to full FP64 precision.  Jacobians it
+ *   cannot certify (and the usual pattern-1 Jacobians, which are cheap) take
+ *   the LAPACK path, so the speeds agree with the plain path to round-off and
+ *   every complex-eigenvalue decision is the reference's.  Needs the network
+ *   (hyq_set_wavespeed_net) before the first step.
+ * HYQ_MODE_CERTIFIED: the same certified solve started from bounds instead of
+ *   predicted speeds (the learned path without its network). */
+#define HYQ_MODE_PLAIN 0
+#define HYQ_MODE_LEARNED 1
+#define HYQ_MODE_CERTIFIED 2
 
 /* Fields read by simulation_runner (src/simulation_runner.jl:74-129). */
 typedef struct hyq_params {
@@ -44,6 +63,8 @@ typedef struct hyq_params {
   int64_t nnmax;       /* params.nnmax */
   double tmax, Kn, Ma, CFL, dtmax;
   double xmin, xmax, ymin, ymax, zmin, zmax; /* domain extents (:123-129) */
+  int32_t mode;        /* HYQ_MODE_* (0 = plain, the reference's path) */
+  int32_t reserved;
 } hyq_params;
 
 typedef struct hyq_stats {
@@ -51,6 +72,11 @@ typedef struct hyq_stats {
   int64_t nn;          /* steps taken */
   int32_t done;        /* 1 once t >= tmax or nn >= nnmax */
   int32_t status;      /* 0 = ok; k > 0: step k met a non-finite wave speed */
+  /* learned / certified modes, summed since hyq_set_state or
+   * hyq_reset_counters: cells of the certified eigenvalue stages (five per
+   * step: x, y, z before the flux, x, y after it) and those of them that fell
+   * back to the LAPACK path (a Jacobian not certified).  0 in plain mode. */
+  int64_t stage_cells, fallback_cells;
 } hyq_stats;
 
 typedef struct hyq_ctx hyq_ctx;
@@ -67,11 +93,70 @@ const char* hyq_last_error(const hyq_ctx* ctx);
  * by hyq_set_state (simulation_runner's t = 0.0; nn = 0, :333-334). */
 int hyq_set_state(hyq_ctx* ctx, const double* M);
 int hyq_get_state(hyq_ctx* ctx, double* M);
-/* Device-pointer variants (same layout, device memory of ctx's device). */
+/* Device-pointer variants (same layout, device memory of ctx's device).
+ * Both copy on the context's stream (hyq_stream), a non-blocking stream that
+ * is not ordered against the caller's streams (nor the legacy default
+ * stream), and return before the copy has finished.  A caller that writes dM
+ * on its own stream must finish that work before hyq_set_state_device, and
+ * must order any use of dM after hyq_get_state_device behind the context's
+ * stream (hyq_synchronize, or an event recorded on hyq_stream). */
 int hyq_set_state_device(hyq_ctx* ctx, const double* dM);
 int hyq_get_state_device(hyq_ctx* ctx, double* dM);
 /* Set the loop clock (t, nn) without touching the state. */
 int hyq_set_clock(hyq_ctx* ctx, double t, int64_t nn);
+/* Zero the fallback counters of hyq_stats. */
+int hyq_reset_counters(hyq_ctx* ctx);
+
+/* The wave-speed network of HYQ_MODE_LEARNED (no reference counterpart: it
+ * replaces nothing, it only seeds the certified solve of
+ * compute_jacobian_eigenvalues, src/numerics/compute_jacobian_eigenvalues.jl:18-50).
+ * w: HYQ_NET_PARAMS floats, the FP32 parameters in this order (row-major,
+ * out x in): W1 (128 x 35), b1 (128), W2 (128 x 128), b2 (128),
+ * W3 (128 x 128), b3 (128), W4 (6 x 128), b4 (6); SiLU between layers.
+ * Inputs: the cell's 35 standardized moments (M2CS4_35's S); outputs: the
+ * extreme eigenvalues of the x, y and z flux Jacobians as (lam - u_a) /
+ * sqrt(C_aa), in the order x min, x max, y min, y max, z min, z max.
+ * margin: normalised distance by which the seeds are moved outward.  The
+ * weights are stored as BF16 on the device. */
+#define HYQ_NET_PARAMS 38406
+int hyq_set_wavespeed_net(hyq_ctx* ctx, const float* w, double margin);
+
+/* ---- the wave-speed network's own kernels (device pointers) ---------------
+ * No reference counterpart: these train and evaluate the network of
+ * HYQ_MODE_LEARNED with hand-written tcgen05 (BF16 x BF16 -> FP32) kernels.
+ * All pointers are device memory of the current device; every call is
+ * asynchronous on `stream` (a cudaStream_t, NULL for the legacy stream).
+ * Kernel waits are bounded: a wait that runs out sets *err (device int) to a
+ * nonzero value instead of hanging; check it after synchronising.
+ *   image: hyq_net_image_bytes() bytes, the BF16 weight image (hyq_net_pack).
+ *   X: training inputs, ceil(n / 128) tiles of hyq_net_tile_bytes() bytes
+ *      (hyq_net_features of the moments, stride n).
+ *   T: targets, n rows of 8 floats (the 6 outputs, 2 unused).
+ *   order: the tiles of one batch (ntiles indices into X).
+ *   partial: nparts * HYQ_NET_PARAMS floats of per-CTA gradients (nparts
+ *      CTAs run the batch); ds_scratch: hyq_net_scratch_bytes(nparts) bytes.
+ *   loss: += the batch's sum of squared errors; the gradient is that of
+ *      dscale / 2 * (sum of squared errors), dscale = 2 / (rows * 6) for the
+ *      mean square error.
+ *   hyq_net_adam sums the partials (into gout, when not NULL) and, with
+ *   lr > 0, takes one Adam step (decoupled weight decay wd) on w. */
+int64_t hyq_net_image_bytes(void);
+int64_t hyq_net_tile_bytes(void);
+int64_t hyq_net_scratch_bytes(int32_t nparts);
+int hyq_net_pack(const float* w, void* image, void* stream);
+int hyq_net_features(const double* M, int64_t n, void* X, void* stream);
+/* out: [6][n] FP32, the standardized extreme speeds of moments M (stride n) */
+int hyq_net_forward(const void* image, const double* M, int64_t n, float* out, int32_t* err, void* stream);
+int hyq_net_train_batch(const void* image, const void* X, const float* T, int64_t n, const int32_t* order, int32_t ntiles,
+                        float dscale, void* ds_scratch, float* partial, int32_t nparts, float* loss, int32_t* err, void* stream);
+int hyq_net_adam(float* w, float* m, float* v, const float* partial, int32_t nparts, float lr, float beta1, float beta2, float eps,
+                 float wd, int32_t step, float* gout, void* stream);
+/* Training targets of n cells (moments M, stride n): the plain path's
+ * extreme eigenvalues of the x, y and z flux Jacobians of the realized
+ * moments, standardized as the network outputs; T: n rows of 8 floats (NaN
+ * where a speed is not finite); Mr (may be NULL): the realized moments. */
+int hyq_cells_wavespeed_targets(const double* M, int64_t n, int32_t flag2D, double Ma, int32_t positivity, float* T, double* Mr,
+                                void* stream);
 
 /* Run up to max_steps steps of the reference loop, stopping on the device
  * once t >= tmax or nn >= nnmax.  Outputs may be NULL.  Returns
@@ -131,7 +216,10 @@ void hyq_batch_destroy(hyq_batch* b);
 int32_t hyq_batch_size(const hyq_batch* b);
 hyq_ctx* hyq_batch_member(hyq_batch* b, int32_t i);  /* NULL when out of range */
 void* hyq_batch_stream(hyq_batch* b);                /* cudaStream_t of the replays */
-/* Queue max_steps replays (after waiting for the members' own streams). */
+/* Queue max_steps replays (after waiting for the members' own streams).
+ * Each member's stream is then made to wait for the replays, so a later
+ * member call (hyq_get_state, hyq_stats_get, hyq_set_state) sees the state
+ * after them. */
 int hyq_batch_advance_async(hyq_batch* b, int64_t max_steps);
 /* Same, then wait; ndone / nfailed (may be NULL) count members that are done
  * and members that met a non-finite wave speed. */

@@ -103,6 +103,13 @@ int hyqo_num_threads(void) {
 #endif
 }
 
+// Threads of the OpenMP loops from now on (1: the serial step).
+void hyqo_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#endif
+}
+
 void hyqo_initialize_m4_35(double rho, double u, double v, double w, double C200, double C110, double C101, double C020,
                            double C011, double C002, double* out) {
   initialize_m4_35<double>(rho, u, v, w, C200, C110, C101, C020, C011, C002, out);

@@ -90,4 +90,16 @@ void sh_eig6_both(const double* A, double* out) {
   for (int i = 0; i < 36; ++i) h2[i] = A[i];
   out[24] = e6::pattern(h2);
 }
+// characteristic polynomial of a flux Jacobian (row-major 6 x 6 with the
+// unit rows of jacobian6): c[0..6]
+void sh_cp_charpoly(const double* A, double* c) {
+  double cc[7];
+  cp::charpoly(A + 12, A + 24, A + 30, cc);
+  for (int k = 0; k < 7; ++k) c[k] = cc[k];
+}
+// certified extremes: out = {ok, vmin, vmax, its}
+void sh_cp_extremes(const double* A, double lo_seed, double hi_seed, double margin, double* out) {
+  const cp::Extremes e = cp::extremes(A + 12, A + 24, A + 30, lo_seed, hi_seed, margin);
+  out[0] = e.ok ? 1.0 : 0.0; out[1] = e.vmin; out[2] = e.vmax; out[3] = e.its;
+}
 }

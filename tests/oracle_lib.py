@@ -34,6 +34,8 @@ def load():
         [ctypes.c_double] * 6 + [ctypes.c_int, _dp, _dp]
     lib.hyqo_delta2starchol_L3.restype = ctypes.c_double
     lib.hyqo_eig6.restype = ctypes.c_int
+    lib.hyqo_set_threads.argtypes = [ctypes.c_int]
+    lib.hyqo_set_threads.restype = None
     _lib = lib
     return lib
 

@@ -24,7 +24,7 @@ def test_library_exports_all_symbols():
     lib = _lib.load()
     for name in declared_symbols():
         assert hasattr(lib, name), name
-    assert lib.hyq_abi_version() == 1
+    assert lib.hyq_abi_version() == 2
 
 
 def test_missing_library_fails_loudly(tmp_path):
@@ -52,3 +52,26 @@ def test_create_rejects_grids_beyond_the_list_limit():
     assert "2^29" in lib.hyq_last_error(None).decode()
     p = ic.default_params(Nx=1, Ny=4, Nz=4)
     assert lib.hyq_create(ctypes.byref(params_struct(p)), ctypes.byref(h)) == -1
+
+
+@pytest.mark.skipif(not os.path.exists(_lib.LIB_PATH), reason="library not built")
+def test_create_rejects_unknown_mode():
+    """The eigenvalue-path mode is checked on the host before any CUDA call."""
+    import ctypes
+    from hyqmom.runner import params_struct
+    from hyqmom import ic
+    lib = _lib.load()
+    hp = params_struct(ic.default_params(Nx=8, Ny=8, Nz=8))
+    hp.mode = 7
+    h = ctypes.c_void_p()
+    assert lib.hyq_create(ctypes.byref(hp), ctypes.byref(h)) == -1
+    assert "mode" in lib.hyq_last_error(None).decode()
+
+
+def test_params_struct_layout_matches_header():
+    """hyq_params / hyq_stats: the ctypes layouts have the C struct sizes
+    (int32 x 6, int64, double x 11, int32 x 2; stats: double x 3, int64,
+    int32 x 2, int64 x 2)."""
+    import ctypes
+    assert ctypes.sizeof(_lib.HyqParams) == 6 * 4 + 8 + 11 * 8 + 2 * 4
+    assert ctypes.sizeof(_lib.HyqStats) == 3 * 8 + 8 + 2 * 4 + 2 * 8

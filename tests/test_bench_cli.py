@@ -36,6 +36,15 @@ def test_cpu_baseline_steps_each_given_slab():
     assert a.shape == (p["Nx"], p["Ny"], 2, 35) and a.flags["F_CONTIGUOUS"]
     base = bench.cpu_baseline(p, [(0, a), (7, b)])
     assert base["value"] > 0 and base["unit"] == bench.UNIT
-    assert "[0, 7]" in base["sample"]
-    # each slab was stepped once, in place
-    assert not np.array_equal(a, bench.slab_of(M, 2)) and np.array_equal(a, b)
+    assert "[0, 7]" in base["sample"] and "OpenMP" in base["sample"]
+    # each slab was stepped on a copy: the caller's states are unchanged
+    assert np.array_equal(a, bench.slab_of(M, 2)) and np.array_equal(a, b)
+    serial = bench.cpu_baseline(p, [(0, a)], threads=1)
+    assert serial["cores"] == 1 and "serial" in serial["sample"]
+
+
+def test_timed_steps_spread_over_the_run():
+    assert bench.timed_steps(500, 20) == list(range(25, 501, 25))
+    assert bench.timed_steps(500, 1) == [500]
+    assert bench.timed_steps(200, 3) == [67, 133, 200]
+    assert bench.timed_steps(10, 50) == list(range(1, 11))

@@ -1,0 +1,233 @@
+"""The learned wave-speed path on the GPU, through the C-ABI.
+
+* The tcgen05 network kernels against the host FP64 reference with the same
+  BF16 roundings: the inference kernel (features computed inline from the
+  moments) and the training kernel's gradients (the gradient check).
+* Training on the device lowers the loss.
+* The certified and learned steps from the same state agree with the oracle
+  (the reference's serial step restated on the CPU) to 1e-12 relative per
+  moment field, FP64 throughout; their fallback counters are reported.
+* The packaged trained network cuts the certified solve's polynomial
+  evaluations against bound starts and against an untrained network.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from hyqmom import _lib, ic, wavenet
+
+torch = pytest.importorskip("torch")
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(os.path.dirname(HERE), "hyqmom.jl_b200", "csrc")
+
+pytestmark = pytest.mark.gpu
+
+
+def need_gpu():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def decode_tiles(X, n):
+    """Host copy of the device input tiles: [n, 35] float (the BF16 values)."""
+    raw = X.cpu().numpy().reshape(-1, 128 * 128)
+    out = np.zeros((raw.shape[0] * 128, 64), dtype=np.float32)
+    for t in range(raw.shape[0]):
+        tile = raw[t]
+        for r in range(128):
+            for u in range(8):
+                off = r * 128 + ((u ^ (r & 7)) << 4)
+                v = tile[off:off + 16].view(np.uint16).astype(np.uint32) << 16
+                out[t * 128 + r, 8 * u:8 * u + 8] = v.view(np.float32)
+    return out[:n, :35]
+
+
+@pytest.fixture(scope="module")
+def states():
+    """Realized moments [35, n] (device) of a 24x24x12 crossing-jet run at
+    Ma=1, Kn=0.01 (plain path), steps 10..40."""
+    need_gpu()
+    S = wavenet.crossing_run_states(1.0, 0.01, grid=(24, 24, 12), steps=40, every=10)
+    M = torch.tensor(S, dtype=torch.float64, device="cuda")
+    T, Mr = wavenet.targets(M, Ma=1.0)
+    torch.cuda.synchronize()
+    return Mr, T
+
+
+def test_wavenet_forward_matches_host(states):
+    Mr, _ = states
+    n = 1000
+    M = Mr[:, :n].contiguous()
+    params = wavenet.init_params(7)
+    img = wavenet.pack(torch.tensor(params, device="cuda"))
+    y = wavenet.forward(img, M).cpu().numpy().T
+    S = decode_tiles(wavenet.features(M), n)
+    ref = wavenet.reference_forward(params, S, emulate=True)
+    err = np.abs(y - ref)
+    assert np.all(np.isfinite(y))
+    assert err.max() <= 5e-3 + 1e-2 * np.abs(ref).max(), err.max()
+
+
+def test_wavenet_gradients_match_host(states):
+    """The gradient check: hand-written tcgen05 forward + backward against the
+    host FP64 backward pass (same BF16 roundings), two tiles, the second
+    partly filled."""
+    Mr, _ = states
+    n = 200
+    M = Mr[:, :n].contiguous()
+    X = wavenet.features(M)
+    rng = np.random.default_rng(2)
+    T = torch.tensor(rng.normal(size=(n, 8)).astype(np.float32), device="cuda")
+    params = wavenet.init_params(11)
+    tr = wavenet.Trainer(params, nparts=2)
+    tiles = torch.tensor([0, 1], dtype=torch.int32, device="cuda")
+    g, sse = tr.gradients(X, T, n, tiles, rows=n)
+    g = g.cpu().numpy().astype(np.float64)
+    S = decode_tiles(X, n)
+    gref, sref = wavenet.reference_gradients(params, S, T.cpu().numpy()[:, :6].astype(np.float64), 2.0 / (n * 6), emulate=True)
+    assert abs(sse - sref) <= 1e-3 * sref
+    blocks = {"W1": (wavenet.P_W1, wavenet.P_B1), "b1": (wavenet.P_B1, wavenet.P_W2), "W2": (wavenet.P_W2, wavenet.P_B2),
+              "b2": (wavenet.P_B2, wavenet.P_W3), "W3": (wavenet.P_W3, wavenet.P_B3), "b3": (wavenet.P_B3, wavenet.P_W4),
+              "W4": (wavenet.P_W4, wavenet.P_B4), "b4": (wavenet.P_B4, wavenet.NPARAM)}
+    for name, (a, b) in blocks.items():
+        rel = np.linalg.norm(g[a:b] - gref[a:b]) / max(np.linalg.norm(gref[a:b]), 1e-30)
+        assert rel < 2e-2, (name, rel)
+
+
+def test_training_lowers_the_loss(states):
+    Mr, T = states
+    ok = torch.isfinite(T[:, :6]).all(dim=1)
+    Mr, T = Mr[:, ok].contiguous(), T[ok].contiguous()
+    n = T.shape[0]
+    X = wavenet.features(Mr)
+    ntiles = (n + 127) // 128
+    tr = wavenet.Trainer(wavenet.init_params(3), lr=2e-3)
+    all_tiles = torch.arange(ntiles, dtype=torch.int32, device="cuda")
+    _, sse0 = tr.gradients(X, T, n, all_tiles, rows=n)
+    rng = np.random.default_rng(0)
+    for step in range(300):
+        tiles = torch.tensor(rng.choice(ntiles, size=min(16, ntiles), replace=False).astype(np.int32), device="cuda")
+        tr.step(X, T, n, tiles, rows=int(tiles.numel()) * 128)
+    tr.check()
+    _, sse1 = tr.gradients(X, T, n, all_tiles, rows=n)
+    assert sse1 < 0.2 * sse0, (sse0, sse1)
+
+
+def field_rel(a, b):
+    a = np.asarray(a).reshape(-1, 35)
+    b = np.asarray(b).reshape(-1, 35)
+    scale = np.maximum(np.max(np.abs(b), axis=0), 1e-300)
+    return float(np.max(np.max(np.abs(a - b), axis=0) / scale))
+
+
+@pytest.mark.parametrize("mode", ["certified", "learned"])
+def test_step_from_same_state_matches_oracle(mode):
+    """One step of the certified / learned path from an evolved state against
+    the oracle step from the same state: <= 1e-12 relative per moment field
+    (FP64), and the same t within 1e-12."""
+    need_gpu()
+    from hyqmom.runner import Solver
+    if mode == "learned" and not os.path.exists(wavenet.WEIGHTS_PATH):
+        pytest.skip("no trained network packaged")
+    p = ic.with_jets(ic.default_params(Nx=20, Ny=20, Nz=20, Ma=1.0, Kn=0.01, CFL=0.5, tmax=10.0, nnmax=1000), "crossing")
+    M0 = ic.initial_state(p)
+    s = Solver(p)
+    s.set_state(M0)
+    s.advance(30)
+    M30, t30 = s.get_state(), s.stats()["t"]
+    s.close()
+    g = Solver(p, mode=mode)
+    try:
+        g.set_state(M30)
+        g.set_clock(t30, 30)
+        for k in range(3):
+            Mprev = g.get_state()
+            tprev = g.stats()["t"]
+            g.advance(1)
+            Mg, st = g.get_state(), g.stats()
+            Mo = np.asfortranarray(Mprev.copy())
+            _, to, _ = ol.step(Mo, dict(p, **ic.grid_spacing(p)), tprev)
+            assert field_rel(Mg, Mo) <= 1e-12, (k, field_rel(Mg, Mo))
+            assert abs(st["t"] - to) <= 1e-12 * to
+        assert st["stage_cells"] == 3 * 5 * 8000
+        print(f"{mode}: fallback {st['fallback_cells']} of {st['stage_cells']} stage cells")
+    finally:
+        g.close()
+
+
+def test_learned_run_tracks_plain_run():
+    """100 steps of the learned and certified paths against the plain path
+    (bit-identical to the oracle) on 20^3 crossing jets, Ma=1, Kn=0.01: the
+    field-relative difference after 100 steps, within the 1e-8 bar."""
+    need_gpu()
+    from hyqmom.runner import Solver
+    modes = ["certified"] + (["learned"] if os.path.exists(wavenet.WEIGHTS_PATH) else [])
+    p = ic.with_jets(ic.default_params(Nx=20, Ny=20, Nz=20, Ma=1.0, Kn=0.01, CFL=0.5, tmax=10.0, nnmax=100), "crossing")
+    M0 = ic.initial_state(p)
+    res = {}
+    for mode in ["plain"] + modes:
+        s = Solver(p, mode=mode)
+        try:
+            s.set_state(M0)
+            s.advance(100)
+            res[mode] = (s.get_state(), s.stats())
+        finally:
+            s.close()
+    Mp, sp = res["plain"]
+    assert sp["nn"] == 100
+    for mode in modes:
+        M, st = res[mode]
+        d = field_rel(M, Mp)
+        print(f"{mode}: 100-step field-relative difference vs plain {d:.3e}, t {st['t']:.17g} vs {sp['t']:.17g}, "
+              f"fallback {st['fallback_cells']}/{st['stage_cells']}")
+        assert st["nn"] == 100 and d <= 1e-8, (mode, d)
+
+
+def test_trained_network_cuts_evaluations(tmp_path):
+    """Seeds from the packaged network against bound starts and against an
+    untrained network, on the Jacobians of evolved states: the certified
+    solve (host build of the device code) spends fewer polynomial evaluations
+    with the trained seeds."""
+    need_gpu()
+    if not os.path.exists(wavenet.WEIGHTS_PATH):
+        pytest.skip("no trained network packaged")
+    out = tmp_path / "libshim.so"
+    subprocess.check_call(["/usr/bin/g++", "-O2", "-std=c++17", "-fno-fast-math", "-ffp-contract=off", "-fPIC", "-shared", "-I", CSRC,
+                           "-o", str(out), os.path.join(HERE, "host_device_shim.cpp")])
+    shim = ctypes.CDLL(str(out))
+    S = wavenet.crossing_run_states(1.0, 0.01, grid=(24, 24, 12), steps=60, every=20)
+    M = torch.tensor(S, dtype=torch.float64, device="cuda")
+    _, Mr = wavenet.targets(M, Ma=1.0)
+    net = wavenet.load_default()
+    preds = {}
+    for name, params in (("trained", net.params), ("untrained", wavenet.init_params(0))):
+        img = wavenet.pack(torch.tensor(params, device="cuda"))
+        preds[name] = wavenet.forward(img, Mr).cpu().numpy()
+    Mh = Mr.cpu().numpy()
+    lib = ol.load()
+    dp = ctypes.POINTER(ctypes.c_double)
+    rng = np.random.default_rng(0)
+    evals = {"bound": [], "trained": [], "untrained": []}
+    for c in rng.choice(Mh.shape[1], 400, replace=False):
+        m = Mh[:, c]
+        u, sd = m[1] / m[0], np.sqrt(m[2] / m[0] - (m[1] / m[0]) ** 2)
+        a = np.ascontiguousarray(m[[0, 5, 9, 12, 14, 1, 6, 10, 13, 2, 7, 11, 3, 8, 4]])
+        J = np.zeros(36)
+        lib.hyqo_jacobian6(a.ctypes.data_as(dp), J.ctypes.data_as(dp))
+        res = {}
+        for name, lo, hi, mg in (("bound", np.nan, np.nan, 0.0),
+                                 ("trained", u + sd * preds["trained"][0, c], u + sd * preds["trained"][1, c], net.margin),
+                                 ("untrained", u + sd * preds["untrained"][0, c], u + sd * preds["untrained"][1, c], net.margin)):
+            o = np.zeros(4)
+            shim.sh_cp_extremes(J.ctypes.data_as(dp), ctypes.c_double(lo), ctypes.c_double(hi), ctypes.c_double(mg), o.ctypes.data_as(dp))
+            res[name] = o
+        if res["bound"][0]:
+            for k in evals:
+                evals[k].append(res[k][3])
+    mean = {k: float(np.mean(v)) for k, v in evals.items()}
+    print("mean polynomial evaluations per certified Jacobian:", mean)
+    assert mean["trained"] < 0.9 * mean["bound"] and mean["trained"] < mean["untrained"], mean
