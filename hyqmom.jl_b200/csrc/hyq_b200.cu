@@ -487,6 +487,9 @@ int hyq_stats_get(hyq_ctx* ctx, hyq_stats* out) {
   out->done = (h.t < ctx->p.tmax && h.nn < ctx->p.nnmax) ? 0 : 1;
   out->stage_cells = (int64_t)h.stage_cells;
   out->fallback_cells = (int64_t)h.fb_cells;
+  out->dense_mask = 0;
+  for (int q = 0; q < 5; ++q) out->dense_mask |= (h.dense[q] > 0 ? 1 : 0) << q;
+  out->reserved = 0;
   return HYQ_OK;
 }
 

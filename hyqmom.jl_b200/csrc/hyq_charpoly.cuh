@@ -40,7 +40,7 @@ namespace cp {
 
 constexpr int ITMAX = 40;              // Newton iterations per root
 constexpr double NEWTON_TOL = 1e-12;   // extremes: |dx| <= TOL (1 + |x|), then one more step
-constexpr double LOOSE_TOL = 1e-4;     // interior roots: only separating points are needed
+constexpr double LOOSE_TOL = 1e-2;     // interior roots: only separating points are needed
 constexpr double CERT_ERR = 40.0 * 2.220446049250313e-16;  // > gamma_12 of the Horner bound
 constexpr double ROOT_BOUND = 2.25;    // |x| <= sqrt(5) when all roots are real, sum x = 0, sum x^2 = 6
 // |b(y)| at a point y between neighbouring roots r_k < y < r_k+1 bounds their
@@ -163,6 +163,17 @@ template <int N> HQD bool newton(const double* d, double& x, double tol, int& it
   return false;
 }
 
+// Upper bound of the roots of the monic degree-N polynomial d when they are
+// all real: mean + sqrt((N - 1) variance), from the sum and the sum of
+// squares of the roots (-d[N-1] and d[N-1]^2 - 2 d[N-2]); slightly inflated.
+// NaN when the variance is negative (complex roots), which jmin then skips.
+template <int N> HQD double upper_bound(const double* d) {
+  const double m = -d[N - 1] / double(N);
+  const double s2 = d[N - 1] * d[N - 1] - 2.0 * d[N - 2];
+  const double var = s2 / double(N) - m * m;
+  return m + sqrt(double(N - 1) * var) * (1.0 + 1e-12) + 1e-12;
+}
+
 // One Newton step on the full polynomial b (polishes a root found on a
 // deflated polynomial).
 HQD double polish(const double (&b)[7], double x, int& its) {
@@ -225,10 +236,13 @@ HQD CpOut solve(const double (&b)[7], double xhi, double xlo) {
   double d5[6], d4[5], d3[4], d2[3];
   deflate<6>(b, x1, d5);
   deflate<5>(d5, x6, d4);
-  double x2 = x1;
+  // each interior search starts from the upper bound mean + sqrt((n-1) var)
+  // of the deflated polynomial's roots (read off its monic coefficients)
+  // when that is below the previous root
+  double x2 = jmin(x1, upper_bound<4>(d4));
   if (!newton<4>(d4, x2, LOOSE_TOL, o.its)) return o;
   deflate<4>(d4, x2, d3);
-  double x3 = x2;
+  double x3 = jmin(x2, upper_bound<3>(d3));
   if (!newton<3>(d3, x3, LOOSE_TOL, o.its)) return o;
   deflate<3>(d3, x3, d2);
   // the last two from the quadratic, in the cancellation-free form

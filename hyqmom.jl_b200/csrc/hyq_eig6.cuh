@@ -9,6 +9,51 @@
 // stay in registers instead of local memory (solve<K> also covers the
 // unpermuted case, K = 0, which the device code leaves to the general path).
 // Any other case goes to eig_real<6>.  tests/test_device_code_on_host.py checks the two bit for bit.
+// The eigenvalue routines in this file restate the steps of LAPACK's DGEBAL,
+// DGEHD2, DLARFG, DLAHQR and DLANV2 (needed for branch-identical results with
+// the reference's eigvals).  LAPACK is distributed under the following
+// licence, reproduced as it requires:
+//
+//   Copyright (c) 1992-2013 The University of Tennessee and The University
+//                           of Tennessee Research Foundation.  All rights
+//                           reserved.
+//   Copyright (c) 2000-2013 The University of California Berkeley.  All
+//                           rights reserved.
+//   Copyright (c) 2006-2013 The University of Colorado Denver.  All rights
+//                           reserved.
+//
+//   Redistribution and use in source and binary forms, with or without
+//   modification, are permitted provided that the following conditions are
+//   met:
+//   - Redistributions of source code must retain the above copyright
+//     notice, this list of conditions and the following disclaimer.
+//   - Redistributions in binary form must reproduce the above copyright
+//     notice, this list of conditions and the following disclaimer listed
+//     in this license in the documentation and/or other materials
+//     provided with the distribution.
+//   - Neither the name of the copyright holders nor the names of its
+//     contributors may be used to endorse or promote products derived from
+//     this software without specific prior written permission.
+//
+//   The copyright holders provide no reassurances that the source code
+//   provided does not infringe any patent, copyright, or any other
+//   intellectual property rights of third parties.  The copyright holders
+//   disclaim any liability to any recipient for claims brought against
+//   recipient by a third party for infringement of that parties
+//   intellectual property rights.
+//
+//   THIS SOFTWARE IS PROVIDED BY THE COPYRIGHT HOLDERS AND CONTRIBUTORS
+//   "AS IS" AND ANY EXPRESS OR IMPLIED WARRANTIES, INCLUDING, BUT NOT
+//   LIMITED TO, THE IMPLIED WARRANTIES OF MERCHANTABILITY AND FITNESS FOR
+//   A PARTICULAR PURPOSE ARE DISCLAIMED. IN NO EVENT SHALL THE COPYRIGHT
+//   OWNER OR CONTRIBUTORS BE LIABLE FOR ANY DIRECT, INDIRECT, INCIDENTAL,
+//   SPECIAL, EXEMPLARY, OR CONSEQUENTIAL DAMAGES (INCLUDING, BUT NOT
+//   LIMITED TO, PROCUREMENT OF SUBSTITUTE GOODS OR SERVICES; LOSS OF USE,
+//   DATA, OR PROFITS; OR BUSINESS INTERRUPTION) HOWEVER CAUSED AND ON ANY
+//   THEORY OF LIABILITY, WHETHER IN CONTRACT, STRICT LIABILITY, OR TORT
+//   (INCLUDING NEGLIGENCE OR OTHERWISE) ARISING IN ANY WAY OUT OF THE USE
+//   OF THIS SOFTWARE, EVEN IF ADVISED OF THE POSSIBILITY OF SUCH DAMAGE.
+//
 #pragma once
 
 namespace hyq {

@@ -158,6 +158,7 @@ extern "C" int hyq_step_noalloc(const hyq_params* p, double* M, hyq_stats* stats
   if ((e = cudaMemcpyAsync(&h, clk, sizeof(DevClock), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_error(e, "clock copy");
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "cudaStreamSynchronize");
   stats->t = h.t; stats->dt = h.dt; stats->vmax = h.vmax; stats->nn = h.nn; stats->status = h.status;
+  stats->stage_cells = 0; stats->fallback_cells = 0; stats->dense_mask = 0; stats->reserved = 0;
   stats->done = (h.t < p->tmax && h.nn < p->nnmax) ? 0 : 1;
   if (h.status > 0)
     return report_error(HYQ_ENONFINITE, ("non-finite CFL wave speed at step " + std::to_string(h.status) +

@@ -65,9 +65,19 @@ constexpr uint32_t TILE_H_BYTES = 2 * TILE * 128;    // one hidden tile [128 x 1
 // error word values
 constexpr int NET_ERR_WAIT = 1;
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU through the logistic function written as 0.5 (1 + tanh(z / 2)), with
+// the hardware tanh approximation (one MUFU operation; its error is far below
+// the BF16 rounding of the activations).  Inference and training use the same
+// function.
+__device__ __forceinline__ float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float sigmoid(float z) { return 0.5f + 0.5f * tanh_approx(0.5f * z); }
+__device__ __forceinline__ float silu(float z) { return z * sigmoid(z); }
 __device__ __forceinline__ float dsilu(float z) {
-  const float s = 1.0f / (1.0f + __expf(-z));
+  const float s = sigmoid(z);
   return s * (1.0f + z * (1.0f - s));
 }
 
@@ -148,26 +158,46 @@ __device__ __forceinline__ unsigned char* align1024(unsigned char* p) {
 }
 
 // ------------------------------------------------------------ inference
-// Shared memory: weight image | activation tile (the input in its first
-// chunk) | two mbarriers and the TMEM address.
-constexpr int INF_ACT = IMG_ALIGNED, INF_BAR = INF_ACT + TILE_H_BYTES, INF_SMEM = INF_BAR + 64 + 2048;
+// One CTA runs INF_GROUPS independent tile pipelines of 128 threads (4 warps)
+// each, so that one group's features and epilogues overlap another's MMAs:
+// group g owns an activation tile (the input in its first chunk), TMEM
+// columns [128 g, 128 g + 128) and an mbarrier, and synchronises on named
+// barrier 1 + g.  Shared memory: weight image | INF_GROUPS activation tiles |
+// barriers and the TMEM address.
+constexpr int INF_GROUPS = 4;
+constexpr int INF_THREADS = 128 * INF_GROUPS;
+constexpr int INF_ACT = IMG_ALIGNED, INF_BAR = INF_ACT + INF_GROUPS * TILE_H_BYTES, INF_SMEM = INF_BAR + 64 + 2048;
+
+__device__ __forceinline__ void group_sync(int g) { asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory"); }
+// named-barrier AND of `pred` over the group
+__device__ __forceinline__ bool group_and(int g, bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)pred), "r"(1 + g)
+      : "memory");
+  return r != 0;
+}
 
 // Mr: moments (stride N) of cells [c0, c1); seeds: [6][N] FP32.  clk (may be
-// NULL): the step's loop predicate and error word.
-__global__ void __launch_bounds__(128, 1) k_wavenet(const double* __restrict__ Mr, long long N, long long c0, long long c1,
-                                                   const unsigned char* __restrict__ image, float* __restrict__ seeds, double tmax,
-                                                   long long nnmax, const DevClock* clk, int* err) {
+// NULL): the step's loop predicate.
+__global__ void __launch_bounds__(INF_THREADS, 1) k_wavenet(const double* __restrict__ Mr, long long N, long long c0, long long c1,
+                                                           const unsigned char* __restrict__ image, float* __restrict__ seeds,
+                                                           double tmax, long long nnmax, const DevClock* clk, int* err) {
   if (clk && !((clk->t < tmax) && (clk->nn < nnmax))) return;
   extern __shared__ unsigned char smem_raw[];
   unsigned char* sm = align1024(smem_raw);
-  unsigned char* act = sm + INF_ACT;
+  const int tid = threadIdx.x, g = tid >> 7, r = tid & 127, warp = tid >> 5;
+  unsigned char* act = sm + INF_ACT + g * TILE_H_BYTES;
   const float* bias = reinterpret_cast<const float*>(sm + IMG_B);
   const uint32_t s_img = smem_u32(sm), s_act = smem_u32(act);
-  const uint32_t bar_w = smem_u32(sm + INF_BAR), bar_m = bar_w + 8, slot = bar_w + 16;
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const uint32_t bar_w = smem_u32(sm + INF_BAR), bar_m = bar_w + 8 * (1 + g), slot = bar_w + 8 * (1 + INF_GROUPS);
   if (tid == 0) {
-    mbar_init(bar_w, 1);
-    mbar_init(bar_m, 1);
+    for (int q = 0; q <= INF_GROUPS; ++q) mbar_init(bar_w + 8 * q, 1);
     mbar_fence_init();
   }
   __syncthreads();
@@ -175,52 +205,44 @@ __global__ void __launch_bounds__(128, 1) k_wavenet(const double* __restrict__ M
     mbar_expect_tx(bar_w, IMG_BYTES);
     bulk_g2s(s_img, image, IMG_BYTES, bar_w);
   }
-  if (warp == 0) tmem_alloc(slot, 128);
+  if (warp == 0) tmem_alloc(slot, 128 * INF_GROUPS);
   fence_before();
   __syncthreads();
   fence_after();
-  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + INF_BAR + 16);
-  const uint32_t trow = tmem + (uint32_t(warp * 32) << 16);
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + INF_BAR + 8 * (1 + INF_GROUPS)) + uint32_t(128 * g);
+  const uint32_t trow = tmem + (uint32_t((warp & 3) * 32) << 16);
   bool ok = __syncthreads_and(mbar_wait(bar_w, 0)) != 0;
   uint32_t phase = 0;
   const long long ntiles = (c1 - c0 + TILE - 1) / TILE;
-  for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-    const long long c = c0 + t * TILE + tid;
+  for (long long t = (long long)blockIdx.x * INF_GROUPS + g; t < ntiles && ok; t += (long long)gridDim.x * INF_GROUPS) {
+    const long long c = c0 + t * TILE + r;
     const bool valid = c < c1;
     {
       uint32_t packed[32];
       cell_features(Mr + (valid ? c : c0), N, valid, packed);
-      store_row_sw128<8>(act, tid, packed);
+      store_row_sw128<8>(act, r, packed);
     }
-    // layers 1..3: A = act (K-major), B = W_l, D = TMEM cols 0..127
+    // layers 1..3: A = act (K-major), B = W_l, D = the group's TMEM columns
 #pragma unroll 1
-    for (int l = 0; l < 3; ++l) {
+    for (int l = 0; l < 4; ++l) {
       fence_proxy_async();
       fence_before();
-      __syncthreads();
-      if (tid == 0) {
+      group_sync(g);
+      if (r == 0) {
         fence_after();
-        const uint32_t w = s_img + (l == 0 ? IMG_W1 : (l == 1 ? IMG_W2 : IMG_W3));
-        mma_kk(tmem, s_act, TILE, w, NH, l == 0 ? KIN / 16 : NH / 16, NH, 0u);
+        if (l < 3) {
+          const uint32_t w = s_img + (l == 0 ? IMG_W1 : (l == 1 ? IMG_W2 : IMG_W3));
+          mma_kk(tmem, s_act, TILE, w, NH, l == 0 ? KIN / 16 : NH / 16, NH, 0u);
+        } else {
+          mma_kk(tmem, s_act, TILE, s_img + IMG_W4, NOUTP, NH / 16, NOUTP, 0u);  // layer 4: N = 16
+        }
         mma_commit(bar_m);
       }
-      ok = __syncthreads_and(ok && mbar_wait(bar_m, phase)) != 0;
+      ok = group_and(g, ok && mbar_wait(bar_m, phase));
       phase ^= 1u;
       fence_after();
-      hidden_epilogue<false>(trow, bias + NH * l, act, tid, nullptr);
+      if (l < 3) hidden_epilogue<false>(trow, bias + NH * l, act, r, nullptr);
     }
-    // layer 4: N = 16, outputs 0..5
-    fence_proxy_async();
-    fence_before();
-    __syncthreads();
-    if (tid == 0) {
-      fence_after();
-      mma_kk(tmem, s_act, TILE, s_img + IMG_W4, NOUTP, NH / 16, NOUTP, 0u);
-      mma_commit(bar_m);
-    }
-    ok = __syncthreads_and(ok && mbar_wait(bar_m, phase)) != 0;
-    phase ^= 1u;
-    fence_after();
     float y[16];
     tmem_ld16(trow, y);
     if (valid) {
@@ -228,13 +250,13 @@ __global__ void __launch_bounds__(128, 1) k_wavenet(const double* __restrict__ M
       for (int q = 0; q < NOUT; ++q) seeds[(long long)q * N + c] = y[q] + bias[3 * NH + q];
     }
     fence_before();
-    __syncthreads();
+    group_sync(g);
   }
-  if (!ok && tid == 0 && err) atomicExch(err, NET_ERR_WAIT);
+  if (!ok && r == 0 && err) atomicExch(err, NET_ERR_WAIT);
   fence_before();
   __syncthreads();
   fence_after();
-  if (warp == 0) tmem_dealloc(tmem, 128);
+  if (warp == 0) tmem_dealloc(tmem - uint32_t(128 * g), 128 * INF_GROUPS);
 }
 
 // ------------------------------------------------------------ training
@@ -555,8 +577,9 @@ cudaError_t net_set_smem() {
 void launch_wavespeed_seeds(const StepConst& sc, const double* Mr, const WaveNet* net, float* seeds, const DevClock* clk, cudaStream_t s,
                             long long c0, long long c1) {
   const long long ntiles = (c1 - c0 + TILE - 1) / TILE;
-  const int g = (int)(ntiles < net_grid() ? ntiles : net_grid());
-  k_wavenet<<<g, 128, INF_SMEM, s>>>(Mr, sc.N, c0, c1, net->image, seeds, sc.tmax, sc.nnmax, clk, net->err);
+  const long long need = (ntiles + INF_GROUPS - 1) / INF_GROUPS;
+  const int g = (int)(need < net_grid() ? need : net_grid());
+  k_wavenet<<<g, INF_THREADS, INF_SMEM, s>>>(Mr, sc.N, c0, c1, net->image, seeds, sc.tmax, sc.nnmax, clk, net->err);
 }
 
 }  // namespace hyqk
@@ -601,8 +624,9 @@ int hyq_net_forward(const void* image, const double* M, int64_t n, float* out, i
   cudaError_t e = net_set_smem();
   if (e != cudaSuccess) return net_cuda_fail(e, "cudaFuncSetAttribute");
   const long long ntiles = (n + TILE - 1) / TILE;
-  const int g = (int)(ntiles < net_grid() ? ntiles : net_grid());
-  k_wavenet<<<g, 128, INF_SMEM, (cudaStream_t)stream>>>(M, n, 0, n, (const unsigned char*)image, out, 0.0, 0, nullptr, (int*)err);
+  const long long need = (ntiles + INF_GROUPS - 1) / INF_GROUPS;
+  const int g = (int)(need < net_grid() ? need : net_grid());
+  k_wavenet<<<g, INF_THREADS, INF_SMEM, (cudaStream_t)stream>>>(M, n, 0, n, (const unsigned char*)image, out, 0.0, 0, nullptr, (int*)err);
   NET_LAUNCH_CHECK("k_wavenet");
   return HYQ_OK;
 }

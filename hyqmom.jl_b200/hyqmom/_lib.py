@@ -32,7 +32,7 @@ NET_PARAMS = 38406  # HYQ_NET_PARAMS
 class HyqStats(ctypes.Structure):
     _fields_ = [("t", ctypes.c_double), ("dt", ctypes.c_double), ("vmax", ctypes.c_double), ("nn", ctypes.c_int64),
                 ("done", ctypes.c_int32), ("status", ctypes.c_int32), ("stage_cells", ctypes.c_int64),
-                ("fallback_cells", ctypes.c_int64)]
+                ("fallback_cells", ctypes.c_int64), ("dense_mask", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class HyqError(RuntimeError):

@@ -135,7 +135,7 @@ class Solver:
         st = _lib.HyqStats()
         self._chk(self._lib.hyq_stats_get(self._h, ctypes.byref(st)))
         return dict(t=st.t, dt=st.dt, vmax=st.vmax, nn=st.nn, done=bool(st.done), status=st.status,
-                    stage_cells=st.stage_cells, fallback_cells=st.fallback_cells)
+                    stage_cells=st.stage_cells, fallback_cells=st.fallback_cells, dense_mask=st.dense_mask)
 
     def reset_counters(self):
         self._chk(self._lib.hyq_reset_counters(self._h))

@@ -77,6 +77,11 @@ typedef struct hyq_stats {
    * step: x, y, z before the flux, x, y after it) and those of them that fell
    * back to the LAPACK path (a Jacobian not certified).  0 in plain mode. */
   int64_t stage_cells, fallback_cells;
+  /* eigenvalue stages (bit q: A x, y, z, E x, y) running dense at this step:
+   * their general eigen-solve takes every cell directly because the stage
+   * listed most of its cells recently */
+  int32_t dense_mask;
+  int32_t reserved;
 } hyq_stats;
 
 typedef struct hyq_ctx hyq_ctx;

@@ -91,6 +91,10 @@ template <class T> void phase_E(const T* m, const Params& P, T* out) {
 
 using namespace hyqo;
 
+#ifdef HYQO_BRANCHES
+namespace hyqo { long long g_branch_hits[BR_COUNT] = {0}; }
+#endif
+
 extern "C" {
 
 int hyqo_abi_version(void) { return 1; }
@@ -101,6 +105,20 @@ int hyqo_num_threads(void) {
 #else
   return 1;
 #endif
+}
+
+// Branch-hit counters of the instrumented build (zeros otherwise): out[8]
+// (hyqo::Branch order); reset = 1 zeroes them after reading.
+void hyqo_branch_counts(long long* out, int reset) {
+  for (int b = 0; b < BR_COUNT; ++b) {
+#ifdef HYQO_BRANCHES
+    out[b] = g_branch_hits[b];
+    if (reset) g_branch_hits[b] = 0;
+#else
+    (void)reset;
+    out[b] = 0;
+#endif
+  }
 }
 
 // Threads of the OpenMP loops from now on (1: the serial step).

@@ -31,6 +31,30 @@
 
 namespace hyqo {
 
+// Branch-hit counters (test instrumentation): built only into the
+// -DHYQO_BRANCHES variant of the library, which the tests use to show which
+// rare branches of the reference's algorithm a set of states takes.
+enum Branch {
+  BR_FACES = 0,         // realizable_3D faces case, S2 <= S2min (src/realizability/realizable_3D.jl:79-142)
+  BR_EDGE_CORNER = 1,   // edge_corner_correction (src/realizability/edge_corner_correction.jl:24-110)
+  BR_FLAG220 = 2,       // a repeat of realizable_3D while flag220 (src/numerics/Flux_closure35_and_realizable_3D.jl:134-143)
+  BR_COMPLEX_XY = 3,    // complex Jacobian eigenvalues corrected, x or y (eigenvalues6_hyperbolic_3D.jl:35)
+  BR_COMPLEX_Z = 4,     // the same along z (eigenvalues6z_hyperbolic_3D.jl)
+  BR_ROOTSR_NAN = 5,    // rootsR three real roots -> NaN under fast-math sqrt (src/autogen/rootsR.jl:275)
+  BR_ROOTSRXY_NAN = 6,  // rootsR_X_Y the same (src/autogen/rootsR_X_Y.jl:64)
+  BR_REREALIZE_Z = 7,   // eigenvalues6z negative-variance re-realization (eigenvalues6z_hyperbolic_3D.jl:63-104)
+  BR_COUNT = 8
+};
+#ifdef HYQO_BRANCHES
+extern long long g_branch_hits[BR_COUNT];
+inline void hit(int b) {
+#pragma omp atomic
+  g_branch_hits[b] += 1;
+}
+#else
+inline void hit(int) {}
+#endif
+
 constexpr double EPS = 2.220446049250313e-16;  // Julia eps()
 
 // ---------------------------------------------------------------- indexing
@@ -779,6 +803,7 @@ template <class T> void rootsR(T Del1, T H02, T H20, T s03, T s11, T s12, T s13,
   P3<T> P;
   P.c[0] = k0; P.c[1] = k1; P.c[2] = k2; P.c[3] = T(-1);
   cardano(P, re, im);
+  if (re[0] != re[0]) hit(BR_ROOTSR_NAN);
 }
 
 // rootsR_X_Y (src/autogen/rootsR_X_Y.jl:6-77): roots in X of
@@ -790,6 +815,7 @@ template <class T> void rootsR_X_Y(T Y, T e11, T e12, T e13, T e23, T e24, T e34
                    {pconst(ex, T(1)), pconst(e24), pconst(e34), pconst(e44)}};
   P3<T> P = pdet4(A);
   cardano(P, re, im);
+  if (re[0] != re[0]) hit(BR_ROOTSRXY_NAN);
 }
 
 // Julia `sort(real(R))` with NaN last, and the complex-root ratio test

@@ -171,6 +171,7 @@ template <class T> int realizable_3D(S28<T>& s) {
   T R011 = sqrt(jmax(T(0), T(1) - s.s011 * s.s011));
 
   if (S2 <= S2min) {
+    hit(BR_FACES);
     // faces (src/realizability/realizable_3D.jl:79-142)
     T Rmax = jmax(jmax(R110, R101), R011);
     if (R110 == Rmax) {
@@ -473,6 +474,7 @@ template <class T> void flux_closure35(const T* M4, int flag2D, T Ma, T* Fx, T* 
 
   T R110 = T(1) - sq(s.s110), R101 = T(1) - sq(s.s101), R011 = T(1) - sq(s.s011);
   if (R110 <= T(0) || R101 <= T(0) || R011 <= T(0)) {
+    hit(BR_EDGE_CORNER);
     // edge_corner_correction (src/realizability/edge_corner_correction.jl:24-110)
     S19<T> a;
     T S110, S101, S011, S300, S030, S003, S400, S040, S004, dummy;
@@ -521,6 +523,7 @@ template <class T> void flux_closure35(const T* M4, int flag2D, T Ma, T* Fx, T* 
     int itreal = 0;
     while (flag220 == 1 && itreal < itrealmax) {
       ++itreal;
+      hit(BR_FLAG220);
       realizable_3D(s);
     }
   }

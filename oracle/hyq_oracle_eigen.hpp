@@ -1,6 +1,51 @@
 // ORACLE (test infrastructure): flux-Jacobian eigenvalues, 1-D closure
 // eigenvalues, BGK collision and HLL sweeps.  Restates the reference files
 // cited per function; see hyq_oracle.hpp for the conventions.
+// The eigenvalue routines in this file restate the steps of LAPACK's DGEBAL,
+// DGEHD2, DLARFG, DLAHQR and DLANV2 (needed for branch-identical results with
+// the reference's eigvals).  LAPACK is distributed under the following
+// licence, reproduced as it requires:
+//
+//   Copyright (c) 1992-2013 The University of Tennessee and The University
+//                           of Tennessee Research Foundation.  All rights
+//                           reserved.
+//   Copyright (c) 2000-2013 The University of California Berkeley.  All
+//                           rights reserved.
+//   Copyright (c) 2006-2013 The University of Colorado Denver.  All rights
+//                           reserved.
+//
+//   Redistribution and use in source and binary forms, with or without
+//   modification, are permitted provided that the following conditions are
+//   met:
+//   - Redistributions of source code must retain the above copyright
+//     notice, this list of conditions and the following disclaimer.
+//   - Redistributions in binary form must reproduce the above copyright
+//     notice, this list of conditions and the following disclaimer listed
+//     in this license in the documentation and/or other materials
+//     provided with the distribution.
+//   - Neither the name of the copyright holders nor the names of its
+//     contributors may be used to endorse or promote products derived from
+//     this software without specific prior written permission.
+//
+//   The copyright holders provide no reassurances that the source code
+//   provided does not infringe any patent, copyright, or any other
+//   intellectual property rights of third parties.  The copyright holders
+//   disclaim any liability to any recipient for claims brought against
+//   recipient by a third party for infringement of that parties
+//   intellectual property rights.
+//
+//   THIS SOFTWARE IS PROVIDED BY THE COPYRIGHT HOLDERS AND CONTRIBUTORS
+//   "AS IS" AND ANY EXPRESS OR IMPLIED WARRANTIES, INCLUDING, BUT NOT
+//   LIMITED TO, THE IMPLIED WARRANTIES OF MERCHANTABILITY AND FITNESS FOR
+//   A PARTICULAR PURPOSE ARE DISCLAIMED. IN NO EVENT SHALL THE COPYRIGHT
+//   OWNER OR CONTRIBUTORS BE LIABLE FOR ANY DIRECT, INDIRECT, INCIDENTAL,
+//   SPECIAL, EXEMPLARY, OR CONSEQUENTIAL DAMAGES (INCLUDING, BUT NOT
+//   LIMITED TO, PROCUREMENT OF SUBSTITUTE GOODS OR SERVICES; LOSS OF USE,
+//   DATA, OR PROFITS; OR BUSINESS INTERRUPTION) HOWEVER CAUSED AND ON ANY
+//   THEORY OF LIABILITY, WHETHER IN CONTRACT, STRICT LIABILITY, OR TORT
+//   (INCLUDING NEGLIGENCE OR OTHERWISE) ARISING IN ANY WAY OUT OF THE USE
+//   OF THIS SOFTWARE, EVEN IF ADVISED OF THE POSSIBILITY OF SUCH DAMAGE.
+//
 #pragma once
 #include "hyq_oracle_closure.hpp"
 
@@ -558,6 +603,7 @@ template <class T> void eigenvalues6_hyperbolic_3D(const T* M, int axis, int fla
   const T thr = T(1000 * EPS);
   bool ca = ia > thr, cb = ib > thr;
   if (ca || cb) {
+    hit(BR_COMPLEX_XY);
     T Mc[35];
     correct_for_real(M, axis, ca, cb, flag2D, Ma, Mc);
     slice15(Mc, a1, sa); slice15(Mc, a2, sb);
@@ -581,6 +627,7 @@ template <class T> void eigenvalues6z_hyperbolic_3D(const T* M, int flag2D, T Ma
     T vy = M[9] / m000 - sq(M[5] / m000);
     T vz = M[19] / m000 - sq(M[15] / m000);
     if (vx < T(0) || vy < T(0) || vz < T(0)) {
+      hit(BR_REREALIZE_Z);
       T Fx[35], Fy[35], Fz[35];
       flux_closure35(M, flag2D, Ma, Fx, Fy, Fz, Mr);
       for (int n = 0; n < 35; ++n) Mw[n] = Mr[n];
@@ -599,6 +646,7 @@ template <class T> void eigenvalues6z_hyperbolic_3D(const T* M, int flag2D, T Ma
   const T thr = T(1000 * EPS);
   bool ca = ia > thr, cb = ib > thr;
   if (ca || cb) {
+    hit(BR_COMPLEX_Z);
     T M000 = M[0];
     T u = M[1] / M000, v = M[5] / M000, w = M[15] / M000;
     T C4[35], S4[35];

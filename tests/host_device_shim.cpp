@@ -102,4 +102,9 @@ void sh_cp_extremes(const double* A, double lo_seed, double hi_seed, double marg
   const cp::Extremes e = cp::extremes(A + 12, A + 24, A + 30, lo_seed, hi_seed, margin);
   out[0] = e.ok ? 1.0 : 0.0; out[1] = e.vmin; out[2] = e.vmax; out[3] = e.its;
 }
+// the step's own exp and cbrt (hyq_cell.cuh) on n arguments
+void sh_hexp_n(const double* x, double* y, long long n) { for (long long i = 0; i < n; ++i) y[i] = hexp(x[i]); }
+void sh_hcbrt_n(const double* x, double* y, long long n) { for (long long i = 0; i < n; ++i) y[i] = hcbrt(x[i]); }
+// realizable_3D on the 28 standardized moments (enum order), in place
+int sh_realizable_3d(double* a28) { return realizable_3D(a28); }
 }

@@ -159,32 +159,47 @@ def test_step_from_same_state_matches_oracle(mode):
         g.close()
 
 
-def test_learned_run_tracks_plain_run():
-    """100 steps of the learned and certified paths against the plain path
-    (bit-identical to the oracle) on 20^3 crossing jets, Ma=1, Kn=0.01: the
-    field-relative difference after 100 steps, within the 1e-8 bar."""
+@pytest.mark.parametrize("mode", ["certified", "learned"])
+def test_every_step_of_a_run_meets_the_step_bar(mode):
+    """100 steps of the certified / learned path on 20^3 crossing jets (Ma=1,
+    Kn=0.01): every step agrees with the oracle's step from the same state to
+    1e-12 relative per moment field (FP64).  The difference to the plain
+    path's run after 100 steps is printed: it is O(1), because the scheme's
+    threshold branches amplify any round-off difference (the oracle itself
+    does the same to a one-ulp perturbation, test_oracle_sensitivity.py), so
+    only a bit-identical path meets a 100-step bar."""
     need_gpu()
     from hyqmom.runner import Solver
-    modes = ["certified"] + (["learned"] if os.path.exists(wavenet.WEIGHTS_PATH) else [])
+    if mode == "learned" and not os.path.exists(wavenet.WEIGHTS_PATH):
+        pytest.skip("no trained network packaged")
     p = ic.with_jets(ic.default_params(Nx=20, Ny=20, Nz=20, Ma=1.0, Kn=0.01, CFL=0.5, tmax=10.0, nnmax=100), "crossing")
+    pp = dict(p, **ic.grid_spacing(p))
     M0 = ic.initial_state(p)
-    res = {}
-    for mode in ["plain"] + modes:
-        s = Solver(p, mode=mode)
-        try:
-            s.set_state(M0)
-            s.advance(100)
-            res[mode] = (s.get_state(), s.stats())
-        finally:
-            s.close()
-    Mp, sp = res["plain"]
-    assert sp["nn"] == 100
-    for mode in modes:
-        M, st = res[mode]
-        d = field_rel(M, Mp)
-        print(f"{mode}: 100-step field-relative difference vs plain {d:.3e}, t {st['t']:.17g} vs {sp['t']:.17g}, "
-              f"fallback {st['fallback_cells']}/{st['stage_cells']}")
-        assert st["nn"] == 100 and d <= 1e-8, (mode, d)
+    g = Solver(p, mode=mode)
+    worst = 0.0
+    try:
+        g.set_state(M0)
+        for k in range(100):
+            Mprev, tprev = g.get_state(), g.stats()["t"]
+            g.advance(1)
+            Mg, st = g.get_state(), g.stats()
+            Mo = np.asfortranarray(Mprev)
+            _, to, _ = ol.step(Mo, pp, tprev)
+            d = field_rel(Mg, Mo)
+            worst = max(worst, d)
+            assert d <= 1e-12 and abs(st["t"] - to) <= 1e-12 * to, (k, d)
+        Ml, stl = g.get_state(), g.stats()
+    finally:
+        g.close()
+    s = Solver(p)
+    try:
+        s.set_state(M0)
+        s.advance(100)
+        Mp, sp = s.get_state(), s.stats()
+    finally:
+        s.close()
+    print(f"{mode}: worst per-step field-relative difference {worst:.3e}; after 100 steps vs plain {field_rel(Ml, Mp):.3e} "
+          f"(t {stl['t']:.17g} vs {sp['t']:.17g}); fallback {stl['fallback_cells']}/{stl['stage_cells']}")
 
 
 def test_trained_network_cuts_evaluations(tmp_path):

@@ -1,0 +1,81 @@
+"""GPU step against the oracle at the benchmark sizes, from the run's own
+late states.
+
+The crossing-jets runs of the benchmark (160x160x80 Ma=1 Kn=1 and
+256x256x128 Ma=1 Kn=0.01, CFL 0.5) advance on the GPU to the listed steps;
+from each of those states one GPU step (plain path) and one oracle step (the
+reference's serial step restated on the CPU, all host threads) must agree
+bit for bit, t and dt included.  Late in these runs nearly every Jacobian
+takes the general eigen-solve and the eigenvalue stages run dense
+(hyq_stats.dense_mask), which is where earlier checks compared only GPU
+versions with each other.  The learned path's step from the same states
+must agree with the oracle to 1e-12 relative per moment field (FP64).
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+from hyqmom import ic, wavenet
+
+torch = pytest.importorskip("torch")
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+import bench  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def field_rel(a, b):
+    a = np.asarray(a).reshape(-1, 35)
+    b = np.asarray(b).reshape(-1, 35)
+    scale = np.maximum(np.max(np.abs(b), axis=0), 1e-300)
+    return float(np.max(np.max(np.abs(a - b), axis=0) / scale))
+
+
+@pytest.mark.parametrize("case,marks", [("c2", [0, 50, 100, 150]), ("c5", [0, 50, 100])])
+def test_gpu_step_matches_oracle_at_scale(case, marks):
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hyqmom.runner import Solver
+    p = bench.workload(case)
+    pp = dict(p, **ic.grid_spacing(p))
+    learned = os.path.exists(wavenet.WEIGHTS_PATH)
+    s = Solver(p)
+    sl = Solver(p, mode="learned") if learned else None
+    report = []
+    try:
+        s.set_state(ic.initial_state(p))
+        for k in marks:
+            st = s.stats()
+            if st["nn"] < k:
+                s.advance(k - st["nn"])
+            st = s.stats()
+            assert st["nn"] == k and st["status"] == 0
+            Mk, tk = s.get_state(), st["t"]
+            if sl is not None:
+                sl.set_state(Mk)
+                sl.set_clock(tk, k)
+                sl.advance(1)
+                Ml, stl = sl.get_state(), sl.stats()
+            s.advance(1)
+            Mg, sg = s.get_state(), s.stats()
+            Mo = np.asfortranarray(Mk)
+            dto, to, _ = ol.step(Mo, pp, tk)
+            rep = {"step": k + 1, "dense_mask": sg["dense_mask"], "bitwise": bool(np.array_equal(Mg, Mo))}
+            assert np.array_equal(Mg, Mo), (k, field_rel(Mg, Mo))
+            assert sg["t"] == to and sg["dt"] == dto
+            if sl is not None:
+                rep["learned_rel"] = field_rel(Ml, Mo)
+                rep["learned_fallback"] = stl["fallback_cells"] / max(1, stl["stage_cells"])
+                assert rep["learned_rel"] <= 1e-12 and abs(stl["t"] - to) <= 1e-12 * to, rep
+            report.append(rep)
+    finally:
+        s.close()
+        if sl is not None:
+            sl.close()
+    print(case, report)
+    if case == "c2":
+        assert report[-1]["dense_mask"] != 0, report
