@@ -43,7 +43,7 @@ B_ALG = 2 * 35 * 8  # bytes per cell-step: state read once, written once
 
 # The step's kernels in launch order (hyq_advance_timed slots); an eigenvalue
 # stage slot holds its kernel and the passes over the cells it listed.
-LAUNCHES_PER_STEP = {"plain": 21, "certified": 21, "learned": 22}
+LAUNCHES_PER_STEP = {"plain": 24, "certified": 24, "learned": 25}
 STAGE_KERNELS = {k: f"k_{p}_eig+k_{p}_fix+k_{p}_corr ({k[-1]})" for k, p in
                  (("A2_eig_x", "A"), ("A3_eig_y", "A"), ("A4_eig_z", "A"), ("E2_eig_x", "E"), ("E3_eig_y", "E"))}
 KERNELS = ["A1_closure", "A2_eig_x", "A3_eig_y", "A4_eig_z", "A5_flux_speeds", "cfl", "hll",

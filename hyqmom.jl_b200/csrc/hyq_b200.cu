@@ -175,6 +175,90 @@ __global__ void k_set_clock(DevClock* clk, double t, long long nn) {
   clk->t = t; clk->nn = nn; clk->dt = 0.0; clk->vmax = 0.0; clk->active = 0; clk->status = 0;
   for (int q = 0; q < 5; ++q) clk->dense[q] = 0;
   clk->fb_cells = 0; clk->stage_cells = 0;
+  for (int q = 0; q < 3; ++q) clk->vdir_bits[q] = 0;
+  clk->worst_cell = ~0ull; clk->worst_dir = -1;
+  clk->maxdiff = 0.0; clk->maxdiff_nn = -1;
+}
+
+// First-step diagnostics (src/simulation_runner.jl:404-470): at step 1 only,
+// the largest |speed| along each axis over all cells (Julia `maximum`
+// semantics: a NaN wins; |speed| bit patterns order like the values, NaN
+// above Inf), then the first cell that attains the global maximum.
+__global__ void __launch_bounds__(256) k_diag_speeds(const double* __restrict__ vp, const StepConst sc, DevClock* clk) {
+  if (!clk->active || clk->nn != 1) return;
+  const long long N = sc.N;
+  unsigned long long m[3] = {0, 0, 0};
+  for (long long c = (long long)blockIdx.x * 256 + threadIdx.x; c < N; c += (long long)gridDim.x * 256)
+    for (int d = 0; d < 3; ++d)
+      for (int q = 0; q < 2; ++q) {
+        const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(vp[c + N * (2 * d + q)]));
+        m[d] = b > m[d] ? b : m[d];
+      }
+  for (int d = 0; d < 3; ++d) {
+    unsigned long long v = m[d];
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+      v = w > v ? w : v;
+    }
+    if ((threadIdx.x & 31) == 0 && v) atomicMax(&clk->vdir_bits[d], v);
+  }
+}
+__global__ void __launch_bounds__(256) k_diag_worst(const double* __restrict__ vp, const StepConst sc, DevClock* clk) {
+  if (!clk->active || clk->nn != 1) return;
+  const long long N = sc.N;
+  unsigned long long g = clk->vdir_bits[0];
+  g = clk->vdir_bits[1] > g ? clk->vdir_bits[1] : g;
+  g = clk->vdir_bits[2] > g ? clk->vdir_bits[2] : g;
+  for (long long c = (long long)blockIdx.x * 256 + threadIdx.x; c < N; c += (long long)gridDim.x * 256)
+    for (int d = 0; d < 3; ++d)
+      for (int q = 0; q < 2; ++q)
+        if ((unsigned long long)__double_as_longlong(fabs(vp[c + N * (2 * d + q)])) == g) {
+          // lowest cell first, then lowest direction (the reference scans x, y, z)
+          const unsigned long long key = ((unsigned long long)c << 2) | (unsigned long long)d;
+          atomicMin(&clk->worst_cell, key);
+        }
+}
+
+// MaxDiff (src/simulation_runner.jl:562-637) of the state after the step, at
+// steps nn % interval == 0 and nn == 1: on the diagonal i = j of the first
+// z-layer, Diff_m(i) = M_m(i,i) -+ M_m(N'-1-i, N'-1-i) for the moments
+// M000, M100, M200, M300, M400 (- for the even ones, + for the odd ones),
+// MaxDiff = max_m |max_i Diff_m(i) / (||Diff_m||_2 + 1)|; NaN propagates.
+__global__ void __launch_bounds__(256) k_maxdiff(const double* __restrict__ M, const StepConst sc, DevClock* clk) {
+  if (!clk->active || sc.symmetry_check_interval <= 0) return;
+  const long long nn = clk->nn;
+  if (!(nn % sc.symmetry_check_interval == 0 || nn == 1)) return;
+  const int Nd = sc.Nx < sc.Ny ? sc.Nx : sc.Ny;
+  const long long N = sc.N;
+  __shared__ double smax[5][8], ssq[5][8];
+  double mx[5], sq[5];
+  for (int m = 0; m < 5; ++m) { mx[m] = -INFINITY; sq[m] = 0.0; }
+  for (int i = threadIdx.x; i < Nd; i += 256) {
+    const int j = Nd - 1 - i;
+    const long long a = (long long)i + (long long)sc.Nx * i, b = (long long)j + (long long)sc.Nx * j;
+    for (int m = 0; m < 5; ++m) {
+      const double d = (m & 1) ? M[a + N * m] + M[b + N * m] : M[a + N * m] - M[b + N * m];
+      mx[m] = nanmax(mx[m], d);
+      sq[m] = sq[m] + d * d;
+    }
+  }
+  for (int m = 0; m < 5; ++m) {
+    mx[m] = warp_nanmax(mx[m]);
+    double v = sq[m];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) { smax[m][threadIdx.x >> 5] = mx[m]; ssq[m][threadIdx.x >> 5] = v; }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double md = 0.0;
+    for (int m = 0; m < 5; ++m) {
+      double a = -INFINITY, q = 0.0;
+      for (int w = 0; w < 8; ++w) { a = nanmax(a, smax[m][w]); q = q + ssq[m][w]; }
+      md = nanmax(md, fabs(a / (sqrt(q) + 1.0)));
+    }
+    clk->maxdiff = md;
+    clk->maxdiff_nn = nn;
+  }
 }
 
 
@@ -223,8 +307,10 @@ void enqueue_step(hyq_ctx* ctx, cudaStream_t s) {
   const long long N = ctx->N;
   launch_phase_A(ctx->sc, ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s, nullptr, 0, -1, &ctx->net);
   k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
+  launch_diagnostics_speeds(ctx->vp, ctx->sc, ctx->clk, s);
   k_hll<<<grid_of(N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
   launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->clk, s);
+  launch_maxdiff(ctx->M, ctx->sc, ctx->clk, s);
 }
 // Capture one step as the context's graph (replacing an earlier one).
 int capture_graph(hyq_ctx* ctx) {
@@ -262,6 +348,12 @@ void launch_hll(const double* M, const double* Fx, const double* Fy, const doubl
   k_hll<<<grid_of(sc.N, BS_HLL), BS_HLL, 0, s>>>(M, Fx, Fy, Fz, vp, Mout, sc, clk);
 }
 void launch_set_clock(DevClock* clk, double t, long long nn, cudaStream_t s) { k_set_clock<<<1, 1, 0, s>>>(clk, t, nn); }
+void launch_diagnostics_speeds(const double* vp, const StepConst& sc, DevClock* clk, cudaStream_t s) {
+  const int g = (int)((sc.N + 255) / 256 < 148 * 8 ? (sc.N + 255) / 256 : 148 * 8);
+  k_diag_speeds<<<g, 256, 0, s>>>(vp, sc, clk);
+  k_diag_worst<<<g, 256, 0, s>>>(vp, sc, clk);
+}
+void launch_maxdiff(const double* M, const StepConst& sc, DevClock* clk, cudaStream_t s) { k_maxdiff<<<1, 256, 0, s>>>(M, sc, clk); }
 int report_error(int code, const char* msg) { return fail(nullptr, code, msg); }
 }  // namespace hyqk
 
@@ -295,6 +387,7 @@ int hyq_create(const hyq_params* p, hyq_ctx** out) {
   sc.dx = (p->xmax - p->xmin) / p->Nx; sc.dy = (p->ymax - p->ymin) / p->Ny; sc.dz = (p->zmax - p->zmin) / p->Nz;
   sc.nblocksA = grid_of(N, BS_A);
   sc.mode = p->mode;
+  sc.symmetry_check_interval = p->symmetry_check_interval;
   sc.seeds = nullptr;
   sc.seed_margin = 0.0;
   const size_t b35 = sizeof(double) * 35 * (size_t)N;
@@ -455,10 +548,12 @@ int hyq_advance_timed(hyq_ctx* ctx, int64_t steps, float* ms) {
     cudaEventRecord(ev[0], s);
     launch_phase_A(ctx->sc, ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s, ev + 1, 0, -1, &ctx->net);
     k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
+    launch_diagnostics_speeds(ctx->vp, ctx->sc, ctx->clk, s);
     cudaEventRecord(ev[6], s);
     k_hll<<<grid_of(N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
     cudaEventRecord(ev[7], s);
     launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->clk, s, ev + 8);
+    launch_maxdiff(ctx->M, ctx->sc, ctx->clk, s);
     HQ_CHECK(ctx, cudaEventSynchronize(ev[K]));
     for (int q = 0; q < K; ++q) {
       float t = 0.0f;
@@ -489,7 +584,15 @@ int hyq_stats_get(hyq_ctx* ctx, hyq_stats* out) {
   out->fallback_cells = (int64_t)h.fb_cells;
   out->dense_mask = 0;
   for (int q = 0; q < 5; ++q) out->dense_mask |= (h.dense[q] > 0 ? 1 : 0) << q;
-  out->reserved = 0;
+  for (int q = 0; q < 3; ++q) {
+    double v;
+    std::memcpy(&v, &h.vdir_bits[q], sizeof v);
+    out->vmax_first[q] = v;
+  }
+  out->worst_cell = h.worst_cell == ~0ull ? -1 : (int64_t)(h.worst_cell >> 2);
+  out->worst_dir = h.worst_cell == ~0ull ? -1 : (int32_t)(h.worst_cell & 3ull);
+  out->maxdiff = h.maxdiff;
+  out->maxdiff_step = h.maxdiff_nn;
   return HYQ_OK;
 }
 
@@ -539,6 +642,7 @@ int hyq_step_host(hyq_ctx* ctx, const double* M_in, double* M_out, int32_t nslab
   }
   // the CFL reduction and the HLL sweep need every cell
   k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
+  launch_diagnostics_speeds(ctx->vp, ctx->sc, ctx->clk, s);
   k_hll<<<grid_of(N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
   // phases E+F slab by slab, each slab downloaded as soon as it is done
   for (int k = 0; k < S; ++k) {
@@ -548,6 +652,7 @@ int hyq_step_host(hyq_ctx* ctx, const double* M_in, double* M_out, int32_t nslab
     HQ_CHECK(ctx, cudaStreamWaitEvent(cs, ctx->down[k], 0));
     HQ_CHECK(ctx, cudaMemcpy2DAsync(M_out + c0, pitch, ctx->M + c0, pitch, sizeof(double) * (size_t)(c1 - c0), 35, cudaMemcpyDeviceToHost, cs));
   }
+  launch_maxdiff(ctx->M, ctx->sc, ctx->clk, s);
   HQ_CHECK(ctx, cudaGetLastError());
   HQ_CHECK(ctx, cudaStreamSynchronize(cs));
   hyq_stats st;

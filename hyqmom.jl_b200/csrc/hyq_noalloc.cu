@@ -135,6 +135,7 @@ extern "C" int hyq_step_noalloc(const hyq_params* p, double* M, hyq_stats* stats
   sc.dx = (p->xmax - p->xmin) / p->Nx; sc.dy = (p->ymax - p->ymin) / p->Ny; sc.dz = (p->zmax - p->zmin) / p->Nz;
   sc.nblocksA = grid_of(N, BS_A);
   sc.mode = MODE_PLAIN;
+  sc.symmetry_check_interval = 0;
   sc.seeds = nullptr;
   sc.seed_margin = 0.0;
 
@@ -158,7 +159,9 @@ extern "C" int hyq_step_noalloc(const hyq_params* p, double* M, hyq_stats* stats
   if ((e = cudaMemcpyAsync(&h, clk, sizeof(DevClock), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_error(e, "clock copy");
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(e, "cudaStreamSynchronize");
   stats->t = h.t; stats->dt = h.dt; stats->vmax = h.vmax; stats->nn = h.nn; stats->status = h.status;
-  stats->stage_cells = 0; stats->fallback_cells = 0; stats->dense_mask = 0; stats->reserved = 0;
+  stats->stage_cells = 0; stats->fallback_cells = 0; stats->dense_mask = 0; stats->worst_dir = -1;
+  stats->vmax_first[0] = stats->vmax_first[1] = stats->vmax_first[2] = 0.0; stats->worst_cell = -1;
+  stats->maxdiff = 0.0; stats->maxdiff_step = -1;
   stats->done = (h.t < p->tmax && h.nn < p->nnmax) ? 0 : 1;
   if (h.status > 0)
     return report_error(HYQ_ENONFINITE, ("non-finite CFL wave speed at step " + std::to_string(h.status) +

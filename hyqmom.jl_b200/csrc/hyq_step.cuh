@@ -19,6 +19,14 @@ struct DevClock {
   // not certify (they fell back to the LAPACK path), and cells the certified
   // stages processed, summed over stages and steps since the last reset
   unsigned long long fb_cells, stage_cells;
+  // first-step diagnostics: per-direction max |speed| (bit patterns, for
+  // atomicMax), the worst cell and its direction
+  unsigned long long vdir_bits[3];
+  unsigned long long worst_cell;
+  int worst_dir;
+  // MaxDiff of the state after step maxdiff_nn (-1: none yet)
+  double maxdiff;
+  long long maxdiff_nn;
 };
 
 // Eigenvalue path of a context (hyq_params.mode).
@@ -38,6 +46,7 @@ struct StepConst {
   // speeds, which the network kernel writes to `seeds` after the first
   // closure of each step.
   int mode;
+  int symmetry_check_interval;
   // predicted standardized extreme speeds, SoA [6][N] (x lo, x hi, y lo,
   // y hi, z lo, z hi): lam = u + sqrt(C_aa) * s; NULL unless MODE_LEARNED
   float* seeds;
@@ -125,6 +134,11 @@ void launch_cells_targets(const double* M, long long n, int flag2D, double Ma, i
 // (defined in hyq_b200.cu) the CFL, HLL and clock-reset launches of one step,
 // and the thread-local error text read by hyq_last_error(NULL)
 void launch_cfl(const double* blockmax, const StepConst& sc, DevClock* clk, cudaStream_t s);
+// the first-step diagnostics (after the CFL reduction, on the six speed
+// arrays vp) and MaxDiff (after the step, on M); both return at once on
+// the steps they do not measure
+void launch_diagnostics_speeds(const double* vp, const StepConst& sc, DevClock* clk, cudaStream_t s);
+void launch_maxdiff(const double* M, const StepConst& sc, DevClock* clk, cudaStream_t s);
 void launch_hll(const double* M, const double* Fx, const double* Fy, const double* Fz, const double* vp, double* Mout, const StepConst& sc,
                 const DevClock* clk, cudaStream_t s);
 void launch_set_clock(DevClock* clk, double t, long long nn, cudaStream_t s);

@@ -20,7 +20,7 @@ class HyqParams(ctypes.Structure):
                 ("tmax", ctypes.c_double), ("Kn", ctypes.c_double), ("Ma", ctypes.c_double), ("CFL", ctypes.c_double),
                 ("dtmax", ctypes.c_double), ("xmin", ctypes.c_double), ("xmax", ctypes.c_double),
                 ("ymin", ctypes.c_double), ("ymax", ctypes.c_double), ("zmin", ctypes.c_double), ("zmax", ctypes.c_double),
-                ("mode", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("mode", ctypes.c_int32), ("symmetry_check_interval", ctypes.c_int32)]
 
 
 # hyq_params.mode
@@ -32,7 +32,9 @@ NET_PARAMS = 38406  # HYQ_NET_PARAMS
 class HyqStats(ctypes.Structure):
     _fields_ = [("t", ctypes.c_double), ("dt", ctypes.c_double), ("vmax", ctypes.c_double), ("nn", ctypes.c_int64),
                 ("done", ctypes.c_int32), ("status", ctypes.c_int32), ("stage_cells", ctypes.c_int64),
-                ("fallback_cells", ctypes.c_int64), ("dense_mask", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("fallback_cells", ctypes.c_int64), ("dense_mask", ctypes.c_int32), ("worst_dir", ctypes.c_int32),
+                ("vmax_first", ctypes.c_double * 3), ("worst_cell", ctypes.c_int64), ("maxdiff", ctypes.c_double),
+                ("maxdiff_step", ctypes.c_int64)]
 
 
 class HyqError(RuntimeError):

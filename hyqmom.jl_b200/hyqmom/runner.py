@@ -25,7 +25,8 @@ def params_struct(p, device=0, mode="plain"):
                           positivity=int(bool(p.get("positivity", True))), device=device, nnmax=int(p["nnmax"]),
                           tmax=float(p["tmax"]), Kn=float(p["Kn"]), Ma=float(p["Ma"]), CFL=float(p["CFL"]),
                           dtmax=float(p["dtmax"]), xmin=xmin, xmax=xmax, ymin=ymin, ymax=ymax, zmin=zmin, zmax=zmax,
-                          mode=_lib.MODES[mode] if isinstance(mode, str) else int(mode))
+                          mode=_lib.MODES[mode] if isinstance(mode, str) else int(mode),
+                          symmetry_check_interval=int(p.get("symmetry_check_interval", 0) or 0))
 
 
 class Solver:
@@ -135,7 +136,9 @@ class Solver:
         st = _lib.HyqStats()
         self._chk(self._lib.hyq_stats_get(self._h, ctypes.byref(st)))
         return dict(t=st.t, dt=st.dt, vmax=st.vmax, nn=st.nn, done=bool(st.done), status=st.status,
-                    stage_cells=st.stage_cells, fallback_cells=st.fallback_cells, dense_mask=st.dense_mask)
+                    stage_cells=st.stage_cells, fallback_cells=st.fallback_cells, dense_mask=st.dense_mask,
+                    vmax_first=tuple(st.vmax_first), worst_cell=st.worst_cell, worst_dir=st.worst_dir, maxdiff=st.maxdiff,
+                    maxdiff_step=st.maxdiff_step)
 
     def reset_counters(self):
         self._chk(self._lib.hyq_reset_counters(self._h))
@@ -202,6 +205,30 @@ def _runner_params(params):
     return p
 
 
+def print_first_step_diagnostics(p, st):
+    """The reference's FIRST STEP DIAGNOSTICS block (src/simulation_runner.jl:404-470)
+    from the device's first-step breakdown."""
+    g = _ic.grid_spacing(p)
+    dx, dy, dz = g["dx"], g["dy"], g["dz"]
+    vmax = max(st["vmax_first"]) if not any(v != v for v in st["vmax_first"]) else float("nan")
+    hmin = min(dx, dy, dz)
+    print("\n  === FIRST STEP DIAGNOSTICS ===")
+    print("  vmax breakdown:")
+    for name, v in zip("xyz", st["vmax_first"]):
+        print("    v%s_max = %.6e" % (name, v))
+    print("    vmax (global) = %.6e" % vmax)
+    print("  Grid spacing:\n    dx = %.6e, dy = %.6e, dz = %.6e\n    min(dx,dy,dz) = %.6e" % (dx, dy, dz, hmin))
+    print("  Time step calculation:\n    CFL = %.6f\n    dtmax = %.6e\n    Kn = %.6e" % (p["CFL"], p["dtmax"], p["Kn"]))
+    print("    CFL*min(dx,dy,dz)/vmax = %.6e" % (p["CFL"] * hmin / vmax))
+    print("    dt (final) = %.6e" % min(p["CFL"] * hmin / vmax, min(p["dtmax"], p["Kn"])))
+    if vmax > 100.0 or vmax != vmax:
+        c = st["worst_cell"]
+        i, j, k = c % p["Nx"], (c // p["Nx"]) % p["Ny"], c // (p["Nx"] * p["Ny"])
+        print("  WARNING: vmax = %.6e (unusually large or invalid)" % vmax)
+        print("  Worst cell: (%d,%d,%d) in %s-direction" % (i + 1, j + 1, k + 1, "xyz"[st["worst_dir"]]))
+    print("  ==============================\n")
+
+
 def simulation_runner(params, device=0, verbose=False, chunk=64):
     """Reference ``simulation_runner(params)`` for one rank.
 
@@ -227,12 +254,19 @@ def simulation_runner(params, device=0, verbose=False, chunk=64):
         t0 = time.time()
         done = False
         t, nn = 0.0, 0
-        step_block = interval if interval > 0 else chunk
+        # verbose: one step at a time, printed as the reference prints them
+        step_block = 1 if verbose else (interval if interval > 0 else chunk)
+        sym = int(p.get("symmetry_check_interval", 0) or 0)
         while not done:
             t, nn, done = solver.advance(step_block)
             if verbose:
                 st = solver.stats()
-                print("Step %4d: t = %.4f, dt = %.4e, wall = %.4f s" % (nn, t, st["dt"], time.time() - t0))
+                if nn == 1:
+                    print_first_step_diagnostics(p, st)
+                line = "Step %4d: t = %.4f, dt = %.4e, wall = %.4f s" % (nn, t, st["dt"], time.time() - t0)
+                if sym > 0 and st["maxdiff_step"] == nn:
+                    line += ", MaxDiff = %.3e" % st["maxdiff"]
+                print(line)
             if writer is not None and (nn % interval == 0 or done):
                 S, C = solver.get_SC()
                 writer.write(solver.get_state(), t, nn, S, C)

@@ -64,7 +64,9 @@ typedef struct hyq_params {
   double tmax, Kn, Ma, CFL, dtmax;
   double xmin, xmax, ymin, ymax, zmin, zmax; /* domain extents (:123-129) */
   int32_t mode;        /* HYQ_MODE_* (0 = plain, the reference's path) */
-  int32_t reserved;
+  int32_t symmetry_check_interval; /* params.symmetry_check_interval: MaxDiff
+                                    * every this many steps and at step 1
+                                    * (:562-637); 0 = never */
 } hyq_params;
 
 typedef struct hyq_stats {
@@ -81,7 +83,17 @@ typedef struct hyq_stats {
    * their general eigen-solve takes every cell directly because the stage
    * listed most of its cells recently */
   int32_t dense_mask;
-  int32_t reserved;
+  /* first-step diagnostics (:404-470): the largest |wave speed| along x, y
+   * and z at step 1, and the cell (c = i + Nx (j + Ny k)) and direction
+   * (0 x, 1 y, 2 z) of the largest one */
+  int32_t worst_dir;
+  double vmax_first[3];
+  int64_t worst_cell;
+  /* the diagonal symmetry measure MaxDiff (:562-637) of the state after step
+   * maxdiff_step (the last step with nn % symmetry_check_interval == 0 or
+   * nn == 1; -1 before any) */
+  double maxdiff;
+  int64_t maxdiff_step;
 } hyq_stats;
 
 typedef struct hyq_ctx hyq_ctx;

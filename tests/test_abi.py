@@ -71,7 +71,7 @@ def test_create_rejects_unknown_mode():
 def test_params_struct_layout_matches_header():
     """hyq_params / hyq_stats: the ctypes layouts have the C struct sizes
     (int32 x 6, int64, double x 11, int32 x 2; stats: double x 3, int64,
-    int32 x 2, int64 x 2, int32 x 2)."""
+    int32 x 2, int64 x 2, int32 x 2, double x 3, int64, double, int64)."""
     import ctypes
     assert ctypes.sizeof(_lib.HyqParams) == 6 * 4 + 8 + 11 * 8 + 2 * 4
-    assert ctypes.sizeof(_lib.HyqStats) == 3 * 8 + 8 + 2 * 4 + 2 * 8 + 2 * 4
+    assert ctypes.sizeof(_lib.HyqStats) == 3 * 8 + 8 + 2 * 4 + 2 * 8 + 2 * 4 + 3 * 8 + 8 + 8 + 8
