@@ -248,15 +248,15 @@ def run_gpu(args, rank, world, local_rank):
     cells = p["Nx"] * p["Ny"] * p["Nz"]
     run_steps = RUN_STEPS[args.config]
     marks = timed_steps(run_steps, args.steps)
-    M0 = ic.initial_state(p)
+    shape = (p["Nx"], p["Ny"], p["Nz"], 35)
     sol = {m: Solver(p, device=local_rank, mode=m) for m in MODES}
     traj = sol["learned"]
     streams = {m: torch.cuda.ExternalStream(sol[m].stream) for m in MODES}
     buf = torch.empty(35 * cells, dtype=torch.float64, device="cuda")  # the state before a timed step
     Mh_flat = torch.empty(35 * cells, dtype=torch.float64).pin_memory()
-    Mh = Mh_flat.numpy().reshape(M0.shape, order="F")
+    Mh = Mh_flat.numpy().reshape(shape, order="F")
     Mh_out_flat = torch.empty(35 * cells, dtype=torch.float64).pin_memory()
-    Mh_out = Mh_out_flat.numpy().reshape(M0.shape, order="F")
+    Mh_out = Mh_out_flat.numpy().reshape(shape, order="F")
 
     def barrier():
         if dist is not None:
@@ -277,11 +277,12 @@ def run_gpu(args, rank, world, local_rank):
         e1.synchronize()
         return e0.elapsed_time(e1)
 
-    traj.set_state(M0)
+    # the initial condition generated on the device (the reference's region fill)
+    traj.set_state_ic()
     # warm-up: the first W steps of the run (untimed), every path once
     for m in MODES:
         if m != "learned":
-            sol[m].set_state(M0)
+            sol[m].set_state_ic()
             sol[m].advance(1)
     traj.advance(max(1, min(args.warmup, marks[0] - 1)))
     ms = {m: [] for m in MODES}
@@ -443,12 +444,12 @@ def run_batch(args, rank, world, local_rank):
     from hyqmom.runner import BatchSolver
     ps = batch_workload()
     cells = [p["Nx"] * p["Ny"] * p["Nz"] for p in ps]
-    M0 = [ic.initial_state(p) for p in ps]
     b = BatchSolver(ps, device=local_rank)
 
     def reset():
-        for m, M in zip(b.members, M0):
-            m.set_state(M)
+        # every member's initial condition generated on the device
+        for m in b.members:
+            m.set_state_ic()
 
     def nn_all():
         return [m.stats()["nn"] for m in b.members]

@@ -335,6 +335,35 @@ int net_status(hyq_ctx* ctx) {
 }
 
 __global__ void k_reset_counters(DevClock* clk) { clk->fb_cells = 0; clk->stage_cells = 0; }
+// The device IC fill (hyq_set_state_ic): one thread per cell, the regions
+// and moments in constant-size parameter arrays read through global memory.
+constexpr int IC_MAX_REGIONS = 64;
+__global__ void __launch_bounds__(256) k_fill_ic(double* __restrict__ M, const StepConst sc, const double* __restrict__ xyz, double dx,
+                                                 double dy, double dz, const double* __restrict__ bg, int nreg,
+                                                 const hyq_ic_region* __restrict__ regs, const double* __restrict__ mom) {
+  const long long N = sc.N;
+  const long long c = (long long)blockIdx.x * 256 + threadIdx.x;
+  if (c >= N) return;
+  const int i = int(c % sc.Nx), j = int((c / sc.Nx) % sc.Ny), k = int(c / ((long long)sc.Nx * sc.Ny));
+  const double x = xyz[i], y = xyz[sc.Nx + j], z = xyz[sc.Nx + sc.Ny + k];
+  int use = -1;
+  for (int r = 0; r < nreg; ++r) {
+    const hyq_ic_region& g = regs[r];
+    bool in;
+    if (g.kind == 1) {
+      in = i >= g.i0 && i <= g.i1 && j >= g.j0 && j <= g.j1 && k >= g.k0 && k <= g.k1;
+    } else if (g.everywhere) {
+      in = true;
+    } else {
+      in = jmax(x - dx / 2.0, g.lo[0]) < jmin(x + dx / 2.0, g.hi[0]) && jmax(y - dy / 2.0, g.lo[1]) < jmin(y + dy / 2.0, g.hi[1]) &&
+           jmax(z - dz / 2.0, g.lo[2]) < jmin(z + dz / 2.0, g.hi[2]);
+    }
+    if (in) use = r;
+  }
+  const double* src = use < 0 ? bg : mom + 35 * use;
+#pragma unroll
+  for (int n = 0; n < 35; ++n) M[c + N * n] = src[n];
+}
 }  // namespace
 
 // Launch helpers for other translation units (same kernels and shapes as
@@ -472,6 +501,36 @@ int hyq_set_state(hyq_ctx* ctx, const double* M) {
   HQ_CHECK(ctx, cudaSetDevice(ctx->device));
   HQ_CHECK(ctx, cudaMemcpyAsync(ctx->M, M, sizeof(double) * 35 * ctx->N, cudaMemcpyHostToDevice, ctx->stream));
   k_set_clock<<<1, 1, 0, ctx->stream>>>(ctx->clk, 0.0, 0);
+  HQ_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  return HYQ_OK;
+}
+
+int hyq_set_state_ic(hyq_ctx* ctx, const double* xm, const double* ym, const double* zm, double dx, double dy, double dz,
+                     const double* bg, int32_t nregions, const hyq_ic_region* regions, const double* moments) {
+  if (!ctx || !xm || !ym || !zm || !bg || nregions < 0 || (nregions > 0 && (!regions || !moments)))
+    return fail(ctx, HYQ_EINVAL, "null argument");
+  if (nregions > IC_MAX_REGIONS) return fail(ctx, HYQ_EINVAL, "at most 64 regions");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  // one small upload of the tables: centres, background, regions, moments
+  const int nx = ctx->p.Nx, ny = ctx->p.Ny, nz = ctx->p.Nz;
+  std::vector<double> tab((size_t)nx + ny + nz + 35 + 35 * (size_t)nregions);
+  std::memcpy(tab.data(), xm, sizeof(double) * nx);
+  std::memcpy(tab.data() + nx, ym, sizeof(double) * ny);
+  std::memcpy(tab.data() + nx + ny, zm, sizeof(double) * nz);
+  std::memcpy(tab.data() + nx + ny + nz, bg, sizeof(double) * 35);
+  if (nregions) std::memcpy(tab.data() + nx + ny + nz + 35, moments, sizeof(double) * 35 * nregions);
+  // the tables ride in the flux buffer Fx (dead between steps)
+  const size_t rbytes = sizeof(hyq_ic_region) * (size_t)nregions;
+  double* dtab = ctx->Fx;
+  hyq_ic_region* dreg = reinterpret_cast<hyq_ic_region*>(ctx->Fx + tab.size() + 8);
+  if ((tab.size() + 8) * sizeof(double) + rbytes > sizeof(double) * 35 * (size_t)ctx->N)
+    return fail(ctx, HYQ_EINVAL, "grid too small for the IC tables");
+  HQ_CHECK(ctx, cudaMemcpyAsync(dtab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, ctx->stream));
+  if (nregions) HQ_CHECK(ctx, cudaMemcpyAsync(dreg, regions, rbytes, cudaMemcpyHostToDevice, ctx->stream));
+  k_fill_ic<<<grid_of(ctx->N, 256), 256, 0, ctx->stream>>>(ctx->M, ctx->sc, dtab, dx, dy, dz, dtab + nx + ny + nz, nregions, dreg,
+                                                           dtab + nx + ny + nz + 35);
+  k_set_clock<<<1, 1, 0, ctx->stream>>>(ctx->clk, 0.0, 0);
+  HQ_CHECK(ctx, cudaGetLastError());
   HQ_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
   return HYQ_OK;
 }

@@ -23,6 +23,12 @@ class HyqParams(ctypes.Structure):
                 ("mode", ctypes.c_int32), ("symmetry_check_interval", ctypes.c_int32)]
 
 
+class HyqIcRegion(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("everywhere", ctypes.c_int32), ("lo", ctypes.c_double * 3), ("hi", ctypes.c_double * 3),
+                ("i0", ctypes.c_int32), ("i1", ctypes.c_int32), ("j0", ctypes.c_int32), ("j1", ctypes.c_int32),
+                ("k0", ctypes.c_int32), ("k1", ctypes.c_int32)]
+
+
 # hyq_params.mode
 MODE_PLAIN, MODE_LEARNED, MODE_CERTIFIED = 0, 1, 2
 MODES = {"plain": MODE_PLAIN, "learned": MODE_LEARNED, "certified": MODE_CERTIFIED}
@@ -50,7 +56,7 @@ SYMBOLS = ["hyq_abi_version", "hyq_create", "hyq_destroy", "hyq_last_error", "hy
            "hyq_cells_eigenvalues", "hyq_cells_closure_eigs", "hyq_cells_collision", "hyq_cells_phase_A", "hyq_step_noalloc", "hyq_batch_create", "hyq_batch_destroy", "hyq_batch_size",
            "hyq_batch_member", "hyq_batch_stream", "hyq_batch_advance_async", "hyq_batch_advance", "hyq_reset_counters",
            "hyq_set_wavespeed_net", "hyq_net_image_bytes", "hyq_net_tile_bytes", "hyq_net_scratch_bytes", "hyq_net_pack",
-           "hyq_net_features", "hyq_net_forward", "hyq_net_train_batch", "hyq_net_adam", "hyq_cells_wavespeed_targets"]
+           "hyq_net_features", "hyq_net_forward", "hyq_net_train_batch", "hyq_net_adam", "hyq_cells_wavespeed_targets", "hyq_set_state_ic"]
 NOALLOC_MAX_CELLS = 16384  # HYQ_NOALLOC_MAX_CELLS
 
 
@@ -112,6 +118,7 @@ def load(path=None):
     lib.hyq_net_train_batch.argtypes = [vp, vp, vp, i64, vp, i32, flt, vp, vp, i32, vp, vp, vp]
     lib.hyq_net_adam.argtypes = [vp, vp, vp, vp, i32, flt, flt, flt, flt, flt, i32, vp, vp]
     lib.hyq_cells_wavespeed_targets.argtypes = [vp, i64, i32, dbl, i32, vp, vp, vp]
+    lib.hyq_set_state_ic.argtypes = [vp, vp, vp, vp, dbl, dbl, dbl, vp, i32, vp, vp]
     _lib = lib
     return lib
 

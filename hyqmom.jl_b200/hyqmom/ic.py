@@ -307,3 +307,43 @@ def with_jets(p, config="crossing"):
     q = dict(p)
     q.update(ic_background=bg, ic_jets=jets, use_custom_ic=True, config=config)
     return q
+
+
+def ic_tables(p):
+    """The tables of the device IC fill (hyq_set_state_ic) that reproduce
+    initial_state(p): (xm, ym, zm, dx, dy, dz, bg[35], regions, moments[35 x R]);
+    a region is (kind, everywhere, lo[3], hi[3], (i0, i1, j0, j1, k0, k1))."""
+    Nx, Ny, Nz = p["Nx"], p["Ny"], p["Nz"]
+    g = grid(p)
+    xm, ym, zm = g["xm"], g["ym"], g["zm"]
+    if p.get("use_custom_ic", False):
+        background, jets = p["ic_background"], list(p["ic_jets"])
+        r = (p.get("r110", 0.0), p.get("r101", 0.0), p.get("r011", 0.0))
+        dx = abs(xm[1] - xm[0]) if Nx > 1 else 0.0
+        dy = abs(ym[1] - ym[0]) if Ny > 1 else 0.0
+        dz = abs(zm[1] - zm[0]) if Nz > 1 else 0.0
+        bg = region_to_moments(background, *r)
+        regions, moments = [], []
+        for jet in jets:
+            every = any(math.isinf(wv) for wv in jet.width)
+            lo = [0.0, 0.0, 0.0] if every else [jet.center[q] - jet.width[q] / 2 for q in range(3)]
+            hi = [0.0, 0.0, 0.0] if every else [jet.center[q] + jet.width[q] / 2 for q in range(3)]
+            regions.append((0, int(every), lo, hi, (0, -1, 0, -1, 0, -1)))
+            moments.append(region_to_moments(jet, *r))
+        return xm, ym, zm, dx, dy, dz, bg, regions, moments
+    T = p["T"]
+    r110, r101, r011 = p.get("r110", 0.0), p.get("r101", 0.0), p.get("r011", 0.0)
+    C2 = (T, r110 * math.sqrt(T * T), r101 * math.sqrt(T * T), T, r011 * math.sqrt(T * T), T)
+    bg = gaussian_moments(p["rhor"], 0.0, 0.0, 0.0, *C2)
+    Uc = p["Ma"] / math.sqrt(2.0)
+    Mt = gaussian_moments(p["rhol"], -Uc, -Uc, 0.0, *C2)
+    Mb = gaussian_moments(p["rhol"], Uc, Uc, 0.0, *C2)
+    Cx, Cy = int(math.floor(0.1 * Nx)), int(math.floor(0.1 * Ny))
+    Mint_x, Maxt_x, Minb_x, Maxb_x = Nx // 2 + 1, Nx // 2 + 1 + Cx, Nx // 2 - Cx, Nx // 2
+    Mint_y, Maxt_y, Minb_y, Maxb_y = Ny // 2 + 1, Ny // 2 + 1 + Cy, Ny // 2 - Cy, Ny // 2
+    Cz = min(Cx, Cy)
+    Mint_z, Maxt_z = Nz // 2 + 1 - Cz // 2, Nz // 2 + 1 + Cz // 2
+    zero3 = [0.0, 0.0, 0.0]
+    regions = [(1, 0, zero3, zero3, (Minb_x - 1, Maxb_x - 1, Minb_y - 1, Maxb_y - 1, Mint_z - 1, Maxt_z - 1)),
+               (1, 0, zero3, zero3, (Mint_x - 1, Maxt_x - 1, Mint_y - 1, Maxt_y - 1, Mint_z - 1, Maxt_z - 1))]
+    return xm, ym, zm, 0.0, 0.0, 0.0, bg, regions, [Mb, Mt]

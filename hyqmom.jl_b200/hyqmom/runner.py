@@ -84,6 +84,24 @@ class Solver:
         assert M.shape == self.shape
         self._chk(self._lib.hyq_set_state(self._h, M.ctypes.data))
 
+    def set_state_ic(self, params=None):
+        """Generate the initial condition of `params` (default: the solver's)
+        on the device (hyq_set_state_ic); equal bit for bit to ic.initial_state."""
+        p = self.params if params is None else params
+        xm, ym, zm, dx, dy, dz, bg, regions, moments = _ic.ic_tables(p)
+        n = len(regions)
+        arr = (_lib.HyqIcRegion * max(n, 1))()
+        for q, (kind, every, lo, hi, idx) in enumerate(regions):
+            arr[q].kind, arr[q].everywhere = kind, every
+            for a in range(3):
+                arr[q].lo[a], arr[q].hi[a] = lo[a], hi[a]
+            arr[q].i0, arr[q].i1, arr[q].j0, arr[q].j1, arr[q].k0, arr[q].k1 = idx
+        xm, ym, zm = (np.ascontiguousarray(a, dtype=np.float64) for a in (xm, ym, zm))
+        bg = np.ascontiguousarray(bg, dtype=np.float64)
+        mom = np.ascontiguousarray(np.array(moments, dtype=np.float64).reshape(-1)) if n else np.zeros(1)
+        self._chk(self._lib.hyq_set_state_ic(self._h, xm.ctypes.data, ym.ctypes.data, zm.ctypes.data, float(dx), float(dy), float(dz),
+                                             bg.ctypes.data, n, ctypes.cast(arr, ctypes.c_void_p), mom.ctypes.data))
+
     def get_state(self):
         M = np.empty(self.shape, dtype=np.float64, order="F")
         self._chk(self._lib.hyq_get_state(self._h, M.ctypes.data))

@@ -119,6 +119,29 @@ int hyq_get_state(hyq_ctx* ctx, double* M);
  * stream (hyq_synchronize, or an event recorded on hyq_stream). */
 int hyq_set_state_device(hyq_ctx* ctx, const double* dM);
 int hyq_get_state_device(hyq_ctx* ctx, double* dM);
+/* The initial condition generated on the device (no host state, no upload):
+ * the reference's region fill of initialize_moment_field_mpi
+ * (src/initial_conditions.jl:152-217, cell_overlaps_cube :281-302) and of the
+ * runner's built-in cubes (src/simulation_runner.jl:200-271).  Every cell
+ * gets bg[35], then, region by region in order, the region's moments where
+ * the region covers the cell:
+ *   kind 0, a box [lo, hi] in coordinates (lo = center - width/2, hi =
+ *     center + width/2 as the reference forms them): the cell with centre
+ *     (xm[i], ym[j], zm[k]) and widths (dx, dy, dz) overlaps it when
+ *     max(x - d/2, lo) < min(x + d/2, hi) on every axis (strict, as the
+ *     reference), or everywhere when `everywhere` is set (infinite width);
+ *   kind 1, an index box: i0 <= i <= i1, j0 <= j <= j1, k0 <= k <= k1
+ *     (0-based, inclusive).
+ * xm, ym, zm: the cell centres (Nx, Ny, Nz doubles, Julia range values);
+ * moments: 35 * nregions doubles.  Time and step count reset to 0. */
+typedef struct hyq_ic_region {
+  int32_t kind, everywhere;
+  double lo[3], hi[3];
+  int32_t i0, i1, j0, j1, k0, k1;
+} hyq_ic_region;
+int hyq_set_state_ic(hyq_ctx* ctx, const double* xm, const double* ym, const double* zm, double dx, double dy, double dz,
+                     const double* bg, int32_t nregions, const hyq_ic_region* regions, const double* moments);
+
 /* Set the loop clock (t, nn) without touching the state. */
 int hyq_set_clock(hyq_ctx* ctx, double t, int64_t nn);
 /* Zero the fallback counters of hyq_stats. */
