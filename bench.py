@@ -417,6 +417,53 @@ def count_ops_on(p, slabs):
     return tot / n, F
 
 
+def run_slabs(args, rank, world, local_rank):
+    """One domain split into z-slabs over the ranks (hyqmom.slabs; ghost
+    exchange and the dt all-reduce over NCCL): the workload's steps W+1 ..
+    W+K on the learned path, strong scaling (the whole grid over N GPUs)."""
+    import torch
+    import torch.distributed as dist
+    from hyqmom import slabs
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    p = workload(args.config)
+    cells = p["Nx"] * p["Ny"] * p["Nz"]
+    eng = slabs.GpuSlab(p, world, rank, device=local_rank, mode="learned")
+    eng.set_initial_condition()
+    d = dist if world > 1 else None
+
+    def buf(shape):
+        return torch.zeros(shape, dtype=torch.float64, device="cuda")
+
+    for _ in range(args.warmup):
+        slabs.step(eng, rank, world, eng.layout, d, buf)
+    torch.cuda.synchronize()
+    if d is not None:
+        d.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        slabs.step(eng, rank, world, eng.layout, d, buf)
+    e1.record()
+    e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), d, "cuda")
+    st = eng.stats()
+    eng.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": cells * args.steps / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference crossing-jets IC generator)",
+                "config": {"workload": f"crossing jets {p['Nx']}x{p['Ny']}x{p['Nz']} Ma={p['Ma']} Kn={p['Kn']} CFL={p['CFL']}, "
+                                       f"learned wave-speed path, z-slabs over {world} GPUs",
+                           "cells": cells, "parallelism": f"z-slabs x{world}", "timed_steps": f"{args.warmup + 1}-{args.warmup + args.steps}",
+                           "steps_done": st["nn"]},
+                "gpu_launches": (LAUNCHES_PER_STEP["learned"] + 4) * args.steps}
+        print(json.dumps(line), flush=True)
+    if d is not None:
+        d.destroy_process_group()
+
+
 def batch_workload(n=64, seed=0, CFL=0.5):
     """Sweep of independent domains: grids uniform from 16^3 to 96x96x48,
     Ma ~ U[0, 2], Kn log-uniform in [1e-3, 1], crossing and triple-jet ICs
@@ -506,6 +553,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c5", choices=["c1", "c2", "c2s", "c4", "c5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--decompose", default="replicas", choices=["replicas", "slabs"],
+                    help="N > 1: independent replicas (default) or one domain split into z-slabs")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -514,6 +563,8 @@ def main():
         return run_reference(args, rank, world)
     if args.config == "c4":
         return run_batch(args, rank, world, local_rank)
+    if args.decompose == "slabs":
+        return run_slabs(args, rank, world, local_rank)
     run_gpu(args, rank, world, local_rank)
 
 

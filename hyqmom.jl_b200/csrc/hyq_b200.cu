@@ -64,6 +64,37 @@ __global__ void __launch_bounds__(1024) k_cfl(const double* __restrict__ blockma
   }
 }
 
+// The CFL reduction split for a domain decomposed over ranks: the local
+// NaN-propagating max |speed| goes to xchg = {max over non-NaN, NaN flag},
+// which the caller reduces with MAX over the ranks in place; k_cfl_global then
+// takes dt from the global value exactly as k_cfl does from its own.
+__global__ void __launch_bounds__(1024) k_vmax_local(const double* __restrict__ blockmax, const StepConst sc, const DevClock* clk,
+                                                     double* xchg) {
+  const bool active = (clk->t < sc.tmax) && (clk->nn < sc.nnmax);
+  double v = 0.0;
+  if (active)
+    for (int b = threadIdx.x; b < sc.nblocksA; b += 1024) v = nanmax(v, blockmax[b]);
+  const double vmax = block_nanmax<1024>(v);
+  if (threadIdx.x == 0) {
+    const bool nan = !(vmax == vmax);
+    xchg[0] = nan ? 0.0 : vmax;
+    xchg[1] = nan ? 1.0 : 0.0;
+  }
+}
+__global__ void k_cfl_global(const double* xchg, const StepConst sc, DevClock* clk) {
+  const bool active = (clk->t < sc.tmax) && (clk->nn < sc.nnmax);
+  if (!active) { clk->active = 0; return; }
+  const double vmax = xchg[1] > 0.0 ? __longlong_as_double(0x7ff8000000000000LL) : xchg[0];
+  if (!(vmax == vmax) || isinf(vmax)) { if (clk->status == 0) clk->status = (int)(clk->nn + 1); }
+  double dt = jmin(sc.CFL * jmin(jmin(sc.dx, sc.dy), sc.dz) / vmax, jmin(sc.dtmax, sc.Kn));
+  dt = jmin(dt, sc.tmax - clk->t);
+  clk->vmax = vmax;
+  clk->dt = dt;
+  clk->t = clk->t + dt;
+  clk->nn = clk->nn + 1;
+  clk->active = 1;
+}
+
 // pas_HLL along one line of Np cells (stride `st`, line start `base`) for the
 // cell at position i of the line.  Its update reads the clamped cell ip and
 // its two neighbours only (cells L = ip-1, C = ip, R = ip+1); everything
@@ -275,6 +306,10 @@ struct hyq_ctx {
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // the step split at the CFL reduction (hyq_step_begin / hyq_step_end),
+  // captured on first use; xchg: the local / global max |speed| and NaN flag
+  cudaGraphExec_t exec_a = nullptr, exec_b = nullptr;
+  double* xchg = nullptr;
   // hyq_step_host: copy stream and per-slab events, made on first use
   cudaStream_t cstream = nullptr;
   std::vector<cudaEvent_t> up, down;
@@ -323,6 +358,37 @@ int capture_graph(hyq_ctx* ctx) {
   if ((e = cudaStreamEndCapture(ctx->stream, &ctx->graph)) != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
   if ((e = cudaGraphInstantiate(&ctx->exec, ctx->graph, 0)) != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
   return HYQ_OK;
+}
+
+// The two halves of a step around the CFL reduction, each as a graph.
+void enqueue_half_a(hyq_ctx* ctx, cudaStream_t s) {
+  launch_phase_A(ctx->sc, ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s, nullptr, 0, -1, &ctx->net);
+  k_vmax_local<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk, ctx->xchg);
+}
+void enqueue_half_b(hyq_ctx* ctx, cudaStream_t s) {
+  k_cfl_global<<<1, 1, 0, s>>>(ctx->xchg, ctx->sc, ctx->clk);
+  launch_diagnostics_speeds(ctx->vp, ctx->sc, ctx->clk, s);
+  k_hll<<<grid_of(ctx->N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
+  launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->clk, s);
+  launch_maxdiff(ctx->M, ctx->sc, ctx->clk, s);
+}
+int capture_one(hyq_ctx* ctx, void (*fn)(hyq_ctx*, cudaStream_t), cudaGraphExec_t* exec) {
+  cudaError_t e;
+  cudaGraph_t g = nullptr;
+  if (*exec) { cudaGraphExecDestroy(*exec); *exec = nullptr; }
+  if ((e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamBeginCapture");
+  fn(ctx, ctx->stream);
+  if ((e = cudaStreamEndCapture(ctx->stream, &g)) != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
+  return HYQ_OK;
+}
+int capture_halves(hyq_ctx* ctx) {
+  if (!ctx->xchg) HQ_CHECK(ctx, cudaMalloc((void**)&ctx->xchg, 2 * sizeof(double)));
+  int r = capture_one(ctx, enqueue_half_a, &ctx->exec_a);
+  if (r == HYQ_OK) r = capture_one(ctx, enqueue_half_b, &ctx->exec_b);
+  return r;
 }
 
 int net_status(hyq_ctx* ctx) {
@@ -471,6 +537,9 @@ void hyq_destroy(hyq_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->exec) cudaGraphExecDestroy(ctx->exec);
   if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  if (ctx->exec_a) cudaGraphExecDestroy(ctx->exec_a);
+  if (ctx->exec_b) cudaGraphExecDestroy(ctx->exec_b);
+  if (ctx->xchg) cudaFree(ctx->xchg);
   double* bufs[] = {ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax};
   for (double* b : bufs) if (b) cudaFree(b);
   if (ctx->clk) cudaFree(ctx->clk);
@@ -581,7 +650,55 @@ int hyq_set_wavespeed_net(hyq_ctx* ctx, const float* w, double margin) {
   ctx->sc.seed_margin = margin;
   // the margin is a kernel argument of the captured step
   if ((r = capture_graph(ctx)) != HYQ_OK) return r;
+  if (ctx->exec_a && (r = capture_halves(ctx)) != HYQ_OK) return r;
   ctx->net_loaded = true;
+  return HYQ_OK;
+}
+
+int hyq_set_spacing(hyq_ctx* ctx, double dx, double dy, double dz) {
+  if (!ctx) return fail(nullptr, HYQ_EINVAL, "null ctx");
+  if (!(dx > 0) || !(dy > 0) || !(dz > 0)) return fail(ctx, HYQ_EINVAL, "spacings must be positive");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  HQ_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->sc.dx = dx; ctx->sc.dy = dy; ctx->sc.dz = dz;
+  int r = capture_graph(ctx);
+  if (r == HYQ_OK && ctx->exec_a) r = capture_halves(ctx);
+  return r;
+}
+
+int hyq_step_begin(hyq_ctx* ctx, double* xchg) {
+  if (!ctx || !xchg) return fail(ctx, HYQ_EINVAL, "null argument");
+  if (ctx->sc.mode == MODE_LEARNED && !ctx->net_loaded)
+    return fail(ctx, HYQ_EINVAL, "HYQ_MODE_LEARNED needs the wave-speed network (hyq_set_wavespeed_net) before stepping");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  if (!ctx->exec_a) {
+    const int r = capture_halves(ctx);
+    if (r != HYQ_OK) return r;
+  }
+  HQ_CHECK(ctx, cudaGraphLaunch(ctx->exec_a, ctx->stream));
+  HQ_CHECK(ctx, cudaMemcpyAsync(xchg, ctx->xchg, 2 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  return HYQ_OK;
+}
+
+int hyq_step_end(hyq_ctx* ctx, const double* xchg) {
+  if (!ctx || !xchg) return fail(ctx, HYQ_EINVAL, "null argument");
+  if (!ctx->exec_b) return fail(ctx, HYQ_EINVAL, "hyq_step_end without hyq_step_begin");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  HQ_CHECK(ctx, cudaMemcpyAsync(ctx->xchg, xchg, 2 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  HQ_CHECK(ctx, cudaGraphLaunch(ctx->exec_b, ctx->stream));
+  return HYQ_OK;
+}
+
+int hyq_copy_layers(hyq_ctx* ctx, int32_t k0, int32_t nk, double* buf, int32_t into_state) {
+  if (!ctx || !buf || nk < 0 || k0 < 0 || k0 + nk > ctx->p.Nz) return fail(ctx, HYQ_EINVAL, "bad layer range");
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  const size_t layer = (size_t)ctx->p.Nx * ctx->p.Ny;
+  const size_t w = sizeof(double) * layer * (size_t)nk, pitch_state = sizeof(double) * (size_t)ctx->N;
+  double* st = ctx->M + layer * (size_t)k0;
+  if (into_state)
+    HQ_CHECK(ctx, cudaMemcpy2DAsync(st, pitch_state, buf, w, w, 35, cudaMemcpyDeviceToDevice, ctx->stream));
+  else
+    HQ_CHECK(ctx, cudaMemcpy2DAsync(buf, w, st, pitch_state, w, 35, cudaMemcpyDeviceToDevice, ctx->stream));
   return HYQ_OK;
 }
 

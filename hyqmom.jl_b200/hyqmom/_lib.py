@@ -56,7 +56,7 @@ SYMBOLS = ["hyq_abi_version", "hyq_create", "hyq_destroy", "hyq_last_error", "hy
            "hyq_cells_eigenvalues", "hyq_cells_closure_eigs", "hyq_cells_collision", "hyq_cells_phase_A", "hyq_step_noalloc", "hyq_batch_create", "hyq_batch_destroy", "hyq_batch_size",
            "hyq_batch_member", "hyq_batch_stream", "hyq_batch_advance_async", "hyq_batch_advance", "hyq_reset_counters",
            "hyq_set_wavespeed_net", "hyq_net_image_bytes", "hyq_net_tile_bytes", "hyq_net_scratch_bytes", "hyq_net_pack",
-           "hyq_net_features", "hyq_net_forward", "hyq_net_train_batch", "hyq_net_adam", "hyq_cells_wavespeed_targets", "hyq_set_state_ic"]
+           "hyq_net_features", "hyq_net_forward", "hyq_net_train_batch", "hyq_net_adam", "hyq_cells_wavespeed_targets", "hyq_set_state_ic", "hyq_step_begin", "hyq_step_end", "hyq_copy_layers", "hyq_set_spacing"]
 NOALLOC_MAX_CELLS = 16384  # HYQ_NOALLOC_MAX_CELLS
 
 
@@ -119,6 +119,10 @@ def load(path=None):
     lib.hyq_net_adam.argtypes = [vp, vp, vp, vp, i32, flt, flt, flt, flt, flt, i32, vp, vp]
     lib.hyq_cells_wavespeed_targets.argtypes = [vp, i64, i32, dbl, i32, vp, vp, vp]
     lib.hyq_set_state_ic.argtypes = [vp, vp, vp, vp, dbl, dbl, dbl, vp, i32, vp, vp]
+    lib.hyq_step_begin.argtypes = [vp, vp]
+    lib.hyq_step_end.argtypes = [vp, vp]
+    lib.hyq_copy_layers.argtypes = [vp, i32, i32, vp, i32]
+    lib.hyq_set_spacing.argtypes = [vp, dbl, dbl, dbl]
     _lib = lib
     return lib
 

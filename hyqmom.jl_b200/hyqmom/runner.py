@@ -84,11 +84,12 @@ class Solver:
         assert M.shape == self.shape
         self._chk(self._lib.hyq_set_state(self._h, M.ctypes.data))
 
-    def set_state_ic(self, params=None):
+    def set_state_ic(self, params=None, tables=None):
         """Generate the initial condition of `params` (default: the solver's)
-        on the device (hyq_set_state_ic); equal bit for bit to ic.initial_state."""
+        on the device (hyq_set_state_ic); equal bit for bit to ic.initial_state.
+        tables: ic.ic_tables output to use instead (a slab's layers)."""
         p = self.params if params is None else params
-        xm, ym, zm, dx, dy, dz, bg, regions, moments = _ic.ic_tables(p)
+        xm, ym, zm, dx, dy, dz, bg, regions, moments = tables if tables is not None else _ic.ic_tables(p)
         n = len(regions)
         arr = (_lib.HyqIcRegion * max(n, 1))()
         for q, (kind, every, lo, hi, idx) in enumerate(regions):

@@ -106,6 +106,32 @@ int hyq_create(const hyq_params* p, hyq_ctx** out);
 void hyq_destroy(hyq_ctx* ctx);
 const char* hyq_last_error(const hyq_ctx* ctx);
 
+/* ---- a domain decomposed into z-slabs (one context per slab) -------------
+ * No reference counterpart as an API: replaces the rank-local parts of the
+ * reference's MPI step (src/mpi/halo_exchange_3d.jl:26-122, the dt
+ * all-reduce at src/simulation_runner.jl:403).  A slab context holds its
+ * own z-layers plus two ghost layers on each side that has a neighbour, and
+ * steps in two halves around the CFL reduction:
+ *   hyq_step_begin: phase [A] on every local layer (ghosts included: their
+ *     inputs are the neighbour's pre-step layers, so they reproduce the
+ *     neighbour's results bit for bit) and the local max |speed|, written to
+ *     the device buffer *xchg = {max |speed| over non-NaN cells, NaN flag};
+ *     the caller reduces it with MAX over the slabs in place (e.g. an NCCL
+ *     all-reduce on the context's stream, hyq_stream) before
+ *   hyq_step_end: dt from the global value, then the HLL sweeps (each owned
+ *     layer is at least two layers from the local ends, so the serial
+ *     boundary rules there touch only ghosts), phases [E]+[F].
+ * The slabs' owned layers then equal the single-domain step bit for bit.
+ * hyq_copy_layers copies z-layers [k0, k0 + nk) of all 35 moment planes
+ * between the state and a packed device buffer (35 planes of nk Nx Ny
+ * doubles; into_state = 1 writes the state), on the context's stream, for
+ * the ghost exchange.  hyq_set_spacing overrides dx, dy, dz (the slab's
+ * extents then need not divide exactly). */
+int hyq_step_begin(hyq_ctx* ctx, double* xchg);
+int hyq_step_end(hyq_ctx* ctx, const double* xchg);
+int hyq_copy_layers(hyq_ctx* ctx, int32_t k0, int32_t nk, double* buf, int32_t into_state);
+int hyq_set_spacing(hyq_ctx* ctx, double dx, double dy, double dz);
+
 /* Host (Nx,Ny,Nz,35) column-major buffers; time and step count reset to 0
  * by hyq_set_state (simulation_runner's t = 0.0; nn = 0, :333-334). */
 int hyq_set_state(hyq_ctx* ctx, const double* M);

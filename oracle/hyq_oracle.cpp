@@ -254,18 +254,29 @@ void hyqo_s4toc4_r(const double* C2, const double* Scube, double* Ccube) {
 // vmax_out (optional): the CFL wave speed of the step.
 static inline size_t at(const Params& P, int i, int j, int k) { return size_t(i) + size_t(P.Nx) * (size_t(j) + size_t(P.Ny) * size_t(k)); }
 
-double hyqo_step(int Nx, int Ny, int Nz, double* M, double Kn, double Ma, int flag2D, double CFL, double dtmax, double tmax,
-                 double dx, double dy, double dz, int positivity, double* t, double* vmax_out) {
-  Params P{Nx, Ny, Nz, flag2D, positivity, Kn, Ma, CFL, dtmax, tmax, dx, dy, dz};
-  const size_t N = size_t(Nx) * Ny * Nz;
-  std::vector<double> Fx(N * 35), Fy(N * 35), Fz(N * 35), Mnp(N * 35), vp(N * 6);
+// The step in two halves around the CFL reduction (a slab of a decomposed
+// domain calls them with the global max |speed| in between): begin runs
+// phase [A] and returns the work state and the local NaN-propagating max.
+struct StepWork {
+  Params P;
+  size_t N;
+  std::vector<double> Fx, Fy, Fz, vp;
+};
+
+void* hyqo_step_begin(int Nx, int Ny, int Nz, double* M, double Kn, double Ma, int flag2D, double CFL, double dtmax, double tmax,
+                      double dx, double dy, double dz, int positivity, double* vmax_local) {
+  StepWork* w = new StepWork{Params{Nx, Ny, Nz, flag2D, positivity, Kn, Ma, CFL, dtmax, tmax, dx, dy, dz}, size_t(Nx) * Ny * Nz, {}, {}, {}, {}};
+  const Params& P = w->P;
+  const size_t N = w->N;
+  w->Fx.resize(N * 35); w->Fy.resize(N * 35); w->Fz.resize(N * 35); w->vp.resize(N * 6);
+  std::vector<double> Mnp(N * 35);
 #pragma omp parallel for schedule(dynamic, 16)
   for (long long c = 0; c < (long long)N; ++c) {
     double m[35], fx[35], fy[35], fz[35], mr[35], v[6];
     for (int n = 0; n < 35; ++n) m[n] = M[c + N * n];
     phase_A<double>(m, P, fx, fy, fz, mr, v);
-    for (int n = 0; n < 35; ++n) { Fx[c + N * n] = fx[n]; Fy[c + N * n] = fy[n]; Fz[c + N * n] = fz[n]; Mnp[c + N * n] = mr[n]; }
-    for (int q = 0; q < 6; ++q) vp[c + N * q] = v[q];
+    for (int n = 0; n < 35; ++n) { w->Fx[c + N * n] = fx[n]; w->Fy[c + N * n] = fy[n]; w->Fz[c + N * n] = fz[n]; Mnp[c + N * n] = mr[n]; }
+    for (int q = 0; q < 6; ++q) w->vp[c + N * q] = v[q];
   }
   for (size_t q = 0; q < N * 35; ++q) M[q] = Mnp[q];
   // vmax = maximum(|vp*|) over all six arrays, NaN-propagating
@@ -273,36 +284,46 @@ double hyqo_step(int Nx, int Ny, int Nz, double* M, double Kn, double Ma, int fl
   bool first = true;
   for (int q = 0; q < 6; ++q)
     for (size_t c = 0; c < N; ++c) {
-      double a = std::fabs(vp[c + N * q]);
+      double a = std::fabs(w->vp[c + N * q]);
       vmax = first ? a : jmax(vmax, a);
       first = false;
     }
-  double dt = jmin(CFL * jmin(jmin(dx, dy), dz) / vmax, jmin(dtmax, Kn));
-  dt = jmin(dt, tmax - *t);
+  *vmax_local = vmax;
+  return w;
+}
+
+// dt from vmax, the HLL sweeps, phases [E]+[F]; frees the work state.
+double hyqo_step_end(void* work, double* M, double vmax, double* t) {
+  StepWork* w = static_cast<StepWork*>(work);
+  const Params& P = w->P;
+  const size_t N = w->N;
+  const int Nx = P.Nx, Ny = P.Ny, Nz = P.Nz;
+  const double dx = P.dx, dy = P.dy, dz = P.dz;
+  double dt = jmin(P.CFL * jmin(jmin(dx, dy), dz) / vmax, jmin(P.dtmax, P.Kn));
+  dt = jmin(dt, P.tmax - *t);
   *t = *t + dt;
-  if (vmax_out) *vmax_out = vmax;
   // HLL sweeps (src/numerics/apply_flux_update_3d.jl:30-213)
   std::vector<double> Mx(M, M + N * 35), My(M, M + N * 35), Mz(M, M + N * 35);
   const int ms = int(N);
+  double* vp = w->vp.data();
 #pragma omp parallel for schedule(static)
   for (int jk = 0; jk < Ny * Nz; ++jk) {
     int j = jk % Ny, k = jk / Ny;
     size_t o = at(P, 0, j, k);
-    pas_HLL_row<double>(Nx, M + o, Fx.data() + o, 1, ms, vp.data() + o, vp.data() + N + o, 1, dt, dx, Mx.data() + o);
+    pas_HLL_row<double>(Nx, M + o, w->Fx.data() + o, 1, ms, vp + o, vp + N + o, 1, dt, dx, Mx.data() + o);
   }
 #pragma omp parallel for schedule(static)
   for (int ik = 0; ik < Nx * Nz; ++ik) {
     int i = ik % Nx, k = ik / Nx;
     size_t o = at(P, i, 0, k);
-    pas_HLL_row<double>(Ny, M + o, Fy.data() + o, Nx, ms, vp.data() + 2 * N + o, vp.data() + 3 * N + o, Nx, dt, dy, My.data() + o);
+    pas_HLL_row<double>(Ny, M + o, w->Fy.data() + o, Nx, ms, vp + 2 * N + o, vp + 3 * N + o, Nx, dt, dy, My.data() + o);
   }
   if (Nz > 1) {
 #pragma omp parallel for schedule(static)
     for (int ij = 0; ij < Nx * Ny; ++ij) {
       int i = ij % Nx, j = ij / Nx;
       size_t o = at(P, i, j, 0);
-      pas_HLL_row<double>(Nz, M + o, Fz.data() + o, Nx * Ny, ms, vp.data() + 4 * N + o, vp.data() + 5 * N + o, Nx * Ny, dt, dz,
-                          Mz.data() + o);
+      pas_HLL_row<double>(Nz, M + o, w->Fz.data() + o, Nx * Ny, ms, vp + 4 * N + o, vp + 5 * N + o, Nx * Ny, dt, dz, Mz.data() + o);
     }
   }
   for (size_t q = 0; q < N * 35; ++q) M[q] = Mx[q] + My[q] + Mz[q] - 2.0 * M[q];
@@ -312,15 +333,21 @@ double hyqo_step(int Nx, int Ny, int Nz, double* M, double Kn, double Ma, int fl
     double m[35], r[35], o[35];
     for (int n = 0; n < 35; ++n) m[n] = M[c + N * n];
     phase_E<double>(m, P, r);
-    collision35<double>(r, dt, Kn, positivity != 0, o);
+    collision35<double>(r, dt, P.Kn, P.positivity != 0, o);
     for (int n = 0; n < 35; ++n) M[c + N * n] = o[n];
   }
+  delete w;
   return dt;
 }
 
-// Per-cell FP64 operation counts of the plain path for the given state and
-// dt: out[0] = phase [A] ops, out[1] = phase [E]+[F] ops (summed over cells),
-// out[2] = HLL ops per interior cell (the three sweeps and the combination).
+double hyqo_step(int Nx, int Ny, int Nz, double* M, double Kn, double Ma, int flag2D, double CFL, double dtmax, double tmax,
+                 double dx, double dy, double dz, int positivity, double* t, double* vmax_out) {
+  double vmax = 0.0;
+  void* w = hyqo_step_begin(Nx, Ny, Nz, M, Kn, Ma, flag2D, CFL, dtmax, tmax, dx, dy, dz, positivity, &vmax);
+  if (vmax_out) *vmax_out = vmax;
+  return hyqo_step_end(w, M, vmax, t);
+}
+
 void hyqo_count_ops(int Nx, int Ny, int Nz, const double* M, double Kn, double Ma, int flag2D, int positivity, double dt,
                     double* out) {
   Params P{Nx, Ny, Nz, flag2D, positivity, Kn, Ma, 0, 0, 0, 0, 0, 0};

@@ -34,6 +34,11 @@ def load():
         [ctypes.c_double] * 6 + [ctypes.c_int, _dp, _dp]
     lib.hyqo_delta2starchol_L3.restype = ctypes.c_double
     lib.hyqo_eig6.restype = ctypes.c_int
+    lib.hyqo_step_begin.restype = ctypes.c_void_p
+    lib.hyqo_step_begin.argtypes = [ctypes.c_int] * 3 + [_dp] + [ctypes.c_double] * 2 + [ctypes.c_int] + \
+        [ctypes.c_double] * 6 + [ctypes.c_int, _dp]
+    lib.hyqo_step_end.restype = ctypes.c_double
+    lib.hyqo_step_end.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double, _dp]
     lib.hyqo_set_threads.argtypes = [ctypes.c_int]
     lib.hyqo_set_threads.restype = None
     _lib = lib
@@ -165,6 +170,24 @@ def step(M, params, t):
     dt = load().hyqo_step(Nx, Ny, Nz, M.ctypes.data_as(_dp), p["Kn"], p["Ma"], int(p["flag2D"]), p["CFL"], p["dtmax"],
                           p["tmax"], p["dx"], p["dy"], p["dz"], int(p.get("positivity", True)), _p(tt), _p(vm))
     return dt, float(tt[0]), float(vm[0])
+
+
+def step_begin(M, params):
+    """Phase [A] of a step on M in place; returns (work handle, local vmax)."""
+    assert M.flags["F_CONTIGUOUS"] and M.dtype == np.float64
+    Nx, Ny, Nz, _ = M.shape
+    vm = np.zeros(1)
+    p = params
+    w = load().hyqo_step_begin(Nx, Ny, Nz, M.ctypes.data_as(_dp), p["Kn"], p["Ma"], int(p["flag2D"]), p["CFL"], p["dtmax"],
+                               p["tmax"], p["dx"], p["dy"], p["dz"], int(p.get("positivity", True)), _p(vm))
+    return w, float(vm[0])
+
+
+def step_end(work, M, vmax, t):
+    """The rest of the step with the (global) vmax; returns (dt, t_new)."""
+    tt = np.array([t], dtype=np.float64)
+    dt = load().hyqo_step_end(ctypes.c_void_p(work), M.ctypes.data_as(_dp), float(vmax), _p(tt))
+    return dt, float(tt[0])
 
 
 def count_ops_stages(M, params, dt):
