@@ -30,9 +30,12 @@
 // data) is NOT certified, and the caller falls back to the LAPACK-path
 // eigen-solve, which decides as the reference does.
 //
-// Arithmetic is plain FP64 (+, -, *, /, sqrt) in a fixed order, compiled
-// without contraction on both the device and the host, so the host build of
-// this header gives the device's bits.
+// Arithmetic is FP64 in a fixed order: the Horner, Taylor-shift and
+// deflation recurrences use explicit fused multiply-adds (fma, correctly
+// rounded on the device and in the host's std::fma), everything else plain
+// operations compiled without contraction, so the host build of this header
+// gives the device's bits.  (The fused operations are this solve's own: its
+// results are compared with the LAPACK path to round-off, not bit for bit.)
 #pragma once
 
 namespace hyq {
@@ -51,6 +54,20 @@ constexpr double ROOT_BOUND = 2.25;    // |x| <= sqrt(5) when all roots are real
 // 1e-16 moves a close pair by about its square root, 1e-8) cannot make the
 // pair complex.
 constexpr double GAP_VAL = 1e-9;
+// With converged interior roots, the smallest computed gap accepted
+// (normalised): a pair that close stays real under LAPACK's rounding, which
+// moves a near-double pair by about sqrt(eps |J|) ~ 1e-8.
+constexpr double GAP_MIN = 1e-6;
+// The extremes must also be well conditioned: the Horner rounding bound of
+// b at the root over |b'| (the first-order error of the computed root) at
+// most EXT_ERR (normalised).  An extreme in a tight cluster has a small b'
+// and an error far above round-off, in this solve and in the LAPACK path
+// alike, so the two would differ by more than round-off; such Jacobians go
+// to the LAPACK path.
+#ifndef HQ_CP_EXT_ERR
+#define HQ_CP_EXT_ERR 2e-13
+#endif
+constexpr double EXT_ERR = HQ_CP_EXT_ERR;
 
 // c[0..6] (c[6] = 1) of det(lam I - J), J given by its rows 2 (r3), 4 (r5)
 // and 5 (r6); rows 0, 1, 3 are the unit rows of jacobian6.
@@ -106,8 +123,8 @@ template <int N> HQD void horner2(const double* d, double x, double& p, double& 
   dp = 0.0;
 #pragma unroll
   for (int k = N - 1; k >= 0; --k) {
-    dp = dp * x + p;
-    p = p * x + d[k];
+    dp = fma(dp, x, p);
+    p = fma(p, x, d[k]);
   }
 }
 
@@ -124,7 +141,7 @@ HQD bool normalize(const double (&c)[7], double& s, double& sig, double (&b)[7])
 #pragma unroll
   for (int i = 0; i < 6; ++i)
 #pragma unroll
-    for (int k = 5; k >= i; --k) a[k] = a[k] + s * a[k + 1];
+    for (int k = 5; k >= i; --k) a[k] = fma(s, a[k + 1], a[k]);
   const double v = (a[5] * a[5] - 2.0 * a[4]) / 6.0;
   if (!(v > 0.0) || !(v < 1.79769313486231571e308)) return false;
   sig = sqrt(v);
@@ -187,7 +204,7 @@ HQD double polish(const double (&b)[7], double x, int& its) {
 template <int N> HQD void deflate(const double* d, double x, double* q) {
   q[N - 1] = d[N];
 #pragma unroll
-  for (int k = N - 1; k >= 1; --k) q[k - 1] = d[k] + x * q[k];
+  for (int k = N - 1; k >= 1; --k) q[k - 1] = fma(x, q[k], d[k]);
 }
 
 // Sign of b at y certified against its Horner rounding error and against
@@ -197,7 +214,7 @@ HQD int certified_sign(const double (&b)[7], double y, double floor_val) {
   const double ay = fabs(y);
 #pragma unroll
   for (int k = 5; k >= 0; --k) {
-    p = p * y + b[k];
+    p = fma(p, y, b[k]);
     bound = bound * ay + fabs(b[k]);
   }
   const double err = jmax(CERT_ERR * bound, floor_val);
@@ -224,6 +241,65 @@ struct CpOut {
 // The extremes are converged to full precision; the four interior roots only
 // need to lie within their gaps (they place the separating points), so their
 // Newton iterations stop early and the last two come from the quadratic.
+// The four interior roots of b between the extremes x6 < x1 (searched by
+// Newton to tolerance `tol`, the last two from the quadratic) and the
+// certificate.  tight = false: interior roots only placed (tol loose), the
+// interior sign values must exceed GAP_VAL (a rigorous lower bound on every
+// gap); tight = true: interior roots converged, their computed gaps must be
+// at least GAP_MIN and the signs only beyond the rounding bound.
+HQD bool interior_certify(const double (&b)[7], double x1, double x6, bool tight, int& its) {
+  double d5[6], d4[5], d3[4], d2[3];
+  deflate<6>(b, x1, d5);
+  deflate<5>(d5, x6, d4);
+  const double tol = tight ? NEWTON_TOL : LOOSE_TOL;
+  // each interior search starts from the upper bound mean + sqrt((n-1) var)
+  // of the deflated polynomial's roots (read off its monic coefficients)
+  // when that is below the previous root
+  double x2 = jmin(x1, upper_bound<4>(d4));
+  if (!newton<4>(d4, x2, tol, its)) return false;
+  if (tight) x2 = polish(b, x2, its);
+  deflate<4>(d4, x2, d3);
+  double x3 = jmin(x2, upper_bound<3>(d3));
+  if (!newton<3>(d3, x3, tol, its)) return false;
+  if (tight) x3 = polish(b, x3, its);
+  deflate<3>(d3, x3, d2);
+  // the last two from the quadratic, in the cancellation-free form
+  const double disc = d2[1] * d2[1] - 4.0 * d2[2] * d2[0];
+  if (!(disc > 0.0)) return false;
+  const double sq = sqrt(disc);
+  const double qq = -0.5 * (d2[1] + (d2[1] < 0.0 ? -sq : sq));
+  if (!(qq != 0.0)) return false;
+  double x4 = qq / d2[2], x5 = d2[0] / qq;
+  if (tight) {
+    x4 = polish(b, x4, its);
+    x5 = polish(b, x5, its);
+  }
+  // ascending order of the interior four (a sorting network); the extremes
+  // must lie outside them
+  double r[6] = {x6, x5, x4, x3, x2, x1};
+  cswap(r[1], r[2]); cswap(r[3], r[4]);
+  cswap(r[1], r[3]); cswap(r[2], r[4]);
+  cswap(r[2], r[3]);
+  if (!(r[0] < r[1] && r[4] < r[5])) return false;
+  bool ok = true;
+  if (tight) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) ok = ok && (r[k + 1] - r[k] >= GAP_MIN);
+    if (!ok) return false;
+  }
+  // alternating certified signs at the seven separating points
+  double y[7];
+  y[0] = r[0] - 0.5 * (r[1] - r[0]);
+#pragma unroll
+  for (int k = 1; k < 6; ++k) y[k] = 0.5 * (r[k - 1] + r[k]);
+  y[6] = r[5] + 0.5 * (r[5] - r[4]);
+#pragma unroll
+  for (int k = 0; k < 7; ++k)
+    ok = ok && (certified_sign(b, y[k], (k == 0 || k == 6 || tight) ? 0.0 : GAP_VAL) == ((k & 1) ? -1 : 1));
+  its += 7;
+  return ok;
+}
+
 HQD CpOut solve(const double (&b)[7], double xhi, double xlo) {
   CpOut o;
   o.ok = false;
@@ -233,77 +309,54 @@ HQD CpOut solve(const double (&b)[7], double xhi, double xlo) {
   if (!newton<6>(b, x1, NEWTON_TOL, o.its)) return o;
   if (!newton<6>(b, x6, NEWTON_TOL, o.its)) return o;
   if (!(x6 < x1)) return o;
-  double d5[6], d4[5], d3[4], d2[3];
-  deflate<6>(b, x1, d5);
-  deflate<5>(d5, x6, d4);
-  // each interior search starts from the upper bound mean + sqrt((n-1) var)
-  // of the deflated polynomial's roots (read off its monic coefficients)
-  // when that is below the previous root
-  double x2 = jmin(x1, upper_bound<4>(d4));
-  if (!newton<4>(d4, x2, LOOSE_TOL, o.its)) return o;
-  deflate<4>(d4, x2, d3);
-  double x3 = jmin(x2, upper_bound<3>(d3));
-  if (!newton<3>(d3, x3, LOOSE_TOL, o.its)) return o;
-  deflate<3>(d3, x3, d2);
-  // the last two from the quadratic, in the cancellation-free form
-  const double disc = d2[1] * d2[1] - 4.0 * d2[2] * d2[0];
-  if (!(disc > 0.0)) return o;
-  const double sq = sqrt(disc);
-  const double qq = -0.5 * (d2[1] + (d2[1] < 0.0 ? -sq : sq));
-  if (!(qq != 0.0)) return o;
-  const double x4 = qq / d2[2], x5 = d2[0] / qq;
-  // ascending order of the interior four (a sorting network); the extremes
-  // must lie outside them
-  double r[6] = {x6, x5, x4, x3, x2, x1};
-  cswap(r[1], r[2]); cswap(r[3], r[4]);
-  cswap(r[1], r[3]); cswap(r[2], r[4]);
-  cswap(r[2], r[3]);
-  if (!(r[0] < r[1] && r[4] < r[5])) return o;
-  // certificate: alternating certified signs at the seven separating
-  // points, the interior five also above GAP_VAL
-  double y[7];
-  y[0] = r[0] - 0.5 * (r[1] - r[0]);
-#pragma unroll
-  for (int k = 1; k < 6; ++k) y[k] = 0.5 * (r[k - 1] + r[k]);
-  y[6] = r[5] + 0.5 * (r[5] - r[4]);
+  // interior roots placed loosely first; a cluster (a near-double interior
+  // pair, common in nearly Gaussian cells) needs them converged
+  if (!interior_certify(b, x1, x6, false, o.its) && !interior_certify(b, x1, x6, true, o.its)) return o;
+  // conditioning of the two extremes
   bool ok = true;
 #pragma unroll
-  for (int k = 0; k < 7; ++k) ok = ok && (certified_sign(b, y[k], (k == 0 || k == 6) ? 0.0 : GAP_VAL) == ((k & 1) ? -1 : 1));
-  o.its += 7;
+  for (int q = 0; q < 2; ++q) {
+    const double x = q ? x1 : x6;
+    double p = b[6], dp = 0.0, bound = 1.0;
+    const double ax = fabs(x);
+#pragma unroll
+    for (int k = 5; k >= 0; --k) {
+      dp = fma(dp, x, p);
+      p = fma(p, x, b[k]);
+      bound = bound * ax + fabs(b[k]);
+    }
+    ok = ok && (CERT_ERR * bound <= EXT_ERR * fabs(dp));
+  }
+  o.its += 2;
   if (!ok) return o;
-  o.xmin = r[0];
-  o.xmax = r[5];
+  o.xmin = x6;
+  o.xmax = x1;
   o.ok = true;
   return o;
 }
 
-// A seed (in the normalised variable) is used when the polynomial and its
-// first two derivatives have the signs they have outside the roots (b is
-// monic of even degree): b, b', b'' > 0 above the largest root; b > 0,
-// b' < 0, b'' > 0 below the smallest.  Otherwise, and for NaN seeds, the
-// bound is used.  (A seed that passes and is still inside the spectrum only
-// costs a failed certificate.)
-HQD void horner3(const double (&b)[7], double x, double& p, double& dp, double& ddp) {
-  p = b[6];
-  dp = 0.0;
-  ddp = 0.0;
+// A seed x (in the normalised variable) is used as the start of the search
+// for the largest root when b has no root at or above it: the coefficients of
+// b(x + y) as a polynomial in y (the Taylor coefficients b^(k)(x) / k!) are
+// all positive, so by Descartes' rule b(x + y) has no positive root.  For the
+// smallest root the coefficients of b(x - y) must all be positive.  Otherwise
+// (and for NaN seeds) the search starts from the bound, so a poor prediction
+// costs a few evaluations and never a wrong start.
+HQD bool taylor_signs(const double (&b)[7], double x, bool above) {
+  double t[7];
 #pragma unroll
-  for (int k = 5; k >= 0; --k) {
-    ddp = ddp * x + dp;
-    dp = dp * x + p;
-    p = p * x + b[k];
-  }
+  for (int k = 0; k < 7; ++k) t[k] = b[k];
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+#pragma unroll
+    for (int k = 5; k >= i; --k) t[k] = fma(x, t[k + 1], t[k]);
+  bool ok = x == x && fabs(x) < 8.0;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) ok = ok && ((above || (k & 1) == 0) ? t[k] > 0.0 : t[k] < 0.0);
+  return ok;
 }
-HQD double start_above(const double (&b)[7], double x) {
-  double p, dp, ddp;
-  horner3(b, x, p, dp, ddp);
-  return (p > 0.0 && dp > 0.0 && ddp > 0.0 && x < 8.0) ? x : ROOT_BOUND + fabs(b[5]);
-}
-HQD double start_below(const double (&b)[7], double x) {
-  double p, dp, ddp;
-  horner3(b, x, p, dp, ddp);
-  return (p > 0.0 && dp < 0.0 && ddp > 0.0 && x > -8.0) ? x : -ROOT_BOUND - fabs(b[5]);
-}
+HQD double start_above(const double (&b)[7], double x) { return taylor_signs(b, x, true) ? x : ROOT_BOUND + fabs(b[5]); }
+HQD double start_below(const double (&b)[7], double x) { return taylor_signs(b, x, false) ? x : -ROOT_BOUND - fabs(b[5]); }
 
 // Extreme eigenvalues of the flux Jacobian (rows r3, r5, r6) when certified.
 // lo_seed, hi_seed: predicted extreme eigenvalues (NaN for none); margin: the

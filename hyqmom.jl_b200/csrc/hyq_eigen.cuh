@@ -658,13 +658,13 @@ HQN void eigenvalues6_corrected(const double* M, int axis, int planes, int flag2
 // test; phase E only needs the corrected moments, so its kernels decide here
 // and leave the corrections to a separate pass over the flagged cells.
 // -1 when MODE defers a Jacobian (JAC_P1).
-template <int MODE> HQN int eigenvalues6_flags_t(const double* M, int axis, long long ist) {
+template <int MODE> HQN int eigenvalues6_flags_t(const double* M, int axis, long long ist, const Seeds sd = no_seeds()) {
   const int sa = axis == 1 ? 0 : 1, sb = axis == 1 ? 2 : 3;
   double a[15], b[15];
   for (int n = 0; n < 15; ++n) { a[n] = M[SLICE[sa][n] * ist]; b[n] = M[SLICE[sb][n] * ist]; }
-  const EigOut ea = jac_eigs_t<MODE>(a);
+  const EigOut ea = jac_eigs_t<MODE>(a, sd);
   if (ea.deferred) return -1;
-  const EigOut eb = jac_eigs_t<MODE>(b);
+  const EigOut eb = jac_eigs_t<MODE>(b, sd);
   if (eb.deferred) return -1;
   const double thr = 1000.0 * EPS;
   return (ea.imax > thr ? 1 : 0) | (eb.imax > thr ? 2 : 0);

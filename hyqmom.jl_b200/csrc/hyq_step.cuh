@@ -153,6 +153,29 @@ void launch_wavespeed_seeds(const StepConst& sc, const double* Mr, const WaveNet
 
 }  // namespace hyqk
 
+#if defined(__CUDACC__) && defined(HQ_SEEDS)
+namespace hyqk {
+// The learned path's seeds of plane Jacobians along `axis` for cell c: the
+// network's standardized extreme speeds mapped back with the stage input's
+// mean velocity and variance along the axis (NaN seeds when there are none).
+__device__ __forceinline__ hyq::Seeds stage_seeds(const double* in, long long c, int axis, const StepConst& sc) {
+  if (!sc.seeds) return hyq::no_seeds();
+  const long long N = sc.N;
+  const int iu = axis == 1 ? 1 : (axis == 2 ? 5 : 15), i2 = axis == 1 ? 2 : (axis == 2 ? 9 : 19);
+  const double m0 = in[c], mu = in[c + N * iu] / m0;
+  const double var = in[c + N * i2] / m0 - mu * mu;
+  const double sd = sqrt(var > 0.0 ? var : 0.0);
+  const float* sp = sc.seeds + 2 * (axis - 1) * N + c;
+  hyq::Seeds s;
+  s.lo = mu + sd * (double)sp[0];
+  s.hi = mu + sd * (double)sp[N];
+  s.margin = sc.seed_margin;
+  return s;
+}
+
+}  // namespace hyqk
+#endif
+
 #ifdef __CUDACC__
 namespace hyqk {
 __device__ __forceinline__ double nanmax(double a, double b) { return (a != a) ? a : ((b != b) ? b : fmax(a, b)); }

@@ -4,6 +4,7 @@
 // 1-D closure speeds; a NaN-propagating block max of |speed| feeds the CFL
 // reduction.
 #include "hyq_eigen.cuh"
+#define HQ_SEEDS
 #include "hyq_step.cuh"
 
 using namespace hyq;
@@ -63,24 +64,6 @@ __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure(const double*
   if (c == c0) { unsigned int* cnt = defer_list(vp, N) + N; cnt[0] = 0; cnt[1] = 0; cnt[2] = 0; }
   if (c >= c1) return;
   flux_closure35(M + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
-}
-
-// The learned path's seeds of plane Jacobians along `axis` for cell c: the
-// network's standardized extreme speeds mapped back with the stage input's
-// mean velocity and variance along the axis (NaN seeds when there are none).
-__device__ __forceinline__ Seeds stage_seeds(const double* in, long long c, int axis, const StepConst& sc) {
-  if (!sc.seeds) return no_seeds();
-  const long long N = sc.N;
-  const int iu = axis == 1 ? 1 : (axis == 2 ? 5 : 15), i2 = axis == 1 ? 2 : (axis == 2 ? 9 : 19);
-  const double m0 = in[c], mu = in[c + N * iu] / m0;
-  const double var = in[c + N * i2] / m0 - mu * mu;
-  const double sd = sqrt(var > 0.0 ? var : 0.0);
-  const float* sp = sc.seeds + 2 * (axis - 1) * N + c;
-  Seeds s;
-  s.lo = mu + sd * (double)sp[0];
-  s.hi = mu + sd * (double)sp[N];
-  s.margin = sc.seed_margin;
-  return s;
 }
 
 // eigenvalues6_hyperbolic_3D along x (axis 1) or y (axis 2), and

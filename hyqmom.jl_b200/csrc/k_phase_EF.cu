@@ -1,6 +1,7 @@
 // Phases [E] realizability and [F] BGK collision of the step
 // (src/simulation_runner.jl:526-557), per cell, out of place.
 #include "hyq_eigen.cuh"
+#define HQ_SEEDS
 #include "hyq_step.cuh"
 
 using namespace hyq;
@@ -58,7 +59,9 @@ __global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* in, dou
   }
   const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
   if (c >= c1) return;
-  const int planes = dense ? 0 : eigenvalues6_flags_t<JM>(in + c, axis, N);
+  // the learned path seeds the certified solve with the network's speeds of
+  // this step (predicted in phase [A]; a poor seed only costs evaluations)
+  const int planes = dense ? 0 : eigenvalues6_flags_t<JM>(in + c, axis, N, JM == JAC_CP ? stage_seeds(in, c, axis, sc) : no_seeds());
   if (JM == JAC_CP && !dense) count_flag_ef(planes < 0, &clk->fb_cells);
   if (out != in) {
 #pragma unroll

@@ -261,11 +261,12 @@ struct StepWork {
   Params P;
   size_t N;
   std::vector<double> Fx, Fy, Fz, vp;
+  int stop_after_hll = 0;
 };
 
 void* hyqo_step_begin(int Nx, int Ny, int Nz, double* M, double Kn, double Ma, int flag2D, double CFL, double dtmax, double tmax,
                       double dx, double dy, double dz, int positivity, double* vmax_local) {
-  StepWork* w = new StepWork{Params{Nx, Ny, Nz, flag2D, positivity, Kn, Ma, CFL, dtmax, tmax, dx, dy, dz}, size_t(Nx) * Ny * Nz, {}, {}, {}, {}};
+  StepWork* w = new StepWork{Params{Nx, Ny, Nz, flag2D, positivity, Kn, Ma, CFL, dtmax, tmax, dx, dy, dz}, size_t(Nx) * Ny * Nz, {}, {}, {}, {}, 0};
   const Params& P = w->P;
   const size_t N = w->N;
   w->Fx.resize(N * 35); w->Fy.resize(N * 35); w->Fz.resize(N * 35); w->vp.resize(N * 6);
@@ -327,6 +328,7 @@ double hyqo_step_end(void* work, double* M, double vmax, double* t) {
     }
   }
   for (size_t q = 0; q < N * 35; ++q) M[q] = Mx[q] + My[q] + Mz[q] - 2.0 * M[q];
+  if (w->stop_after_hll) { delete w; return dt; }
   // [E] realizability and [F] collision
 #pragma omp parallel for schedule(dynamic, 16)
   for (long long c = 0; c < (long long)N; ++c) {
@@ -338,6 +340,13 @@ double hyqo_step_end(void* work, double* M, double vmax, double* t) {
   }
   delete w;
   return dt;
+}
+
+// The step's end stopped after the HLL combination (M = the state phase [E]
+// starts from); frees the work state.
+double hyqo_step_end_hll(void* work, double* M, double vmax, double* t) {
+  static_cast<StepWork*>(work)->stop_after_hll = 1;
+  return hyqo_step_end(work, M, vmax, t);
 }
 
 double hyqo_step(int Nx, int Ny, int Nz, double* M, double Kn, double Ma, int flag2D, double CFL, double dtmax, double tmax,

@@ -107,4 +107,25 @@ void sh_hexp_n(const double* x, double* y, long long n) { for (long long i = 0; 
 void sh_hcbrt_n(const double* x, double* y, long long n) { for (long long i = 0; i < n; ++i) y[i] = hcbrt(x[i]); }
 // realizable_3D on the 28 standardized moments (enum order), in place
 int sh_realizable_3d(double* a28) { return realizable_3D(a28); }
+// phase [A] of one cell as the step kernels run it on the plain path
+// (cp = 0) or the certified path (cp = 1: the certified solve where it
+// certifies, the complete LAPACK-path function for the cells it leaves):
+// v[6] the six Jacobian extremes (x, y, z), Mr the stage output
+void sh_phaseA_eigs(const double* m, int cp, double* v, double* Mr) {
+  double a[35], b[35], c[35];
+  for (int n = 0; n < 35; ++n) a[n] = m[n];
+  int planes = 0;
+  if (!cp || eigenvalues6_s<JAC_CP, false>(a, 1, 0, 1.0, v[0], v[1], b, 1, 1, &planes) != EIG_DONE)
+    eigenvalues6(a, 1, 0, 1.0, v[0], v[1], b);
+  if (!cp || eigenvalues6_s<JAC_CP, false>(b, 2, 0, 1.0, v[2], v[3], c, 1, 1, &planes) != EIG_DONE)
+    eigenvalues6(b, 2, 0, 1.0, v[2], v[3], c);
+  if (!cp || eigenvalues6z_s<JAC_CP, false>(c, 0, 1.0, 1, v[4], v[5], Mr, 1, 1, &planes) != EIG_DONE)
+    eigenvalues6z(c, 0, 1.0, 1, v[4], v[5], Mr);
+}
+// the complex-eigenvalue flags of phase [E] along `axis` on the certified
+// path (the certified solve, else the general code)
+int sh_flags_cp(const double* m, int axis) {
+  const int f = eigenvalues6_flags_t<JAC_CP>(m, axis, 1);
+  return f >= 0 ? f : eigenvalues6_flags_t<JAC_GEN>(m, axis, 1);
+}
 }
