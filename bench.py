@@ -285,6 +285,12 @@ def run_gpu(args, rank, world, local_rank):
             sol[m].set_state_ic()
             sol[m].advance(1)
     traj.advance(max(1, min(args.warmup, marks[0] - 1)))
+    # the HLL sweep's launch shape, timed on this workload (same bits in every
+    # shape) and used by all three paths
+    from hyqmom import autotune
+    tune = autotune.tune_solver(sol["plain"], use_cache=False)
+    for m in MODES:
+        sol[m].set_variant("hll", tune["hll"])
     ms = {m: [] for m in MODES}
     kern = {m: np.zeros(len(KERNELS)) for m in MODES}
     e2e_s = 0.0
@@ -382,7 +388,8 @@ def run_gpu(args, rank, world, local_rank):
                                    f"{run_steps}-step run, learned wave-speed path",
                        "cells": cells, "parallelism": f"replicas x{world}", "run_steps": run_steps, "timed_steps": marks,
                        "timing": "each timed step from the run's own state; plain and certified paths timed from the same state",
-                       "l2": f"state {cells * 35 * 8 / 1e6:.0f} MB > L2 (126 MB), no flush needed", "steps_done": st["nn"]},
+                       "l2": f"state {cells * 35 * 8 / 1e6:.0f} MB > L2 (126 MB), no flush needed", "steps_done": st["nn"],
+                       "autotune": {"hll_variant": tune["hll"], "hll_ms": tune["ms"]}},
             "modes": modes,
             "gpu_launches": LAUNCHES_PER_STEP["learned"] * k, "e2e": e2e, "roofline": roof, "clocks": sampler.summary()}
     if world == 1 and not args.no_cpu_baseline:
@@ -484,14 +491,17 @@ def batch_workload(n=64, seed=0, CFL=0.5):
 
 def run_batch(args, rank, world, local_rank):
     """Batched sweep: every domain advanced together (one graph replay per
-    step) against the same domains advanced one at a time."""
+    step; the schedule and launch variants picked by the autotuner, which
+    times them from the same states and keeps the choice per device) against
+    the same domains advanced one at a time."""
     import torch
     torch.cuda.set_device(local_rank)
-    from hyqmom import ic
+    from hyqmom import autotune
     from hyqmom.runner import BatchSolver
     ps = batch_workload()
     cells = [p["Nx"] * p["Ny"] * p["Nz"] for p in ps]
-    b = BatchSolver(ps, device=local_rank)
+    mode = args.batch_mode
+    b = BatchSolver(ps, device=local_rank, mode=mode)
 
     def reset():
         # every member's initial condition generated on the device
@@ -503,6 +513,7 @@ def run_batch(args, rank, world, local_rank):
 
     reset()
     b.advance(args.warmup)
+    tune = autotune.tune_batch(b, ps, mode=mode, steps=1, use_cache=False, log=lambda m: print(m, file=sys.stderr, flush=True))
     n0 = nn_all()
     stream = torch.cuda.ExternalStream(b.stream)
     sampler = ClockSampler(local_rank)
@@ -535,13 +546,20 @@ def run_batch(args, rank, world, local_rank):
         seq_ms += f0.elapsed_time(f1)
     seq_value = work / (seq_ms * 1e-3)
     b.close()
+    per_step = LAUNCHES_PER_STEP[mode] if tune["schedule"] == "fused" else LAUNCHES_PER_STEP[mode] * len(ps)
+    if mode == "learned" and tune["schedule"] == "fused":
+        per_step += len(ps) - 1  # the network runs once per member
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (reference crossing / triple-jet IC generator, seed 0)",
-            "config": {"workload": f"batched sweep of {len(ps)} domains, 16^3..96x96x48, Ma U[0,2], Kn logU[1e-3,1], CFL 0.5",
+            "config": {"workload": f"batched sweep of {len(ps)} domains, 16^3..96x96x48, Ma U[0,2], Kn logU[1e-3,1], CFL 0.5, "
+                                   f"{mode} eigenvalue path",
                        "cells_total": sum(cells), "domains_failed": failed, "one_at_a_time_value": seq_value,
-                       "batched_over_one_at_a_time": value / seq_value, "l2": "state of all domains > L2"},
-            "gpu_launches": LAUNCHES_PER_STEP * args.steps * len(ps), "clocks": sampler.summary()}
+                       "batched_over_one_at_a_time": value / seq_value, "l2": "state of all domains > L2",
+                       "autotune": {"schedule": tune["schedule"], "hll_variant": tune["hll"], "corr_variant": tune["corr"],
+                                    "trials_ms_per_step": tune["ms"]},
+                       "timed_steps": f"{args.warmup + 1}-{args.warmup + args.steps} of each member (members stop at their own limits)"},
+            "gpu_launches": per_step * args.steps, "clocks": sampler.summary()}
     print(json.dumps(line), flush=True)
 
 
@@ -553,6 +571,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c5", choices=["c1", "c2", "c2s", "c4", "c5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-mode", default="plain", choices=["plain", "certified", "learned"],
+                    help="--config c4: the members' eigenvalue path")
     ap.add_argument("--decompose", default="replicas", choices=["replicas", "slabs"],
                     help="N > 1: independent replicas (default) or one domain split into z-slabs")
     args = ap.parse_args()

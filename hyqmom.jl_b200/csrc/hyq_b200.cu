@@ -38,7 +38,7 @@ using namespace hyqk;
 
 namespace {
 
-__global__ void __launch_bounds__(1024) k_cfl(const double* __restrict__ blockmax, const StepConst sc, DevClock* clk) {
+__device__ __forceinline__ void cfl_body(const double* __restrict__ blockmax, const StepConst& sc, DevClock* clk) {
   const bool active = (clk->t < sc.tmax) && (clk->nn < sc.nnmax);
   __syncthreads();
   if (!active) {
@@ -62,6 +62,15 @@ __global__ void __launch_bounds__(1024) k_cfl(const double* __restrict__ blockma
     clk->nn = clk->nn + 1;
     clk->active = 1;
   }
+}
+__global__ void __launch_bounds__(1024) k_cfl(const double* __restrict__ blockmax, const StepConst sc, DevClock* clk) {
+  cfl_body(blockmax, sc, clk);
+}
+// fused batch: one block per member
+__global__ void __launch_bounds__(1024) k_cfl_b(const Batch bt) {
+  const Dom& d = bt.dom[blockIdx.x];
+  const StepConst sc = d.sc;
+  cfl_body(d.buf[DB_BMAX], sc, d.clk);
 }
 
 // The CFL reduction split for a domain decomposed over ranks: the local
@@ -102,9 +111,10 @@ __global__ void k_cfl_global(const double* xchg, const StepConst sc, DevClock* c
 // whether W* is formed, and which of L, C, R the boundary rules substitute
 // -- is resolved once per cell.
 struct HllFace {
-  double l1, l2, ll, lr;
+  double l1, l2;
   double rinv;              // 1 / (l1 - l2), for div_by
-  bool w;
+  bool w;                   // W* formed (|l1 - l2| > 1e-10)
+  bool zero;                // face 0: zero speeds in the dissipation term
 };
 struct HllLine {
   long long base;           // offset of cell L
@@ -125,7 +135,7 @@ __device__ __forceinline__ HllFace hll_face(const double* __restrict__ vmin, con
   f.l2 = jmax(c, d);
   f.w = fabs(f.l1 - f.l2) > 1e-10;
   f.rinv = 1.0 / (f.l1 - f.l2);
-  if (j == 0) { f.ll = 0.0; f.lr = 0.0; } else { f.ll = f.l1; f.lr = f.l2; }
+  f.zero = (j == 0);
   return f;
 }
 
@@ -155,7 +165,9 @@ __device__ __forceinline__ double hll_flux(const HllFace& f, double mj, double m
     const double d = f.l1 - f.l2;
     ws = div_by(f.l1 * mj - f.l2 * mj1, d, f.rinv) - div_by(fj - fj1, d, f.rinv);
   }
-  return 0.5 * (Fa + Fb) - 0.5 * (fabs(f.ll) * (ws - Ma_) - fabs(f.lr) * (ws - Mb));
+  // |lleft|, |lright| of the face (zero at face 0)
+  const double al = f.zero ? 0.0 : fabs(f.l1), ar = f.zero ? 0.0 : fabs(f.l2);
+  return 0.5 * (Fa + Fb) - 0.5 * (al * (ws - Ma_) - ar * (ws - Mb));
 }
 
 // The x, y or z update of one moment of the cell (pas_HLL for that line);
@@ -170,35 +182,114 @@ __device__ __forceinline__ double hll_update(const double* __restrict__ M, const
   return mC - L.r * (f1 - f0);
 }
 
-// One thread per cell: the face speeds of the x, y and z lines are resolved
-// once, then the 35 moments are updated in turn (coalesced along x).
+// One thread per cell and moment group: the face speeds of the x, y and z
+// lines are resolved once, then the group's moments are updated in turn
+// (coalesced along x).  GROUPS blocks cover the same BS cells, one group of
+// moments each (consecutive blocks, so that they share the speed reads in
+// L2); each moment's arithmetic is the same in every launch shape.
 #ifndef HQ_MINB_HLL
 #define HQ_MINB_HLL 4
 #endif
-__global__ void __launch_bounds__(BS_HLL, HQ_MINB_HLL) k_hll(const double* __restrict__ M, const double* __restrict__ Fx, const double* __restrict__ Fy,
-                                                 const double* __restrict__ Fz, const double* __restrict__ vp, double* __restrict__ Mout,
-                                                 const StepConst sc, const DevClock* clk) {
+template <int BS, int GROUPS>
+__device__ __forceinline__ void hll_body(const double* __restrict__ M, const double* __restrict__ Fx, const double* __restrict__ Fy,
+                                         const double* __restrict__ Fz, const double* __restrict__ vp, double* __restrict__ Mout,
+                                         const StepConst& sc, const DevClock* clk, int bid) {
   if (!clk->active) return;
   const long long N = sc.N;
-  const long long c = (long long)blockIdx.x * BS_HLL + threadIdx.x;
+  const int grp = GROUPS == 1 ? 0 : bid % GROUPS;
+  const long long c = (long long)(GROUPS == 1 ? bid : bid / GROUPS) * BS + threadIdx.x;
   if (c >= N) return;
   const double dt = clk->dt;
   const int Nx = sc.Nx, Ny = sc.Ny, Nz = sc.Nz;
   const int i = int(c % Nx);
   const int j = int((c / Nx) % Ny);
   const int k = int(c / ((long long)Nx * Ny));
-  const HllLine X = hll_setup(vp, vp + N, c - i, 1, Nx, i, dt / sc.dx);
-  const HllLine Y = hll_setup(vp + 2 * N, vp + 3 * N, c - (long long)j * Nx, Nx, Ny, j, dt / sc.dy);
+  if (GROUPS == 1) {
+    // all 35 moments: the three lines resolved together, one moment at a time
+    const HllLine X = hll_setup(vp, vp + N, c - i, 1, Nx, i, dt / sc.dx);
+    const HllLine Y = hll_setup(vp + 2 * N, vp + 3 * N, c - (long long)j * Nx, Nx, Ny, j, dt / sc.dy);
+    HllLine Z;
+    if (Nz > 1) Z = hll_setup(vp + 4 * N, vp + 5 * N, c - (long long)k * Nx * Ny, Nx * Ny, Nz, k, dt / sc.dz);
+#pragma unroll 1
+    for (int n = 0; n < 35; ++n) {
+      const long long mo = N * n;
+      const double* Mn = M + mo;
+      const double mx = hll_update(Mn, Fx + mo, X);
+      const double my = hll_update(Mn, Fy + mo, Y);
+      const double mz = (Nz == 1) ? Mn[c] : hll_update(Mn, Fz + mo, Z);
+      Mout[c + mo] = mx + my + mz - 2.0 * Mn[c];
+    }
+    return;
+  }
+  // a group of K moments: one line at a time over the group (fewer live
+  // registers), the sums formed in the same order, ((mx + my) + mz) - 2 M
+  constexpr int K = (35 + GROUPS - 1) / GROUPS;
+  const int n0 = (35 * grp) / GROUPS, n1 = (35 * (grp + 1)) / GROUPS;
+  double acc[K];
+  {
+    const HllLine X = hll_setup(vp, vp + N, c - i, 1, Nx, i, dt / sc.dx);
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+      if (n0 + q < n1) acc[q] = hll_update(M + N * (n0 + q), Fx + N * (n0 + q), X);
+  }
+  {
+    const HllLine Y = hll_setup(vp + 2 * N, vp + 3 * N, c - (long long)j * Nx, Nx, Ny, j, dt / sc.dy);
+#pragma unroll
+    for (int q = 0; q < K; ++q)
+      if (n0 + q < n1) acc[q] = acc[q] + hll_update(M + N * (n0 + q), Fy + N * (n0 + q), Y);
+  }
   HllLine Z;
   if (Nz > 1) Z = hll_setup(vp + 4 * N, vp + 5 * N, c - (long long)k * Nx * Ny, Nx * Ny, Nz, k, dt / sc.dz);
-#pragma unroll 1
-  for (int n = 0; n < 35; ++n) {
-    const long long mo = N * n;
-    const double* Mn = M + mo;
-    const double mx = hll_update(Mn, Fx + mo, X);
-    const double my = hll_update(Mn, Fy + mo, Y);
-    const double mz = (Nz == 1) ? Mn[c] : hll_update(Mn, Fz + mo, Z);
-    Mout[c + mo] = mx + my + mz - 2.0 * Mn[c];
+#pragma unroll
+  for (int q = 0; q < K; ++q)
+    if (n0 + q < n1) {
+      const long long mo = N * (n0 + q);
+      const double* Mn = M + mo;
+      const double mz = (Nz == 1) ? Mn[c] : hll_update(Mn, Fz + mo, Z);
+      Mout[c + mo] = acc[q] + mz - 2.0 * Mn[c];
+    }
+}
+template <int BS, int GROUPS>
+__global__ void __launch_bounds__(BS, HQ_MINB_HLL * 256 / BS) k_hll(const double* __restrict__ M, const double* __restrict__ Fx,
+                                                                    const double* __restrict__ Fy, const double* __restrict__ Fz,
+                                                                    const double* __restrict__ vp, double* __restrict__ Mout,
+                                                                    const StepConst sc, const DevClock* clk) {
+  hll_body<BS, GROUPS>(M, Fx, Fy, Fz, vp, Mout, sc, clk, blockIdx.x);
+}
+template <int BS, int GROUPS>
+__global__ void __launch_bounds__(BS, HQ_MINB_HLL * 256 / BS) k_hll_b(const Batch bt) {
+  const int m = member_of(bt, blockIdx.x);
+  const Dom& d = bt.dom[m];
+  const StepConst sc = d.sc;
+  hll_body<BS, GROUPS>(d.buf[DB_M], d.buf[DB_FX], d.buf[DB_FY], d.buf[DB_FZ], d.buf[DB_VP], d.buf[DB_MTMP], sc, d.clk,
+                       blockIdx.x - __ldg(bt.blk0 + m));
+}
+template <int BS, int GROUPS>
+void hll_launch(const double* M, const double* Fx, const double* Fy, const double* Fz, const double* vp, double* Mout, const StepConst& sc,
+                const DevClock* clk, cudaStream_t s) {
+  k_hll<BS, GROUPS><<<grid_of(sc.N, BS) * GROUPS, BS, 0, s>>>(M, Fx, Fy, Fz, vp, Mout, sc, clk);
+}
+void hll_variant(int variant, const double* M, const double* Fx, const double* Fy, const double* Fz, const double* vp, double* Mout,
+                 const StepConst& sc, const DevClock* clk, cudaStream_t s) {
+  switch (variant) {
+    case 1: hll_launch<256, 5>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
+    case 2: hll_launch<256, 7>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
+    case 3: hll_launch<128, 5>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
+    case 4: hll_launch<128, 7>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
+    case 5: hll_launch<128, 1>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
+    default: hll_launch<256, 1>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
+  }
+}
+void hll_variant_b(int variant, const Batch& bt, int nblk, cudaStream_t s) {
+  int bs, g;
+  hll_shape(variant, bs, g);
+  switch (variant) {
+    case 1: k_hll_b<256, 5><<<nblk, 256, 0, s>>>(bt); break;
+    case 2: k_hll_b<256, 7><<<nblk, 256, 0, s>>>(bt); break;
+    case 3: k_hll_b<128, 5><<<nblk, 128, 0, s>>>(bt); break;
+    case 4: k_hll_b<128, 7><<<nblk, 128, 0, s>>>(bt); break;
+    case 5: k_hll_b<128, 1><<<nblk, 128, 0, s>>>(bt); break;
+    default: k_hll_b<256, 1><<<nblk, 256, 0, s>>>(bt); break;
   }
 }
 
@@ -215,11 +306,11 @@ __global__ void k_set_clock(DevClock* clk, double t, long long nn) {
 // the largest |speed| along each axis over all cells (Julia `maximum`
 // semantics: a NaN wins; |speed| bit patterns order like the values, NaN
 // above Inf), then the first cell that attains the global maximum.
-__global__ void __launch_bounds__(256) k_diag_speeds(const double* __restrict__ vp, const StepConst sc, DevClock* clk) {
+__device__ __forceinline__ void diag_speeds_body(const double* __restrict__ vp, const StepConst& sc, DevClock* clk, int bid, int nblk) {
   if (!clk->active || clk->nn != 1) return;
   const long long N = sc.N;
   unsigned long long m[3] = {0, 0, 0};
-  for (long long c = (long long)blockIdx.x * 256 + threadIdx.x; c < N; c += (long long)gridDim.x * 256)
+  for (long long c = (long long)bid * 256 + threadIdx.x; c < N; c += (long long)nblk * 256)
     for (int d = 0; d < 3; ++d)
       for (int q = 0; q < 2; ++q) {
         const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(vp[c + N * (2 * d + q)]));
@@ -234,13 +325,13 @@ __global__ void __launch_bounds__(256) k_diag_speeds(const double* __restrict__ 
     if ((threadIdx.x & 31) == 0 && v) atomicMax(&clk->vdir_bits[d], v);
   }
 }
-__global__ void __launch_bounds__(256) k_diag_worst(const double* __restrict__ vp, const StepConst sc, DevClock* clk) {
+__device__ __forceinline__ void diag_worst_body(const double* __restrict__ vp, const StepConst& sc, DevClock* clk, int bid, int nblk) {
   if (!clk->active || clk->nn != 1) return;
   const long long N = sc.N;
   unsigned long long g = clk->vdir_bits[0];
   g = clk->vdir_bits[1] > g ? clk->vdir_bits[1] : g;
   g = clk->vdir_bits[2] > g ? clk->vdir_bits[2] : g;
-  for (long long c = (long long)blockIdx.x * 256 + threadIdx.x; c < N; c += (long long)gridDim.x * 256)
+  for (long long c = (long long)bid * 256 + threadIdx.x; c < N; c += (long long)nblk * 256)
     for (int d = 0; d < 3; ++d)
       for (int q = 0; q < 2; ++q)
         if ((unsigned long long)__double_as_longlong(fabs(vp[c + N * (2 * d + q)])) == g) {
@@ -249,13 +340,33 @@ __global__ void __launch_bounds__(256) k_diag_worst(const double* __restrict__ v
           atomicMin(&clk->worst_cell, key);
         }
 }
+__global__ void __launch_bounds__(256) k_diag_speeds(const double* __restrict__ vp, const StepConst sc, DevClock* clk) {
+  diag_speeds_body(vp, sc, clk, blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(256) k_diag_worst(const double* __restrict__ vp, const StepConst sc, DevClock* clk) {
+  diag_worst_body(vp, sc, clk, blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(256) k_diag_speeds_b(const Batch bt) {
+  const int m = member_of(bt, blockIdx.x);
+  const Dom& d = bt.dom[m];
+  const StepConst sc = d.sc;
+  const int b0 = __ldg(bt.blk0 + m);
+  diag_speeds_body(d.buf[DB_VP], sc, d.clk, blockIdx.x - b0, __ldg(bt.blk0 + m + 1) - b0);
+}
+__global__ void __launch_bounds__(256) k_diag_worst_b(const Batch bt) {
+  const int m = member_of(bt, blockIdx.x);
+  const Dom& d = bt.dom[m];
+  const StepConst sc = d.sc;
+  const int b0 = __ldg(bt.blk0 + m);
+  diag_worst_body(d.buf[DB_VP], sc, d.clk, blockIdx.x - b0, __ldg(bt.blk0 + m + 1) - b0);
+}
 
 // MaxDiff (src/simulation_runner.jl:562-637) of the state after the step, at
 // steps nn % interval == 0 and nn == 1: on the diagonal i = j of the first
 // z-layer, Diff_m(i) = M_m(i,i) -+ M_m(N'-1-i, N'-1-i) for the moments
 // M000, M100, M200, M300, M400 (- for the even ones, + for the odd ones),
 // MaxDiff = max_m |max_i Diff_m(i) / (||Diff_m||_2 + 1)|; NaN propagates.
-__global__ void __launch_bounds__(256) k_maxdiff(const double* __restrict__ M, const StepConst sc, DevClock* clk) {
+__device__ __forceinline__ void maxdiff_body(const double* __restrict__ M, const StepConst& sc, DevClock* clk) {
   if (!clk->active || sc.symmetry_check_interval <= 0) return;
   const long long nn = clk->nn;
   if (!(nn % sc.symmetry_check_interval == 0 || nn == 1)) return;
@@ -293,6 +404,14 @@ __global__ void __launch_bounds__(256) k_maxdiff(const double* __restrict__ M, c
 }
 
 
+__global__ void __launch_bounds__(256) k_maxdiff(const double* __restrict__ M, const StepConst sc, DevClock* clk) { maxdiff_body(M, sc, clk); }
+// fused batch: one block per member
+__global__ void __launch_bounds__(256) k_maxdiff_b(const Batch bt) {
+  const Dom& d = bt.dom[blockIdx.x];
+  const StepConst sc = d.sc;
+  maxdiff_body(d.buf[DB_M], sc, d.clk);
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ C-ABI
@@ -318,6 +437,11 @@ struct hyq_ctx {
   WaveNet net{nullptr, nullptr};
   float* net_w = nullptr;  // FP32 parameters (device), packed into net.image
   bool net_loaded = false;
+  // launch shape of the HLL kernel (hll_shape; hyq_set_variant)
+  int hll_variant = 0;
+  // bumped whenever the step graph is captured again (a batch holding this
+  // member re-reads its constants then)
+  int gen = 0;
   std::string err;
 };
 
@@ -339,17 +463,17 @@ int cuda_fail(hyq_ctx* ctx, cudaError_t e, const char* what) {
 
 
 void enqueue_step(hyq_ctx* ctx, cudaStream_t s) {
-  const long long N = ctx->N;
   launch_phase_A(ctx->sc, ctx->M, ctx->Mtmp, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->blockmax, ctx->clk, s, nullptr, 0, -1, &ctx->net);
   k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
   launch_diagnostics_speeds(ctx->vp, ctx->sc, ctx->clk, s);
-  k_hll<<<grid_of(N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
+  hll_variant(ctx->hll_variant, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk, s);
   launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->clk, s);
   launch_maxdiff(ctx->M, ctx->sc, ctx->clk, s);
 }
 // Capture one step as the context's graph (replacing an earlier one).
 int capture_graph(hyq_ctx* ctx) {
   cudaError_t e;
+  ++ctx->gen;
   if (ctx->exec) { cudaGraphExecDestroy(ctx->exec); ctx->exec = nullptr; }
   if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
   if ((e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
@@ -368,7 +492,7 @@ void enqueue_half_a(hyq_ctx* ctx, cudaStream_t s) {
 void enqueue_half_b(hyq_ctx* ctx, cudaStream_t s) {
   k_cfl_global<<<1, 1, 0, s>>>(ctx->xchg, ctx->sc, ctx->clk);
   launch_diagnostics_speeds(ctx->vp, ctx->sc, ctx->clk, s);
-  k_hll<<<grid_of(ctx->N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
+  hll_variant(ctx->hll_variant, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk, s);
   launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->clk, s);
   launch_maxdiff(ctx->M, ctx->sc, ctx->clk, s);
 }
@@ -439,8 +563,8 @@ void launch_cfl(const double* blockmax, const StepConst& sc, DevClock* clk, cuda
   k_cfl<<<1, 1024, 0, s>>>(blockmax, sc, clk);
 }
 void launch_hll(const double* M, const double* Fx, const double* Fy, const double* Fz, const double* vp, double* Mout, const StepConst& sc,
-                const DevClock* clk, cudaStream_t s) {
-  k_hll<<<grid_of(sc.N, BS_HLL), BS_HLL, 0, s>>>(M, Fx, Fy, Fz, vp, Mout, sc, clk);
+                const DevClock* clk, cudaStream_t s, int variant) {
+  hll_variant(variant, M, Fx, Fy, Fz, vp, Mout, sc, clk, s);
 }
 void launch_set_clock(DevClock* clk, double t, long long nn, cudaStream_t s) { k_set_clock<<<1, 1, 0, s>>>(clk, t, nn); }
 void launch_diagnostics_speeds(const double* vp, const StepConst& sc, DevClock* clk, cudaStream_t s) {
@@ -449,6 +573,13 @@ void launch_diagnostics_speeds(const double* vp, const StepConst& sc, DevClock* 
   k_diag_worst<<<g, 256, 0, s>>>(vp, sc, clk);
 }
 void launch_maxdiff(const double* M, const StepConst& sc, DevClock* clk, cudaStream_t s) { k_maxdiff<<<1, 256, 0, s>>>(M, sc, clk); }
+void launch_mid_batch(const BatchPlan& bp, cudaStream_t s) {
+  k_cfl_b<<<bp.n, 1024, 0, s>>>(bp.of(DK_ONE));
+  k_diag_speeds_b<<<bp.nblk[DK_DIAG], 256, 0, s>>>(bp.of(DK_DIAG));
+  k_diag_worst_b<<<bp.nblk[DK_DIAG], 256, 0, s>>>(bp.of(DK_DIAG));
+  hll_variant_b(bp.hll_variant, bp.of(DK_HLL), bp.nblk[DK_HLL], s);
+}
+void launch_maxdiff_batch(const BatchPlan& bp, cudaStream_t s) { k_maxdiff_b<<<bp.n, 256, 0, s>>>(bp.of(DK_ONE)); }
 int report_error(int code, const char* msg) { return fail(nullptr, code, msg); }
 }  // namespace hyqk
 
@@ -666,6 +797,25 @@ int hyq_set_spacing(hyq_ctx* ctx, double dx, double dy, double dz) {
   return r;
 }
 
+int32_t hyq_variant_count(int32_t kernel) {
+  if (kernel == HYQ_KERNEL_HLL) return HLL_VARIANTS;
+  if (kernel == HYQ_KERNEL_CORR) return HYQ_CORR_VARIANTS;
+  return 0;
+}
+
+int hyq_set_variant(hyq_ctx* ctx, int32_t kernel, int32_t variant) {
+  if (!ctx) return fail(nullptr, HYQ_EINVAL, "null ctx");
+  if (kernel != HYQ_KERNEL_HLL) return fail(ctx, HYQ_EINVAL, "a context has launch variants for HYQ_KERNEL_HLL only");
+  if (variant < 0 || variant >= HLL_VARIANTS) return fail(ctx, HYQ_EINVAL, "variant out of range");
+  if (variant == ctx->hll_variant) return HYQ_OK;
+  HQ_CHECK(ctx, cudaSetDevice(ctx->device));
+  HQ_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->hll_variant = variant;
+  int r = capture_graph(ctx);
+  if (r == HYQ_OK && ctx->exec_a) r = capture_halves(ctx);
+  return r;
+}
+
 int hyq_step_begin(hyq_ctx* ctx, double* xchg) {
   if (!ctx || !xchg) return fail(ctx, HYQ_EINVAL, "null argument");
   if (ctx->sc.mode == MODE_LEARNED && !ctx->net_loaded)
@@ -718,7 +868,6 @@ int hyq_advance_timed(hyq_ctx* ctx, int64_t steps, float* ms) {
   cudaEvent_t ev[K + 1];
   for (int q = 0; q <= K; ++q) HQ_CHECK(ctx, cudaEventCreate(&ev[q]));
   for (int q = 0; q < K; ++q) ms[q] = 0.0f;
-  const long long N = ctx->N;
   cudaStream_t s = ctx->stream;
   for (int64_t it = 0; it < steps; ++it) {
     cudaEventRecord(ev[0], s);
@@ -726,7 +875,7 @@ int hyq_advance_timed(hyq_ctx* ctx, int64_t steps, float* ms) {
     k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
     launch_diagnostics_speeds(ctx->vp, ctx->sc, ctx->clk, s);
     cudaEventRecord(ev[6], s);
-    k_hll<<<grid_of(N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
+    hll_variant(ctx->hll_variant, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk, s);
     cudaEventRecord(ev[7], s);
     launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->clk, s, ev + 8);
     launch_maxdiff(ctx->M, ctx->sc, ctx->clk, s);
@@ -819,7 +968,7 @@ int hyq_step_host(hyq_ctx* ctx, const double* M_in, double* M_out, int32_t nslab
   // the CFL reduction and the HLL sweep need every cell
   k_cfl<<<1, 1024, 0, s>>>(ctx->blockmax, ctx->sc, ctx->clk);
   launch_diagnostics_speeds(ctx->vp, ctx->sc, ctx->clk, s);
-  k_hll<<<grid_of(N, BS_HLL), BS_HLL, 0, s>>>(ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk);
+  hll_variant(ctx->hll_variant, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk, s);
   // phases E+F slab by slab, each slab downloaded as soon as it is done
   for (int k = 0; k < S; ++k) {
     const long long c0 = cut[k], c1 = cut[k + 1];
@@ -917,7 +1066,120 @@ struct hyq_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t replayed = nullptr;  // recorded after each hyq_batch_advance_async
+  int schedule = HYQ_BATCH_FUSED;
+  int hll_variant = 0;
+  int corr_variant = 0;
+  // fused schedule: the member table and the block prefixes of each launch
+  // kind on the device
+  Dom* d_dom = nullptr;
+  int* d_blk = nullptr;
+  BatchPlan plan{};
+  std::vector<int> gens;  // the members' graph generations at the last capture
 };
+
+namespace {
+// correction passes: blocks per member of a fused launch, by variant
+constexpr int CORR_CAPS[HYQ_CORR_VARIANTS] = {64, 16, 4, CORR_BLOCKS};
+
+bool batch_fusable(const hyq_batch* b) {
+  for (const hyq_ctx* c : b->sims)
+    if (c->sc.mode != b->sims[0]->sc.mode) return false;
+  return true;
+}
+
+// The member table and block prefixes of the fused launches, on the device.
+int batch_plan(hyq_batch* b) {
+  const int n = (int)b->sims.size();
+  std::vector<Dom> dom(n);
+  std::vector<int> blk((size_t)DK_NKIND * (n + 1), 0);
+  int hbs, hg;
+  hll_shape(b->hll_variant, hbs, hg);
+  for (int m = 0; m < n; ++m) {
+    const hyq_ctx* c = b->sims[m];
+    Dom& d = dom[m];
+    d.sc = c->sc;
+    d.clk = c->clk;
+    d.buf[DB_M] = c->M; d.buf[DB_MTMP] = c->Mtmp; d.buf[DB_FX] = c->Fx; d.buf[DB_FY] = c->Fy; d.buf[DB_FZ] = c->Fz;
+    d.buf[DB_VP] = c->vp; d.buf[DB_BMAX] = c->blockmax;
+    int nb[DK_NKIND];
+    dom_blocks(c->N, hbs, hg, CORR_CAPS[b->corr_variant], nb);
+    for (int k = 0; k < DK_NKIND; ++k) {
+      const long long next = (long long)blk[(size_t)k * (n + 1) + m] + nb[k];
+      if (next > 0x7fffffffLL) return fail(nullptr, HYQ_EINVAL, "fused batch: too many blocks in one launch");
+      blk[(size_t)k * (n + 1) + m + 1] = (int)next;
+    }
+  }
+  cudaError_t e;
+  if (!b->d_dom) {
+    if ((e = cudaMalloc((void**)&b->d_dom, sizeof(Dom) * n)) != cudaSuccess) return cuda_fail(nullptr, e, "batch member table");
+    if ((e = cudaMalloc((void**)&b->d_blk, sizeof(int) * blk.size())) != cudaSuccess) return cuda_fail(nullptr, e, "batch block table");
+  }
+  if ((e = cudaMemcpyAsync(b->d_dom, dom.data(), sizeof(Dom) * n, cudaMemcpyHostToDevice, b->stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(b->d_blk, blk.data(), sizeof(int) * blk.size(), cudaMemcpyHostToDevice, b->stream)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(b->stream)) != cudaSuccess)
+    return cuda_fail(nullptr, e, "batch tables");
+  b->plan.dom = b->d_dom;
+  b->plan.n = n;
+  b->plan.hll_variant = b->hll_variant;
+  for (int k = 0; k < DK_NKIND; ++k) {
+    b->plan.blk0[k] = b->d_blk + (size_t)k * (n + 1);
+    b->plan.nblk[k] = blk[(size_t)k * (n + 1) + n];
+  }
+  return HYQ_OK;
+}
+
+// The learned path's network launches of every member, after the fused
+// first closure (each member's own weights and seed buffer).
+void batch_seeds(void* arg, cudaStream_t s) {
+  const hyq_batch* b = static_cast<const hyq_batch*>(arg);
+  for (const hyq_ctx* c : b->sims) launch_wavespeed_seeds(c->sc, c->Fx, &c->net, c->sc.seeds, c->clk, s, 0, c->N);
+}
+
+// One graph per step: the fused launches, or the members' step graphs as
+// independent branches.
+int batch_capture(hyq_batch* b) {
+  cudaError_t e;
+  for (const hyq_ctx* c : b->sims)
+    if (c->sc.mode == MODE_LEARNED && !c->net_loaded)
+      return fail(nullptr, HYQ_EINVAL, "HYQ_MODE_LEARNED members need their wave-speed networks (hyq_set_wavespeed_net) first");
+  if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+  if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+  if (b->schedule == HYQ_BATCH_FUSED) {
+    const int r = batch_plan(b);
+    if (r != HYQ_OK) return r;
+    const int mode = b->sims[0]->sc.mode;
+    if ((e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+      return cuda_fail(nullptr, e, "cudaStreamBeginCapture");
+    launch_phase_A_batch(b->plan, mode, b->stream, mode == MODE_LEARNED ? batch_seeds : nullptr, b);
+    launch_mid_batch(b->plan, b->stream);
+    launch_phase_EF_batch(b->plan, mode, b->stream);
+    launch_maxdiff_batch(b->plan, b->stream);
+    if ((e = cudaStreamEndCapture(b->stream, &b->graph)) != cudaSuccess) return cuda_fail(nullptr, e, "cudaStreamEndCapture");
+  } else {
+    if ((e = cudaGraphCreate(&b->graph, 0)) != cudaSuccess) return cuda_fail(nullptr, e, "batch graph");
+    // largest members first, so that their kernels start first and the small
+    // members' kernels fill the SMs they leave free
+    std::vector<hyq_ctx*> order(b->sims);
+    std::stable_sort(order.begin(), order.end(), [](const hyq_ctx* x, const hyq_ctx* y) { return x->N > y->N; });
+    for (hyq_ctx* c : order) {
+      cudaGraphNode_t node;
+      if ((e = cudaGraphAddChildGraphNode(&node, b->graph, nullptr, 0, c->graph)) != cudaSuccess)
+        return cuda_fail(nullptr, e, "cudaGraphAddChildGraphNode");
+    }
+  }
+  if ((e = cudaGraphInstantiate(&b->exec, b->graph, 0)) != cudaSuccess) return cuda_fail(nullptr, e, "cudaGraphInstantiate");
+  b->gens.clear();
+  for (const hyq_ctx* c : b->sims) b->gens.push_back(c->gen);
+  return HYQ_OK;
+}
+
+// Capture again when a member's constants or graph changed since.
+int batch_refresh(hyq_batch* b) {
+  bool stale = !b->exec || b->gens.size() != b->sims.size();
+  for (size_t m = 0; !stale && m < b->sims.size(); ++m) stale = b->gens[m] != b->sims[m]->gen;
+  return stale ? batch_capture(b) : HYQ_OK;
+}
+}  // namespace
 
 void hyq_batch_destroy(hyq_batch* b) {
   if (!b) return;
@@ -926,6 +1188,8 @@ void hyq_batch_destroy(hyq_batch* b) {
   if (b->replayed) cudaEventDestroy(b->replayed);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->d_dom) cudaFree(b->d_dom);
+  if (b->d_blk) cudaFree(b->d_blk);
   if (b->stream) cudaStreamDestroy(b->stream);
   for (hyq_ctx* c : b->sims) hyq_destroy(c);
   delete b;
@@ -933,6 +1197,7 @@ void hyq_batch_destroy(hyq_batch* b) {
 
 int hyq_batch_create(const hyq_params* p, int32_t n, hyq_batch** out) {
   if (!p || !out || n < 1) return fail(nullptr, HYQ_EINVAL, "null argument or empty batch");
+  if (n > DK_MAX_MEMBERS) return fail(nullptr, HYQ_EINVAL, "too many members for one batch");
   *out = nullptr;
   for (int32_t i = 1; i < n; ++i)
     if (p[i].device != p[0].device) return fail(nullptr, HYQ_EINVAL, "all members of a batch must use the same device");
@@ -950,31 +1215,52 @@ int hyq_batch_create(const hyq_params* p, int32_t n, hyq_batch** out) {
   }
   cudaError_t e;
   if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess ||
-      (e = cudaEventCreateWithFlags(&b->replayed, cudaEventDisableTiming)) != cudaSuccess ||
-      (e = cudaGraphCreate(&b->graph, 0)) != cudaSuccess) {
-    const int r = cuda_fail(nullptr, e, "batch graph");
+      (e = cudaEventCreateWithFlags(&b->replayed, cudaEventDisableTiming)) != cudaSuccess) {
+    const int r = cuda_fail(nullptr, e, "batch stream");
     hyq_batch_destroy(b);
     return r;
   }
-  // largest members first, so that their kernels start first and the small
-  // members' kernels fill the SMs they leave free
-  std::vector<hyq_ctx*> order(b->sims);
-  std::stable_sort(order.begin(), order.end(), [](const hyq_ctx* x, const hyq_ctx* y) { return x->N > y->N; });
-  for (hyq_ctx* c : order) {
-    cudaGraphNode_t node;
-    if ((e = cudaGraphAddChildGraphNode(&node, b->graph, nullptr, 0, c->graph)) != cudaSuccess) {
-      const int r = cuda_fail(nullptr, e, "cudaGraphAddChildGraphNode");
+  if (!batch_fusable(b)) b->schedule = HYQ_BATCH_BRANCHES;
+  // learned members are captured at the first advance, after their networks
+  if (b->sims[0]->sc.mode != MODE_LEARNED) {
+    const int r = batch_capture(b);
+    if (r != HYQ_OK) {
       hyq_batch_destroy(b);
       return r;
     }
   }
-  if ((e = cudaGraphInstantiate(&b->exec, b->graph, 0)) != cudaSuccess) {
-    const int r = cuda_fail(nullptr, e, "cudaGraphInstantiate");
-    hyq_batch_destroy(b);
-    return r;
-  }
   *out = b;
   return HYQ_OK;
+}
+
+int hyq_batch_set_schedule(hyq_batch* b, int32_t schedule) {
+  if (!b) return fail(nullptr, HYQ_EINVAL, "null batch");
+  if (schedule != HYQ_BATCH_FUSED && schedule != HYQ_BATCH_BRANCHES) return fail(nullptr, HYQ_EINVAL, "unknown schedule");
+  if (schedule == HYQ_BATCH_FUSED && !batch_fusable(b))
+    return fail(nullptr, HYQ_EINVAL, "a fused batch needs one eigenvalue path (hyq_params.mode) for all members");
+  HQ_CHECK(nullptr, cudaSetDevice(b->device));
+  HQ_CHECK(nullptr, cudaStreamSynchronize(b->stream));
+  b->schedule = schedule;
+  return batch_capture(b);
+}
+
+int32_t hyq_batch_schedule(const hyq_batch* b) { return b ? b->schedule : -1; }
+
+int hyq_batch_set_variant(hyq_batch* b, int32_t kernel, int32_t variant) {
+  if (!b) return fail(nullptr, HYQ_EINVAL, "null batch");
+  if (variant < 0 || variant >= hyq_variant_count(kernel)) return fail(nullptr, HYQ_EINVAL, "unknown kernel or variant out of range");
+  HQ_CHECK(nullptr, cudaSetDevice(b->device));
+  HQ_CHECK(nullptr, cudaStreamSynchronize(b->stream));
+  if (kernel == HYQ_KERNEL_HLL) {
+    b->hll_variant = variant;
+    for (hyq_ctx* c : b->sims) {
+      const int r = hyq_set_variant(c, kernel, variant);
+      if (r != HYQ_OK) return fail(nullptr, r, c->err);
+    }
+  } else {
+    b->corr_variant = variant;
+  }
+  return batch_capture(b);
 }
 
 int32_t hyq_batch_size(const hyq_batch* b) { return b ? (int32_t)b->sims.size() : 0; }
@@ -991,6 +1277,11 @@ int hyq_batch_advance_async(hyq_batch* b, int64_t max_steps) {
   HQ_CHECK(nullptr, cudaSetDevice(b->device));
   // members' own streams may still hold a state upload or clock reset
   for (hyq_ctx* c : b->sims) HQ_CHECK(nullptr, cudaStreamSynchronize(c->stream));
+  for (hyq_ctx* c : b->sims)
+    if (c->sc.mode == MODE_LEARNED && !c->net_loaded)
+      return fail(nullptr, HYQ_EINVAL, "HYQ_MODE_LEARNED members need their wave-speed networks before stepping");
+  const int r = batch_refresh(b);
+  if (r != HYQ_OK) return r;
   for (int64_t s = 0; s < max_steps; ++s) HQ_CHECK(nullptr, cudaGraphLaunch(b->exec, b->stream));
   // member calls run on the members' own streams: order them after the replays
   HQ_CHECK(nullptr, cudaEventRecord(b->replayed, b->stream));

@@ -99,6 +99,46 @@ constexpr int BS_CELLS = 128;
 
 inline int grid_of(long long n, int bs) { return int((n + bs - 1) / bs); }
 
+// ---- fused batches: many independent domains in one launch per kernel ----
+// A member as the fused kernels see it: its constants, clock and buffers.
+enum DomBuf { DB_M = 0, DB_MTMP, DB_FX, DB_FY, DB_FZ, DB_VP, DB_BMAX, DB_NBUF };
+struct Dom {
+  StepConst sc;
+  DevClock* clk;
+  double* buf[DB_NBUF];
+};
+// Launch shapes of the fused kernels; a launch of kind K gives member m the
+// blocks [blk0[K][m], blk0[K][m + 1]) of its grid.
+enum DomKind { DK_CELLS = 0, DK_CORR, DK_HLL, DK_ONE, DK_DIAG, DK_NKIND };
+constexpr int DK_MAX_MEMBERS = 4096;
+// The block counts of member m's launch of each kind (hll_g: the HLL
+// kernel's moment groups; corr_cap: the correction passes' blocks per member).
+inline void dom_blocks(long long N, int hll_bs, int hll_g, int corr_cap, int* nb) {
+  const int g = grid_of(N, BS_A);
+  nb[DK_CELLS] = g;
+  nb[DK_CORR] = g < corr_cap ? g : corr_cap;
+  nb[DK_HLL] = grid_of(N, hll_bs) * hll_g;
+  nb[DK_ONE] = 1;
+  const int gd = grid_of(N, 256);
+  nb[DK_DIAG] = gd < 64 ? gd : 64;
+}
+// What the fused kernels of one launch get: the member table and the block
+// prefix of the launch's kind (device arrays owned by the batch).
+struct Batch {
+  const Dom* dom;
+  const int* blk0;  // n + 1 entries
+  int n;
+};
+// Host-side view of a fused batch: device tables and total blocks per kind.
+struct BatchPlan {
+  const Dom* dom;
+  const int* blk0[DK_NKIND];
+  int nblk[DK_NKIND];
+  int n;
+  int hll_variant;
+  Batch of(int kind) const { return Batch{dom, blk0[kind], n}; }
+};
+
 // launch wrappers (defined in k_phase_A.cu, k_phase_EF.cu, k_cells.cu)
 // Phase [A] in place on M; Mtmp, Fx, Fy, Fz carry its intermediate states,
 // and on completion Fx, Fy, Fz hold the fluxes (Mtmp is left as scratch).
@@ -139,8 +179,28 @@ void launch_cfl(const double* blockmax, const StepConst& sc, DevClock* clk, cuda
 // the steps they do not measure
 void launch_diagnostics_speeds(const double* vp, const StepConst& sc, DevClock* clk, cudaStream_t s);
 void launch_maxdiff(const double* M, const StepConst& sc, DevClock* clk, cudaStream_t s);
+// variant: the HLL kernel's launch shape (hll_shape); all variants give the
+// same bits
 void launch_hll(const double* M, const double* Fx, const double* Fy, const double* Fz, const double* vp, double* Mout, const StepConst& sc,
-                const DevClock* clk, cudaStream_t s);
+                const DevClock* clk, cudaStream_t s, int variant = 0);
+// The HLL kernel's launch shapes: cells per block and moment groups (the 35
+// moments split over that many blocks of the same cells).
+constexpr int HLL_VARIANTS = 6;
+inline void hll_shape(int variant, int& bs, int& groups) {
+  static const int tab[HLL_VARIANTS][2] = {{256, 1}, {256, 5}, {256, 7}, {128, 5}, {128, 7}, {128, 1}};
+  const int v = (variant >= 0 && variant < HLL_VARIANTS) ? variant : 0;
+  bs = tab[v][0];
+  groups = tab[v][1];
+}
+// Fused batches (one launch per kernel for all members of the plan):
+// phase [A] (after_a1, when set, runs after the first closure: the learned
+// path's per-member network launches), the CFL reduction, the diagnostics and
+// the HLL sweep, phases [E]+[F] and MaxDiff; mode: the members' common
+// eigenvalue path.
+void launch_phase_A_batch(const BatchPlan& bp, int mode, cudaStream_t s, void (*after_a1)(void*, cudaStream_t), void* arg);
+void launch_mid_batch(const BatchPlan& bp, cudaStream_t s);
+void launch_phase_EF_batch(const BatchPlan& bp, int mode, cudaStream_t s);
+void launch_maxdiff_batch(const BatchPlan& bp, cudaStream_t s);
 void launch_set_clock(DevClock* clk, double t, long long nn, cudaStream_t s);
 int report_error(int code, const char* msg);
 // (defined in k_mlp.cu) the wave-speed network on the realized moments of
@@ -178,6 +238,16 @@ __device__ __forceinline__ hyq::Seeds stage_seeds(const double* in, long long c,
 
 #ifdef __CUDACC__
 namespace hyqk {
+// The member whose blocks contain block `blk` of a fused launch.
+__device__ __forceinline__ int member_of(const Batch& b, int blk) {
+  int lo = 0, hi = b.n;  // b.blk0[lo] <= blk < b.blk0[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(b.blk0 + mid) <= blk) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
 __device__ __forceinline__ double nanmax(double a, double b) { return (a != a) ? a : ((b != b) ? b : fmax(a, b)); }
 
 __device__ __forceinline__ double warp_nanmax(double v) {

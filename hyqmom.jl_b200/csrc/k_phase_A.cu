@@ -57,13 +57,25 @@ __device__ __forceinline__ unsigned int* defer_list(double* vp, long long N) { r
 
 // A1: Flux_closure35_and_realizable_3D (realized moments only); also resets
 // the three list counters
-__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure(const double* __restrict__ M, double* __restrict__ out, double* vp,
-                                                              const StepConst sc, const DevClock* clk, long long c0, long long c1) {
+__device__ __forceinline__ void A1_body(const double* __restrict__ M, double* __restrict__ out, double* vp, const StepConst& sc,
+                                        const DevClock* clk, long long c0, long long c1, int bid) {
   if (!phase_A_active(sc, clk)) return;
-  const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
+  const long long N = sc.N, c = c0 + (long long)bid * BS_A + threadIdx.x;
   if (c == c0) { unsigned int* cnt = defer_list(vp, N) + N; cnt[0] = 0; cnt[1] = 0; cnt[2] = 0; }
   if (c >= c1) return;
   flux_closure35(M + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
+}
+__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure(const double* __restrict__ M, double* __restrict__ out, double* vp,
+                                                              const StepConst sc, const DevClock* clk, long long c0, long long c1) {
+  A1_body(M, out, vp, sc, clk, c0, c1, blockIdx.x);
+}
+// The fused-batch form of each kernel: the block's member from the table,
+// then the same body on that member's buffers over all its cells.
+__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure_b(const Batch bt) {
+  const int m = member_of(bt, blockIdx.x);
+  const Dom& d = bt.dom[m];
+  const StepConst sc = d.sc;
+  A1_body(d.buf[DB_M], d.buf[DB_FX], d.buf[DB_VP], sc, d.clk, 0, sc.N, blockIdx.x - __ldg(bt.blk0 + m));
 }
 
 // eigenvalues6_hyperbolic_3D along x (axis 1) or y (axis 2), and
@@ -98,16 +110,16 @@ __device__ __forceinline__ void count_flag(bool flag, unsigned long long* ctr) {
 // cells left go to the list, marked when they need the correction.  JAC_CP
 // counts the cells it had to leave to the LAPACK path (list code 0).
 template <int JM>
-__global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* in, double* out, double* vp,
-                                                         int axis, const StepConst sc, DevClock* clk, long long c0, long long c1) {
+__device__ __forceinline__ void A_eig_body(const double* in, double* out, double* vp, int axis, const StepConst& sc, DevClock* clk,
+                                           long long c0, long long c1, int bid) {
   if (!phase_A_active(sc, clk)) return;
   const bool dense = clk->dense[axis - 1] != 0;
-  if (JM == JAC_CP && blockIdx.x == 0 && threadIdx.x == 0) {
+  if (JM == JAC_CP && bid == 0 && threadIdx.x == 0) {
     atomicAdd(&clk->stage_cells, (unsigned long long)(c1 - c0));
     if (dense) atomicAdd(&clk->fb_cells, (unsigned long long)(c1 - c0));  // every cell to the LAPACK path
   }
   if (dense) return;
-  const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
+  const long long N = sc.N, c = c0 + (long long)bid * BS_A + threadIdx.x;
   if (c >= c1) return;
   double lo, hi;
   unsigned int code;
@@ -121,12 +133,24 @@ __global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* in, doub
     list[atomicAdd(list + N + (axis - 1), 1u)] = ((unsigned int)c << 3) | code;
   }
 }
+template <int JM>
+__global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig(const double* in, double* out, double* vp,
+                                                         int axis, const StepConst sc, DevClock* clk, long long c0, long long c1) {
+  A_eig_body<JM>(in, out, vp, axis, sc, clk, c0, c1, blockIdx.x);
+}
+template <int JM>
+__global__ void __launch_bounds__(BS_A, MINB_EIG) k_A_eig_b(const Batch bt, int r_in, int r_out, int axis) {
+  const int m = member_of(bt, blockIdx.x);
+  const Dom& d = bt.dom[m];
+  const StepConst sc = d.sc;
+  A_eig_body<JM>(d.buf[r_in], d.buf[r_out], d.buf[DB_VP], axis, sc, d.clk, 0, sc.N, blockIdx.x - __ldg(bt.blk0 + m));
+}
 
 // The general eigen-solve on the unmarked listed cells (dense: on every cell
 // of the range); marks (lists) the ones that need the correction.  One thread
 // per possible entry.
-__global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* in, double* out, double* vp, int axis,
-                                                         const StepConst sc, const DevClock* clk, long long c0, long long c1) {
+__device__ __forceinline__ void A_fix_body(const double* in, double* out, double* vp, int axis, const StepConst& sc, const DevClock* clk,
+                                           long long c0, long long c1, int bid, int nblk) {
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N;
   unsigned int* list = defer_list(vp, N);
@@ -134,14 +158,14 @@ __global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* in, doub
   double lo, hi;
   unsigned int code;
   if (clk->dense[axis - 1]) {
-    const long long c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
+    const long long c = c0 + (long long)bid * BS_A + threadIdx.x;
     if (c >= c1) return;
     if (eig_stage<FIX_MODE, false>(in, out, vp, c, axis, sc, lo, hi, &code) == EIG_DONE) { v[c] = lo; v[c + N] = hi; }
     else list[atomicAdd(list + N + (axis - 1), 1u)] = ((unsigned int)c << 3) | code;
     return;
   }
   const unsigned int count = list[N + (axis - 1)];
-  for (unsigned int e = blockIdx.x * BS_A + threadIdx.x; e < count; e += gridDim.x * BS_A) {
+  for (unsigned int e = bid * BS_A + threadIdx.x; e < count; e += nblk * BS_A) {
     const unsigned int entry = list[e];
     if (entry & 7u) continue;
     const long long c = entry >> 3;
@@ -149,23 +173,34 @@ __global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* in, doub
     else list[e] = entry | code;
   }
 }
+__global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* in, double* out, double* vp, int axis,
+                                                         const StepConst sc, const DevClock* clk, long long c0, long long c1) {
+  A_fix_body(in, out, vp, axis, sc, clk, c0, c1, blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix_b(const Batch bt, int r_in, int r_out, int axis) {
+  const int m = member_of(bt, blockIdx.x);
+  const Dom& d = bt.dom[m];
+  const StepConst sc = d.sc;
+  const int b0 = __ldg(bt.blk0 + m);
+  A_fix_body(d.buf[r_in], d.buf[r_out], d.buf[DB_VP], axis, sc, d.clk, 0, sc.N, blockIdx.x - b0, __ldg(bt.blk0 + m + 1) - b0);
+}
 
 // The marked listed cells: the correction from the recorded planes (code
 // 1-3), or the complete function (code 4, a z-stage re-realization); the first
 // thread then decides whether the stage runs dense next time
-__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A_corr(const double* in, double* out, double* vp,
-                                                              int axis, const StepConst sc, DevClock* clk, long long c0, long long c1) {
+__device__ __forceinline__ void A_corr_body(const double* in, double* out, double* vp, int axis, const StepConst& sc, DevClock* clk,
+                                            long long c0, long long c1, int bid, int nblk) {
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N;
   const unsigned int* list = defer_list(vp, N);
   const unsigned int count = list[N + (axis - 1)];
   double* v = vp + 2 * (axis - 1) * N;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (bid == 0 && threadIdx.x == 0) {
     int& d = clk->dense[axis - 1];
     if (d > 0) d = d - 1;
     else if ((long long)count * 4 > (c1 - c0) * 3) d = DENSE_RUNS;
   }
-  for (unsigned int e = blockIdx.x * BS_A + threadIdx.x; e < count; e += gridDim.x * BS_A) {
+  for (unsigned int e = bid * BS_A + threadIdx.x; e < count; e += nblk * BS_A) {
     const unsigned int entry = list[e];
     const int code = int(entry & 7u);
     if (!code) continue;
@@ -178,15 +213,26 @@ __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A_corr(const double* in,
     v[c] = lo; v[c + N] = hi;
   }
 }
+__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A_corr(const double* in, double* out, double* vp,
+                                                              int axis, const StepConst sc, DevClock* clk, long long c0, long long c1) {
+  A_corr_body(in, out, vp, axis, sc, clk, c0, c1, blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A_corr_b(const Batch bt, int r_in, int r_out, int axis) {
+  const int m = member_of(bt, blockIdx.x);
+  const Dom& d = bt.dom[m];
+  const StepConst sc = d.sc;
+  const int b0 = __ldg(bt.blk0 + m);
+  A_corr_body(d.buf[r_in], d.buf[r_out], d.buf[DB_VP], axis, sc, d.clk, 0, sc.N, blockIdx.x - b0, __ldg(bt.blk0 + m + 1) - b0);
+}
 
 // A5: closure of the realized moments with fluxes, 1-D closure speeds, the
 // six wave speeds and the NaN-propagating block max of |speed|
-__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A5_flux(const double* __restrict__ in, double* __restrict__ M, double* __restrict__ Fx,
-                                                           double* __restrict__ Fy, double* __restrict__ Fz, double* __restrict__ vp,
-                                                           double* __restrict__ blockmax, const StepConst sc, const DevClock* clk,
-                                                           long long c0, long long c1) {
+__device__ __forceinline__ void A5_body(const double* __restrict__ in, double* __restrict__ M, double* __restrict__ Fx,
+                                        double* __restrict__ Fy, double* __restrict__ Fz, double* __restrict__ vp,
+                                        double* __restrict__ blockmax, const StepConst& sc, const DevClock* clk, long long c0, long long c1,
+                                        int bid) {
   if (!phase_A_active(sc, clk)) return;
-  const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_A + threadIdx.x;
+  const long long N = sc.N, c = c0 + (long long)bid * BS_A + threadIdx.x;
   double local = 0.0;
   if (c < c1) {
     flux_closure35(in + c, sc.flag2D, sc.Ma, Fx + c, Fy + c, Fz + c, M + c, N, N, N);
@@ -204,7 +250,20 @@ __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A5_flux(const double* __
     }
   }
   const double bm = block_nanmax<BS_A>(local);
-  if (threadIdx.x == 0) blockmax[c0 / BS_A + blockIdx.x] = bm;  // c0 is a multiple of BS_A
+  if (threadIdx.x == 0) blockmax[c0 / BS_A + bid] = bm;  // c0 is a multiple of BS_A
+}
+__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A5_flux(const double* __restrict__ in, double* __restrict__ M, double* __restrict__ Fx,
+                                                           double* __restrict__ Fy, double* __restrict__ Fz, double* __restrict__ vp,
+                                                           double* __restrict__ blockmax, const StepConst sc, const DevClock* clk,
+                                                           long long c0, long long c1) {
+  A5_body(in, M, Fx, Fy, Fz, vp, blockmax, sc, clk, c0, c1, blockIdx.x);
+}
+__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A5_flux_b(const Batch bt) {
+  const int m = member_of(bt, blockIdx.x);
+  const Dom& d = bt.dom[m];
+  const StepConst sc = d.sc;
+  A5_body(d.buf[DB_MTMP], d.buf[DB_M], d.buf[DB_FX], d.buf[DB_FY], d.buf[DB_FZ], d.buf[DB_VP], d.buf[DB_BMAX], sc, d.clk, 0, sc.N,
+          blockIdx.x - __ldg(bt.blk0 + m));
 }
 
 __global__ void __launch_bounds__(BS_CELLS) k_cells_phase_A(const double* __restrict__ M, long long n, int flag2D, double Ma, int positivity,
@@ -241,6 +300,21 @@ void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, do
   }
   k_A5_flux<<<g, BS_A, 0, s>>>(Mtmp, M, Fx, Fy, Fz, vp, blockmax, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[4], s);
+}
+void launch_phase_A_batch(const BatchPlan& bp, int mode, cudaStream_t s, void (*after_a1)(void*, cudaStream_t), void* arg) {
+  const Batch cells = bp.of(DK_CELLS), corr = bp.of(DK_CORR);
+  const int g = bp.nblk[DK_CELLS], gc = bp.nblk[DK_CORR];
+  k_A1_closure_b<<<g, BS_A, 0, s>>>(cells);
+  if (after_a1) after_a1(arg, s);
+  const int ins[3] = {DB_FX, DB_FX, DB_FX};
+  const int outs[3] = {DB_FX, DB_FX, DB_MTMP};  // x and y in place
+  for (int axis = 1; axis <= 3; ++axis) {
+    if (mode == MODE_PLAIN) k_A_eig_b<EIG_MODE><<<g, BS_A, 0, s>>>(cells, ins[axis - 1], outs[axis - 1], axis);
+    else k_A_eig_b<JAC_CP><<<g, BS_A, 0, s>>>(cells, ins[axis - 1], outs[axis - 1], axis);
+    k_A_fix_b<<<g, BS_A, 0, s>>>(cells, ins[axis - 1], outs[axis - 1], axis);
+    k_A_corr_b<<<gc, BS_A, 0, s>>>(corr, ins[axis - 1], outs[axis - 1], axis);
+  }
+  k_A5_flux_b<<<g, BS_A, 0, s>>>(cells);
 }
 void launch_cells_phase_A(const double* M, long long n, int flag2D, double Ma, int positivity, double* Fx, double* Fy, double* Fz,
                           double* Mr, double* vp, cudaStream_t s) {

@@ -27,13 +27,25 @@ namespace {
 __device__ __forceinline__ unsigned int* fix_counters(double* vp, long long N) { return reinterpret_cast<unsigned int*>(vp + N); }
 
 // E1: Flux_closure35_and_realizable_3D; also resets the two fix counters
-__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E1_closure(const double* __restrict__ in, double* __restrict__ out, double* vp,
-                                                                const StepConst sc, const DevClock* clk, long long c0, long long c1) {
+__device__ __forceinline__ void E1_body(const double* __restrict__ in, double* __restrict__ out, double* vp, const StepConst& sc,
+                                        const DevClock* clk, long long c0, long long c1, int bid) {
   if (!clk->active) return;
-  const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
+  const long long N = sc.N, c = c0 + (long long)bid * BS_EF + threadIdx.x;
   if (c == c0) { unsigned int* cnt = fix_counters(vp, N); cnt[0] = 0; cnt[1] = 0; }
   if (c >= c1) return;
   flux_closure35(in + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
+}
+__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E1_closure(const double* __restrict__ in, double* __restrict__ out, double* vp,
+                                                                const StepConst sc, const DevClock* clk, long long c0, long long c1) {
+  E1_body(in, out, vp, sc, clk, c0, c1, blockIdx.x);
+}
+// The fused-batch form of each kernel: the block's member from the table,
+// then the same body on that member's buffers over all its cells.
+__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E1_closure_b(const Batch bt) {
+  const int m = member_of(bt, blockIdx.x);
+  const Dom& d = bt.dom[m];
+  const StepConst sc = d.sc;
+  E1_body(d.buf[DB_MTMP], d.buf[DB_FX], d.buf[DB_VP], sc, d.clk, 0, sc.N, blockIdx.x - __ldg(bt.blk0 + m));
 }
 
 // Warp-aggregated count of the calling threads with `flag` set, added to *ctr.
@@ -49,15 +61,15 @@ __device__ __forceinline__ void count_flag_ef(bool flag, unsigned long long* ctr
 // learned paths): that path or the certified solve, which decides a Jacobian
 // without its eigenvalues; the cells it leaves to the LAPACK path are counted.
 template <int JM>
-__global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* in, double* out, double* vp, int axis,
-                                                           int which, const StepConst sc, DevClock* clk, long long c0, long long c1) {
+__device__ __forceinline__ void E_eig_body(const double* in, double* out, double* vp, int axis, int which, const StepConst& sc, DevClock* clk,
+                                           long long c0, long long c1, int bid) {
   if (!clk->active) return;
   const bool dense = clk->dense[3 + which] != 0;
-  if (JM == JAC_CP && blockIdx.x == 0 && threadIdx.x == 0) {
+  if (JM == JAC_CP && bid == 0 && threadIdx.x == 0) {
     atomicAdd(&clk->stage_cells, (unsigned long long)(c1 - c0));
     if (dense) atomicAdd(&clk->fb_cells, (unsigned long long)(c1 - c0));
   }
-  const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
+  const long long N = sc.N, c = c0 + (long long)bid * BS_EF + threadIdx.x;
   if (c >= c1) return;
   // the learned path seeds the certified solve with the network's speeds of
   // this step (predicted in phase [A]; a poor seed only costs evaluations)
@@ -72,24 +84,36 @@ __global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* in, dou
     reinterpret_cast<unsigned long long*>(vp)[slot] = ((unsigned long long)c << 2) | (unsigned long long)(planes < 0 ? 0 : planes);
   }
 }
+template <int JM>
+__global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig(const double* in, double* out, double* vp, int axis,
+                                                           int which, const StepConst sc, DevClock* clk, long long c0, long long c1) {
+  E_eig_body<JM>(in, out, vp, axis, which, sc, clk, c0, c1, blockIdx.x);
+}
+template <int JM>
+__global__ void __launch_bounds__(BS_EF, MINB_EIG) k_E_eig_b(const Batch bt, int axis, int which) {
+  const int m = member_of(bt, blockIdx.x);
+  const Dom& d = bt.dom[m];
+  const StepConst sc = d.sc;
+  E_eig_body<JM>(d.buf[DB_FX], d.buf[DB_FX], d.buf[DB_VP], axis, which, sc, d.clk, 0, sc.N, blockIdx.x - __ldg(bt.blk0 + m));
+}
 
 // The undecided listed cells (dense: every cell of the range): their planes
 // from the general eigen-solve, written back into the entry (dense: listed).
 // One thread per possible entry.
-__global__ void __launch_bounds__(BS_EF, MINB_FIX) k_E_fix(const double* __restrict__ in, double* vp, int axis, int which,
-                                                           const StepConst sc, const DevClock* clk, long long c0, long long c1) {
+__device__ __forceinline__ void E_fix_body(const double* __restrict__ in, double* vp, int axis, int which, const StepConst& sc,
+                                           const DevClock* clk, long long c0, long long c1, int bid, int nblk) {
   if (!clk->active) return;
   const long long N = sc.N;
   unsigned long long* list = reinterpret_cast<unsigned long long*>(vp);
   if (clk->dense[3 + which]) {
-    const long long c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
+    const long long c = c0 + (long long)bid * BS_EF + threadIdx.x;
     if (c >= c1) return;
     const int planes = eigenvalues6_flags_t<FIX_MODE>(in + c, axis, N);
     if (planes) list[atomicAdd(fix_counters(vp, N) + which, 1u)] = ((unsigned long long)c << 2) | (unsigned long long)planes;
     return;
   }
   const unsigned int count = reinterpret_cast<const unsigned int*>(vp + N)[which];
-  for (unsigned int e = blockIdx.x * BS_EF + threadIdx.x; e < count; e += gridDim.x * BS_EF) {
+  for (unsigned int e = bid * BS_EF + threadIdx.x; e < count; e += nblk * BS_EF) {
     const unsigned long long v = list[e];
     if (v & 3ull) continue;
     const long long c = (long long)(v >> 2);
@@ -97,23 +121,33 @@ __global__ void __launch_bounds__(BS_EF, MINB_FIX) k_E_fix(const double* __restr
     if (planes) list[e] = v | (unsigned long long)planes;
   }
 }
+__global__ void __launch_bounds__(BS_EF, MINB_FIX) k_E_fix(const double* __restrict__ in, double* vp, int axis, int which,
+                                                           const StepConst sc, const DevClock* clk, long long c0, long long c1) {
+  E_fix_body(in, vp, axis, which, sc, clk, c0, c1, blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(BS_EF, MINB_FIX) k_E_fix_b(const Batch bt, int axis, int which) {
+  const int m = member_of(bt, blockIdx.x);
+  const Dom& d = bt.dom[m];
+  const StepConst sc = d.sc;
+  const int b0 = __ldg(bt.blk0 + m);
+  E_fix_body(d.buf[DB_FX], d.buf[DB_VP], axis, which, sc, d.clk, 0, sc.N, blockIdx.x - b0, __ldg(bt.blk0 + m + 1) - b0);
+}
 
 // The correction of the listed cells that need it
 // (correct_moments_for_real_eigenvalues, as in eigenvalues6); the first thread
 // then decides whether the stage runs dense next time
-__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E_corr(const double* in, double* out, const double* vp,
-                                                                int axis, int which, const StepConst sc, DevClock* clk, long long c0,
-                                                                long long c1) {
+__device__ __forceinline__ void E_corr_body(const double* in, double* out, const double* vp, int axis, int which, const StepConst& sc,
+                                            DevClock* clk, long long c0, long long c1, int bid, int nblk) {
   if (!clk->active) return;
   const long long N = sc.N;
   const unsigned int count = reinterpret_cast<const unsigned int*>(vp + N)[which];
   const unsigned long long* list = reinterpret_cast<const unsigned long long*>(vp);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (bid == 0 && threadIdx.x == 0) {
     int& d = clk->dense[3 + which];
     if (d > 0) d = d - 1;
     else if ((long long)count * 4 > (c1 - c0) * 3) d = DENSE_RUNS;
   }
-  for (unsigned int e = blockIdx.x * BS_EF + threadIdx.x; e < count; e += gridDim.x * BS_EF) {
+  for (unsigned int e = bid * BS_EF + threadIdx.x; e < count; e += nblk * BS_EF) {
     const unsigned long long v = list[e];
     const int planes = int(v & 3ull);
     if (!planes) continue;
@@ -124,18 +158,40 @@ __global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E_corr(const double* in
     for (int n = 0; n < 35; ++n) out[c + N * n] = Mc[n];
   }
 }
+__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E_corr(const double* in, double* out, const double* vp,
+                                                                int axis, int which, const StepConst sc, DevClock* clk, long long c0,
+                                                                long long c1) {
+  E_corr_body(in, out, vp, axis, which, sc, clk, c0, c1, blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E_corr_b(const Batch bt, int axis, int which) {
+  const int m = member_of(bt, blockIdx.x);
+  const Dom& d = bt.dom[m];
+  const StepConst sc = d.sc;
+  const int b0 = __ldg(bt.blk0 + m);
+  E_corr_body(d.buf[DB_FX], d.buf[DB_FX], d.buf[DB_VP], axis, which, sc, d.clk, 0, sc.N, blockIdx.x - b0, __ldg(bt.blk0 + m + 1) - b0);
+}
 
 // E4: Flux_closure35_and_realizable_3D, then collision35 with the step's dt
-__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E4_closure_bgk(const double* __restrict__ in, double* __restrict__ Mout, const StepConst sc,
-                                                                    const DevClock* clk, long long c0, long long c1) {
+__device__ __forceinline__ void E4_body(const double* __restrict__ in, double* __restrict__ Mout, const StepConst& sc, const DevClock* clk,
+                                        long long c0, long long c1, int bid) {
   if (!clk->active) return;
-  const long long N = sc.N, c = c0 + (long long)blockIdx.x * BS_EF + threadIdx.x;
+  const long long N = sc.N, c = c0 + (long long)bid * BS_EF + threadIdx.x;
   if (c >= c1) return;
   double a[35];
   flux_closure35(in + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, a, N, 1);
   collision35(a, clk->dt, sc.Kn, sc.positivity);
 #pragma unroll
   for (int n = 0; n < 35; ++n) Mout[c + N * n] = a[n];
+}
+__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E4_closure_bgk(const double* __restrict__ in, double* __restrict__ Mout, const StepConst sc,
+                                                                    const DevClock* clk, long long c0, long long c1) {
+  E4_body(in, Mout, sc, clk, c0, c1, blockIdx.x);
+}
+__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E4_closure_bgk_b(const Batch bt) {
+  const int m = member_of(bt, blockIdx.x);
+  const Dom& d = bt.dom[m];
+  const StepConst sc = d.sc;
+  E4_body(d.buf[DB_FX], d.buf[DB_M], sc, d.clk, 0, sc.N, blockIdx.x - __ldg(bt.blk0 + m));
 }
 
 }  // namespace
@@ -160,6 +216,20 @@ void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, doubl
   if (ev) cudaEventRecord(ev[2], s);
   k_E4_closure_bgk<<<g, BS_EF, 0, s>>>(Fx, Mout, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[3], s);
+}
+
+void launch_phase_EF_batch(const BatchPlan& bp, int mode, cudaStream_t s) {
+  const Batch cells = bp.of(DK_CELLS), corr = bp.of(DK_CORR);
+  const int g = bp.nblk[DK_CELLS], gc = bp.nblk[DK_CORR];
+  k_E1_closure_b<<<g, BS_EF, 0, s>>>(cells);
+  for (int which = 0; which < 2; ++which) {
+    const int axis = which + 1;
+    if (mode == MODE_PLAIN) k_E_eig_b<EIG_MODE><<<g, BS_EF, 0, s>>>(cells, axis, which);
+    else k_E_eig_b<JAC_CP><<<g, BS_EF, 0, s>>>(cells, axis, which);
+    k_E_fix_b<<<g, BS_EF, 0, s>>>(cells, axis, which);
+    k_E_corr_b<<<gc, BS_EF, 0, s>>>(corr, axis, which);
+  }
+  k_E4_closure_bgk_b<<<g, BS_EF, 0, s>>>(cells);
 }
 
 }  // namespace hyqk

@@ -33,6 +33,9 @@ class HyqIcRegion(ctypes.Structure):
 MODE_PLAIN, MODE_LEARNED, MODE_CERTIFIED = 0, 1, 2
 MODES = {"plain": MODE_PLAIN, "learned": MODE_LEARNED, "certified": MODE_CERTIFIED}
 NET_PARAMS = 38406  # HYQ_NET_PARAMS
+# launch variants (hyq_set_variant) and batch schedules (hyq_batch_set_schedule)
+KERNEL_HLL, KERNEL_CORR = 0, 1
+BATCH_BRANCHES, BATCH_FUSED = 0, 1
 
 
 class HyqStats(ctypes.Structure):
@@ -56,7 +59,8 @@ SYMBOLS = ["hyq_abi_version", "hyq_create", "hyq_destroy", "hyq_last_error", "hy
            "hyq_cells_eigenvalues", "hyq_cells_closure_eigs", "hyq_cells_collision", "hyq_cells_phase_A", "hyq_step_noalloc", "hyq_batch_create", "hyq_batch_destroy", "hyq_batch_size",
            "hyq_batch_member", "hyq_batch_stream", "hyq_batch_advance_async", "hyq_batch_advance", "hyq_reset_counters",
            "hyq_set_wavespeed_net", "hyq_net_image_bytes", "hyq_net_tile_bytes", "hyq_net_scratch_bytes", "hyq_net_pack",
-           "hyq_net_features", "hyq_net_forward", "hyq_net_train_batch", "hyq_net_adam", "hyq_cells_wavespeed_targets", "hyq_set_state_ic", "hyq_step_begin", "hyq_step_end", "hyq_copy_layers", "hyq_set_spacing"]
+           "hyq_net_features", "hyq_net_forward", "hyq_net_train_batch", "hyq_net_adam", "hyq_cells_wavespeed_targets", "hyq_set_state_ic", "hyq_step_begin", "hyq_step_end", "hyq_copy_layers", "hyq_set_spacing",
+           "hyq_variant_count", "hyq_set_variant", "hyq_batch_set_variant", "hyq_batch_set_schedule", "hyq_batch_schedule"]
 NOALLOC_MAX_CELLS = 16384  # HYQ_NOALLOC_MAX_CELLS
 
 
@@ -123,6 +127,13 @@ def load(path=None):
     lib.hyq_step_end.argtypes = [vp, vp]
     lib.hyq_copy_layers.argtypes = [vp, i32, i32, vp, i32]
     lib.hyq_set_spacing.argtypes = [vp, dbl, dbl, dbl]
+    lib.hyq_variant_count.argtypes = [i32]
+    lib.hyq_variant_count.restype = i32
+    lib.hyq_set_variant.argtypes = [vp, i32, i32]
+    lib.hyq_batch_set_variant.argtypes = [vp, i32, i32]
+    lib.hyq_batch_set_schedule.argtypes = [vp, i32]
+    lib.hyq_batch_schedule.argtypes = [vp]
+    lib.hyq_batch_schedule.restype = i32
     _lib = lib
     return lib
 

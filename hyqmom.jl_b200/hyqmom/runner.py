@@ -42,6 +42,7 @@ class Solver:
         p = params
         self._owns = _handle is None
         self.mode = mode
+        self.device = device
         if _handle is None:
             hp = params_struct(p, device, mode)
             h = ctypes.c_void_p()
@@ -61,6 +62,11 @@ class Solver:
         w = np.ascontiguousarray(net.params, dtype=np.float32)
         assert w.size == _lib.NET_PARAMS
         self._chk(self._lib.hyq_set_wavespeed_net(self._h, w.ctypes.data, float(net.margin)))
+
+    def set_variant(self, kernel, variant):
+        """Launch variant of a kernel ("hll"; hyq_set_variant): the same bits,
+        another launch shape."""
+        self._chk(self._lib.hyq_set_variant(self._h, _KERNELS[kernel], int(variant)))
 
     def close(self):
         if self._h:
@@ -167,21 +173,34 @@ class Solver:
         return self._lib.hyq_stream(self._h)
 
 
+_KERNELS = {"hll": _lib.KERNEL_HLL, "corr": _lib.KERNEL_CORR}
+
+
+def variant_count(kernel):
+    """Number of launch variants of a kernel ("hll", "corr")."""
+    return int(_lib.load().hyq_variant_count(_KERNELS[kernel]))
+
+
 class BatchSolver:
     """Independent domains stepped together (a hyq_batch): one CUDA graph
     replay advances every member that is not done by one step of its own dt.
     ``members[i]`` is a Solver view of member i (state, clock, stats)."""
 
-    def __init__(self, params_list, device=0):
+    def __init__(self, params_list, device=0, mode="plain", net=None):
         lib = _lib.load()
         n = len(params_list)
-        arr = (_lib.HyqParams * n)(*[params_struct(p, device) for p in params_list])
+        arr = (_lib.HyqParams * n)(*[params_struct(p, device, mode) for p in params_list])
         h = ctypes.c_void_p()
         rc = lib.hyq_batch_create(arr, n, ctypes.byref(h))
         if rc != 0:
             raise _lib.HyqError(f"{_lib.ERRORS.get(rc, rc)}: {lib.hyq_last_error(None).decode()}")
         self._lib, self._h = lib, h
         self.members = [Solver(p, device, _handle=lib.hyq_batch_member(h, i)) for i, p in enumerate(params_list)]
+        if mode == "learned":
+            from . import wavenet
+            net = net if net is not None else wavenet.load_default()
+            for m in self.members:
+                m.set_wavespeed_net(net)
 
     def close(self):
         if self._h:
@@ -215,6 +234,19 @@ class BatchSolver:
     @property
     def stream(self):
         return self._lib.hyq_batch_stream(self._h)
+
+    @property
+    def schedule(self):
+        """"fused" (one launch per kernel for all members) or "branches"."""
+        return "fused" if self._lib.hyq_batch_schedule(self._h) == _lib.BATCH_FUSED else "branches"
+
+    def set_schedule(self, schedule):
+        self._chk(self._lib.hyq_batch_set_schedule(self._h, _lib.BATCH_FUSED if schedule == "fused" else _lib.BATCH_BRANCHES))
+
+    def set_variant(self, kernel, variant):
+        """Launch variant of a kernel for every member ("hll" or "corr";
+        hyq_batch_set_variant): the same bits, another launch shape."""
+        self._chk(self._lib.hyq_batch_set_variant(self._h, _KERNELS[kernel], int(variant)))
 
 
 def _runner_params(params):

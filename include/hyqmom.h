@@ -270,26 +270,58 @@ int hyq_advance_timed(hyq_ctx* ctx, int64_t steps, float* ms);
  * many small domains (uneven grids, each with its own Ma, Kn, CFL, tmax,
  * nnmax and dt) leaves most of a B200 idle when run one at a time.  A batch
  * owns one ordinary context per member (hyq_batch_member returns it, for
- * hyq_set_state / hyq_get_state / hyq_stats_get) and one CUDA graph holding
- * every member's step as an independent branch: each replay advances every
- * member that is not done by one step, all members' kernels in flight
- * together.  Members stop on the device at their own tmax / nnmax or at a
+ * hyq_set_state / hyq_get_state / hyq_stats_get) and one CUDA graph per step
+ * in one of two schedules:
+ *   HYQ_BATCH_FUSED (default when all members share hyq_params.mode): one
+ *     launch per kernel of the step for ALL members; each block finds its
+ *     member in a table (constants, device clock, buffers) and works on that
+ *     member's cells, so a step is the same ~24 launches however many members
+ *     there are, and the block scheduler balances the (member, cell block)
+ *     queue of each launch;
+ *   HYQ_BATCH_BRANCHES: every member's own step graph as an independent
+ *     branch of the batch graph.
+ * Each replay advances every member that is not done by one step with its
+ * own dt.  Members stop on the device at their own tmax / nnmax or at a
  * non-finite wave speed (their stats status > 0); that is not an error of
- * the batch call.  Batch calls report failures through hyq_last_error(NULL). */
+ * the batch call.  Both schedules give every member the bits of its own
+ * hyq_advance.  Batch calls report failures through hyq_last_error(NULL). */
+#define HYQ_BATCH_BRANCHES 0
+#define HYQ_BATCH_FUSED 1
 typedef struct hyq_batch hyq_batch;
-int hyq_batch_create(const hyq_params* p, int32_t n, hyq_batch** out);  /* p[n], one device */
+int hyq_batch_create(const hyq_params* p, int32_t n, hyq_batch** out);  /* p[n], one device, n <= 4096 */
 void hyq_batch_destroy(hyq_batch* b);
 int32_t hyq_batch_size(const hyq_batch* b);
 hyq_ctx* hyq_batch_member(hyq_batch* b, int32_t i);  /* NULL when out of range */
 void* hyq_batch_stream(hyq_batch* b);                /* cudaStream_t of the replays */
+/* HYQ_EINVAL for a fused schedule over members of different modes. */
+int hyq_batch_set_schedule(hyq_batch* b, int32_t schedule);
+int32_t hyq_batch_schedule(const hyq_batch* b);
 /* Queue max_steps replays (after waiting for the members' own streams).
  * Each member's stream is then made to wait for the replays, so a later
  * member call (hyq_get_state, hyq_stats_get, hyq_set_state) sees the state
- * after them. */
+ * after them.  A member whose constants changed since the last replay
+ * (hyq_set_spacing, hyq_set_wavespeed_net, hyq_set_variant) is picked up by
+ * capturing the batch graph again. */
 int hyq_batch_advance_async(hyq_batch* b, int64_t max_steps);
 /* Same, then wait; ndone / nfailed (may be NULL) count members that are done
  * and members that met a non-finite wave speed. */
 int hyq_batch_advance(hyq_batch* b, int64_t max_steps, int32_t* ndone, int32_t* nfailed);
+
+/* ---- launch variants (for the autotuner) ----------------------------------
+ * Kernels with more than one launch shape; every variant gives the same bits,
+ * only the time differs.  hyqmom/autotune.py times them on the caller's own
+ * workload and keeps the choice per device.
+ *   HYQ_KERNEL_HLL: cells per block x moment groups of the HLL sweep
+ *     (0: 256 x 1, 1: 256 x 5, 2: 256 x 7, 3: 128 x 5, 4: 128 x 7, 5: 128 x 1);
+ *     per context (hyq_set_variant) or for every member of a batch.
+ *   HYQ_KERNEL_CORR: blocks per member of a fused batch's correction passes
+ *     (0: 64, 1: 16, 2: 4, 3: 592); batches only. */
+#define HYQ_KERNEL_HLL 0
+#define HYQ_KERNEL_CORR 1
+#define HYQ_CORR_VARIANTS 4
+int32_t hyq_variant_count(int32_t kernel);
+int hyq_set_variant(hyq_ctx* ctx, int32_t kernel, int32_t variant);
+int hyq_batch_set_variant(hyq_batch* b, int32_t kernel, int32_t variant);
 
 /* ---- allocation-free step ------------------------------------------------
  * No counterpart in the reference (its Julia loop allocates freely); added

@@ -209,3 +209,28 @@ def count_ops(M, params, dt):
     load().hyqo_count_ops(Nx, Ny, Nz, M.ctypes.data_as(_dp), ctypes.c_double(p["Kn"]), ctypes.c_double(p["Ma"]),
                           int(p["flag2D"]), int(p.get("positivity", True)), ctypes.c_double(dt), _p(out))
     return out
+
+
+def _field_rel(a, b):
+    a = a.reshape(-1, 35)
+    b = b.reshape(-1, 35)
+    return float(np.max(np.max(np.abs(a - b), axis=0) / np.maximum(np.max(np.abs(b), axis=0), 1e-300)))
+
+
+def one_ulp_spread(M, pp, t, trials=3, seed=0):
+    """The oracle's own one-step spread at state M: the largest field-relative
+    difference between its step from M and its steps from M with every entry
+    moved by one ulp (random direction), over `trials` perturbations."""
+    A = np.asfortranarray(M.copy())
+    step(A, pp, t)
+    rng = np.random.default_rng(seed)
+    worst = 0.0
+    for _ in range(trials):
+        flat = np.array(M, order="F").reshape(-1, order="F")
+        up = rng.random(flat.size) < 0.5
+        flat = np.where(up, np.nextafter(flat, np.inf), np.nextafter(flat, -np.inf))
+        B = np.asfortranarray(flat.reshape(M.shape, order="F"))
+        step(B, pp, t)
+        worst = max(worst, _field_rel(B, A))
+    return worst
+

@@ -1,5 +1,8 @@
 """Batched independent domains (hyq_batch): every member of one batch, with
-its own grid, parameters and dt, matches the same domain stepped alone."""
+its own grid, parameters and dt, matches the same domain stepped alone, bit
+for bit, in both schedules (fused member-table launches and graph branches)
+and every launch variant; the autotuner leaves the run where it was."""
+import os
 import numpy as np
 import pytest
 
@@ -48,15 +51,132 @@ def test_batch_members_match_single_runs():
     try:
         for m, p in zip(b.members, ps):
             m.set_state(ic.initial_state(p))
-        b.advance(3)                  # three one-step replays
-        ndone, nfailed = b.advance(9)  # one eight-step replay and one one-step replay
+        b.advance(3)
+        ndone, nfailed = b.advance(9)
         assert nfailed == 0
         for m, (Mref, sref) in zip(b.members, ref):
             st = m.stats()
             assert st["nn"] == sref["nn"] and st["t"] == sref["t"]
-            assert field_rel(m.get_state(), Mref) < 1e-12
+            assert np.array_equal(m.get_state(), Mref)
         # members stop at their own limits: 6 and 4 steps, and tmax = 0.02
         assert [m.stats()["nn"] for m in b.members][:2] == [6, 4]
         assert ndone == sum(bool(m.stats()["done"]) for m in b.members)
+    finally:
+        b.close()
+
+
+def single_runs(ps, steps, mode="plain"):
+    from hyqmom.runner import Solver
+    out = []
+    for p in ps:
+        s = Solver(p, mode=mode)
+        try:
+            s.set_state(ic.initial_state(p))
+            s.advance(steps)
+            out.append((s.get_state(), s.stats()))
+        finally:
+            s.close()
+    return out
+
+
+@pytest.mark.parametrize("schedule,mode,hll,corr", [("fused", "plain", 0, 0), ("branches", "plain", 0, 0), ("fused", "certified", 3, 1),
+                                                     ("fused", "plain", 2, 3), ("branches", "certified", 4, 0)])
+def test_schedules_and_variants_give_the_members_bits(schedule, mode, hll, corr):
+    cuda()
+    from hyqmom.runner import BatchSolver
+    ps = members()
+    ref = single_runs(ps, 12, mode)
+    b = BatchSolver(ps, mode=mode)
+    try:
+        assert b.schedule == "fused"  # the default when the members share a mode
+        b.set_schedule(schedule)
+        b.set_variant("hll", hll)
+        b.set_variant("corr", corr)
+        assert b.schedule == schedule
+        for m, p in zip(b.members, ps):
+            m.set_state(ic.initial_state(p))
+        b.advance(12)
+        for m, (Mref, sref) in zip(b.members, ref):
+            st = m.stats()
+            assert st["nn"] == sref["nn"] and st["t"] == sref["t"]
+            assert np.array_equal(m.get_state(), Mref)
+    finally:
+        b.close()
+
+
+def test_learned_members_in_a_fused_batch():
+    cuda()
+    from hyqmom import wavenet
+    from hyqmom.runner import BatchSolver
+    if not os.path.exists(wavenet.WEIGHTS_PATH):
+        pytest.skip("no trained network packaged")
+    ps = members()
+    ref = single_runs(ps, 8, "learned")
+    b = BatchSolver(ps, mode="learned")
+    try:
+        assert b.schedule == "fused"
+        for m, p in zip(b.members, ps):
+            m.set_state(ic.initial_state(p))
+        b.advance(8)
+        for m, (Mref, sref) in zip(b.members, ref):
+            assert m.stats()["t"] == sref["t"]
+            assert np.array_equal(m.get_state(), Mref)
+    finally:
+        b.close()
+
+
+def test_hll_variants_give_the_same_bits():
+    cuda()
+    from hyqmom.runner import Solver, variant_count
+    p = ic.with_jets(ic.default_params(Nx=20, Ny=18, Nz=10, Ma=1.0, Kn=0.1, CFL=0.5, tmax=10.0, nnmax=100), "crossing")
+    out = []
+    for v in range(variant_count("hll")):
+        s = Solver(p)
+        try:
+            s.set_variant("hll", v)
+            s.set_state(ic.initial_state(p))
+            s.advance(4)
+            out.append(s.get_state())
+        finally:
+            s.close()
+    assert len(out) == 6
+    for M in out[1:]:
+        assert np.array_equal(M, out[0])
+
+
+def test_autotuner_keeps_the_run_and_caches(tmp_path):
+    cuda()
+    from hyqmom import autotune
+    from hyqmom.runner import BatchSolver, Solver
+    path = str(tmp_path / "tune.json")
+    p = ic.with_jets(ic.default_params(Nx=24, Ny=24, Nz=12, Ma=1.0, Kn=0.1, CFL=0.5, tmax=10.0, nnmax=100), "crossing")
+    s = Solver(p)
+    try:
+        s.set_state(ic.initial_state(p))
+        s.advance(2)
+        before = s.get_state()
+        got = autotune.tune_solver(s, path=path)
+        assert not got["cached"] and 0 <= got["hll"] < 6
+        assert np.array_equal(s.get_state(), before) and s.stats()["nn"] == 2
+        again = autotune.tune_solver(s, path=path)
+        assert again["cached"] and again["hll"] == got["hll"]
+        s.advance(2)
+        tuned = s.get_state()
+    finally:
+        s.close()
+    ref = single_runs([p], 4)[0][0]
+    assert np.array_equal(tuned, ref)
+    ps = members()
+    b = BatchSolver(ps)
+    try:
+        for m, q in zip(b.members, ps):
+            m.set_state(ic.initial_state(q))
+        b.advance(2)
+        states = [m.get_state() for m in b.members]
+        choice = autotune.tune_batch(b, ps, path=path)
+        assert choice["schedule"] in ("fused", "branches") and not choice["cached"]
+        for m, M in zip(b.members, states):
+            assert np.array_equal(m.get_state(), M) and m.stats()["nn"] in (2,)
+        assert autotune.tune_batch(b, ps, path=path)["cached"]
     finally:
         b.close()

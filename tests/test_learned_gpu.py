@@ -163,11 +163,14 @@ def test_step_from_same_state_matches_oracle(mode):
 def test_every_step_of_a_run_meets_the_step_bar(mode):
     """100 steps of the certified / learned path on 20^3 crossing jets (Ma=1,
     Kn=0.01): every step agrees with the oracle's step from the same state to
-    1e-12 relative per moment field (FP64).  The difference to the plain
-    path's run after 100 steps is printed: it is O(1), because the scheme's
-    threshold branches amplify any round-off difference (the oracle itself
-    does the same to a one-ulp perturbation, test_oracle_sensitivity.py), so
-    only a bit-identical path meets a 100-step bar."""
+    1e-12 relative per moment field (FP64), or, at states where the oracle's
+    own step spreads one-ulp input perturbations further than that, to twice
+    that spread (oracle_lib.one_ulp_spread; around step 9, where the jets
+    meet, it is ~1e-10: test_oracle_sensitivity.py).  A path that rounds
+    differently cannot do better there, because the reference's own step does
+    not.  The difference to the plain path's run after 100 steps is printed:
+    it is O(1), as the threshold branches amplify any round-off difference,
+    so only a bit-identical path meets a 100-step bar."""
     need_gpu()
     from hyqmom.runner import Solver
     if mode == "learned" and not os.path.exists(wavenet.WEIGHTS_PATH):
@@ -177,6 +180,7 @@ def test_every_step_of_a_run_meets_the_step_bar(mode):
     M0 = ic.initial_state(p)
     g = Solver(p, mode=mode)
     worst = 0.0
+    conditioned = []
     try:
         g.set_state(M0)
         for k in range(100):
@@ -187,7 +191,11 @@ def test_every_step_of_a_run_meets_the_step_bar(mode):
             _, to, _ = ol.step(Mo, pp, tprev)
             d = field_rel(Mg, Mo)
             worst = max(worst, d)
-            assert d <= 1e-12 and abs(st["t"] - to) <= 1e-12 * to, (k, d)
+            assert abs(st["t"] - to) <= 1e-12 * to, (k, st["t"], to)
+            if d > 1e-12:
+                spread = ol.one_ulp_spread(Mprev, pp, tprev)
+                conditioned.append((k + 1, d, spread))
+                assert d <= 2.0 * spread, (k + 1, d, spread)
         Ml, stl = g.get_state(), g.stats()
     finally:
         g.close()
@@ -198,6 +206,8 @@ def test_every_step_of_a_run_meets_the_step_bar(mode):
         Mp, sp = s.get_state(), s.stats()
     finally:
         s.close()
+    print(f"{mode}: steps over 1e-12 (step, difference, oracle's one-ulp spread): "
+          + ", ".join(f"({k}, {d:.2e}, {s_:.2e})" for k, d, s_ in conditioned))
     print(f"{mode}: worst per-step field-relative difference {worst:.3e}; after 100 steps vs plain {field_rel(Ml, Mp):.3e} "
           f"(t {stl['t']:.17g} vs {sp['t']:.17g}); fallback {stl['fallback_cells']}/{stl['stage_cells']}")
 
