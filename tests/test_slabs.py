@@ -109,6 +109,55 @@ def test_gloo_slabs_equal_single_domain(world):
         assert np.array_equal(own, M[:, :, k0:k0 + own.shape[2], :]), rank
 
 
+def _rank_leaves(rank, world, port, q):
+    """Rank 1 steps once and leaves (between steps, nothing in flight); rank
+    0 goes on and its next collective must end with an error, not hang."""
+    import datetime
+    import time
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    p = crossing()
+    eng = OracleSlab(p, world, rank)
+    buf = lambda shape: torch.zeros(shape, dtype=torch.float64)  # noqa: E731
+    slabs.step(eng, rank, world, eng.layout, dist, buf)
+    def put(x):  # flushed before the process ends without clean-up
+        q.put(x)
+        q.close()
+        q.join_thread()
+
+    if rank == 1:
+        put((rank, "left"))
+        os._exit(0)
+    t0 = time.time()
+    try:
+        slabs.step(eng, rank, world, eng.layout, dist, buf)
+        put((rank, "no error"))
+    except Exception as e:  # the gloo timeout or the closed connection
+        put((rank, f"error after {time.time() - t0:.1f} s: {type(e).__name__}"))
+    os._exit(0)
+
+
+def test_a_rank_that_leaves_ends_the_next_step_with_an_error():
+    """Failure detection on the host: a slab rank that exits between steps
+    makes the other rank's next step raise within the process group's
+    timeout instead of waiting for ever (no GPU involved)."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_rank_leaves, args=(r, 2, port, q)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    got = dict(q.get(timeout=120) for _ in range(2))
+    for pr in procs:
+        pr.join(timeout=60)
+    print(got)
+    assert got[1] == "left"
+    assert got[0].startswith("error after"), got[0]
+    assert float(got[0].split()[2]) < 60.0
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("nslabs", [2, 3])
 def test_gpu_slabs_equal_single_domain(nslabs):
