@@ -48,22 +48,27 @@ STAGE_KERNELS = {k: f"k_{p}_eig+k_{p}_fix+k_{p}_corr ({k[-1]})" for k, p in
                  (("A2_eig_x", "A"), ("A3_eig_y", "A"), ("A4_eig_z", "A"), ("E2_eig_x", "E"), ("E3_eig_y", "E"))}
 KERNELS = ["A1_closure", "A2_eig_x", "A3_eig_y", "A4_eig_z", "A5_flux_speeds", "cfl", "hll",
            "E1_closure", "E2_eig_x", "E3_eig_y", "E4_closure_bgk"]
-# DRAM bytes (read + write) per cell of each kernel from ncu captures of the
-# plain step on 96 x 96 x 48 crossing jets (eigenvalue stages at step 151,
-# closures and HLL at the first step), scaled to a launch by its cells.
-TRAFFIC_PER_CELL = {"A1_closure": 3221.0, "A2_eig_x": 3531.0, "A3_eig_y": 3546.0, "A4_eig_z": 4028.0, "A5_flux_speeds": 4487.0,
-                    "hll": 1609.0, "E1_closure": 3211.0, "E4_closure_bgk": 3951.0}
-TRAFFIC_SOURCE = ("ncu dram__bytes_read+write per cell of the plain step on 96x96x48 crossing jets, scaled to this launch's cells")
+# DRAM bytes (read + write) per cell of each timed slot of the learned path
+# (an eigenvalue stage: its kernel and passes; A1: the closure and the
+# network), from ncu captures of steps 151-152 of crossing jets 128 x 128 x 64
+# (Ma=1, Kn=0.01), scaled to a launch by its cells; the HLL slot per launch
+# variant.
+TRAFFIC_PER_CELL = {"A1_closure": 2647.0, "A2_eig_x": 837.6, "A3_eig_y": 863.2, "A4_eig_z": 1797.3, "A5_flux_speeds": 3592.8,
+                    "E1_closure": 2345.6, "E2_eig_x": 676.3, "E3_eig_y": 663.3, "E4_closure_bgk": 3125.7}
+TRAFFIC_HLL = {0: 1741.0, 1: 1532.7, 2: 1507.0, 3: 1531.3, 4: 1508.3, 5: 1750.8}
+TRAFFIC_SOURCE = ("ncu dram__bytes_read+write per cell, learned path, steps 151-152 of crossing jets 128x128x64 (Ma=1, Kn=0.01), "
+                  "scaled to this launch's cells")
 MODES = ("plain", "certified", "learned")
 E2E_SLABS = 4
 
 
-RUN_STEPS = {"c5": 500, "c2": 200, "c2s": 200, "c1": 100}
+RUN_STEPS = {"c5": 500, "c5s": 500, "c2": 200, "c2s": 200, "c1": 100}
 
 
 def workload(name="c5"):
     """Crossing jets (the reference's IC generator): c5 256x256x128 Ma=1
-    Kn=0.01 (the headline, 500 steps); c2 160x160x80 Ma=1 Kn=1 (200 steps);
+    Kn=0.01 (the headline, 500 steps); c5s the c5 case on 128x128x64
+    (profiling captures); c2 160x160x80 Ma=1 Kn=1 (200 steps);
     c2s the c2 case on 96x96x48 (profiling captures); c1 20^3 Ma=0 Kn=1.
     CFL 0.5 for c5/c2/c2s: at the named 0.7 the scheme turns a flux Jacobian
     non-finite within a few steps of this IC (the reference's eigvals throws
@@ -71,6 +76,8 @@ def workload(name="c5"):
     from hyqmom import ic
     if name == "c5":
         p = ic.default_params(Nx=256, Ny=256, Nz=128, Ma=1.0, Kn=0.01, CFL=0.5, tmax=1e9, nnmax=1000000)
+    elif name == "c5s":
+        p = ic.default_params(Nx=128, Ny=128, Nz=64, Ma=1.0, Kn=0.01, CFL=0.5, tmax=1e9, nnmax=1000000)
     elif name == "c2":
         p = ic.default_params(Nx=160, Ny=160, Nz=80, Ma=1.0, Kn=1.0, CFL=0.5, tmax=1e9, nnmax=1000000)
     elif name == "c2s":
@@ -157,6 +164,15 @@ def fp64_peak_tflops(torch):
         best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
     del a, b
     return best
+
+
+def measured_hbm_gbs():
+    """The measured HBM copy bandwidth of this pool's B200s, when recorded."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return None
 
 
 def slab_of(M, nz):
@@ -365,7 +381,8 @@ def run_gpu(args, rank, world, local_rank):
     ach = F_kernel[dom] * cells / (lk[dom] * 1e-3) / 1e12
     step_ms = tot["learned"] / k
     step_tflops = F_alg * cells / (step_ms * 1e-3) / 1e12
-    traffic = TRAFFIC_PER_CELL[dom] * cells if dom in TRAFFIC_PER_CELL else None
+    per_cell = TRAFFIC_HLL.get(tune["hll"]) if dom == "hll" else TRAFFIC_PER_CELL.get(dom)
+    traffic = per_cell * cells if per_cell else None
     roof = {"bound": "fp64", "achieved": ach, "peak": fp64, "unit": "TFLOP/s", "frac": ach / fp64, "traffic": traffic,
             "traffic_source": TRAFFIC_SOURCE if traffic else None,
             "peak_source": "measured in this run: FP64 DGEMM 8192^3 (cuBLAS via torch), best of 3",
@@ -374,6 +391,11 @@ def run_gpu(args, rank, world, local_rank):
                      "the learned path's mean launch time; built with -fmad=false, so an FMA-free kernel tops out at peak/2"),
             "step": {"f_alg_per_cell": F_alg, "achieved": step_tflops, "frac": step_tflops / fp64,
                      "hbm_achieved_gbs": B_ALG * cells / (step_ms * 1e-3) / 1e9}}
+    hbm_peak = measured_hbm_gbs()
+    if hbm_peak:
+        roof["step"]["hbm_peak_gbs"] = hbm_peak
+        roof["step"]["hbm_frac"] = roof["step"]["hbm_achieved_gbs"] / hbm_peak
+        roof["step"]["hbm_peak_source"] = "MEASURED_PEAKS.json (copy bandwidth)"
     modes = {m: {"value": value[m], "ms_per_step": tot[m] / k, "kernels_ms": per_kernel[m],
                  "launches_per_step": LAUNCHES_PER_STEP[m]} for m in MODES}
     for m in fb:
@@ -563,13 +585,54 @@ def run_batch(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_case(args, local_rank):
+    """A fixed sequence of launches for ncu captures (no timing): the
+    workload on one path from its initial condition, `before` steps, then
+    `after` more; or (hll) one step per HLL launch variant from the state
+    after `before` steps, checking that every variant gives the same bits."""
+    import torch
+    from hyqmom import ic
+    from hyqmom.runner import Solver, variant_count
+    torch.cuda.set_device(local_rank)
+    p = workload(args.config)
+    mode, before, after = args.profile[0], int(args.profile[1]), int(args.profile[2])
+    s = Solver(p, device=local_rank, mode="plain" if mode == "hll" else mode)
+    s.set_state(ic.initial_state(p))
+    s.advance(before)
+    if mode != "hll":
+        s.advance(after)
+        print(json.dumps({"profile": mode, "config": args.config, "stats": s.stats()}), flush=True)
+        s.close()
+        return
+    st = s.stats()
+    buf = torch.empty(35 * p["Nx"] * p["Ny"] * p["Nz"], dtype=torch.float64, device="cuda")
+    s.get_state_device(buf.data_ptr())
+    s.synchronize()
+    ref, same = None, []
+    for v in range(variant_count("hll")):
+        s.set_variant("hll", v)
+        s.set_state_device(buf.data_ptr())
+        s.set_clock(st["t"], st["nn"])
+        s.synchronize()
+        s.advance(1)
+        M = s.get_state()
+        ref = M if ref is None else ref
+        same.append(bool(np.array_equal(M, ref)))
+    s.close()
+    print(json.dumps({"profile": "hll", "config": args.config, "variants_same_bits": same}), flush=True)
+    if not all(same):
+        raise SystemExit("HLL variants differ")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20, help="steps timed, spread evenly over the run")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c5", choices=["c1", "c2", "c2s", "c4", "c5"])
+    ap.add_argument("--config", default="c5", choices=["c1", "c2", "c2s", "c4", "c5", "c5s"])
+    ap.add_argument("--profile", nargs=3, metavar=("MODE", "BEFORE", "AFTER"),
+                    help="launch sequence for ncu captures: MODE plain|certified|learned|hll")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-mode", default="plain", choices=["plain", "certified", "learned"],
                     help="--config c4: the members' eigenvalue path")
@@ -581,6 +644,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.profile:
+        return run_profile_case(args, local_rank)
     if args.config == "c4":
         return run_batch(args, rank, world, local_rank)
     if args.decompose == "slabs":

@@ -620,7 +620,7 @@ int hyq_create(const hyq_params* p, hyq_ctx** out) {
   auto alloc = [&](double** ptr, size_t bytes) { return cudaMalloc((void**)ptr, bytes); };
   if (alloc(&ctx->M, b35) != cudaSuccess || alloc(&ctx->Mtmp, b35) != cudaSuccess || alloc(&ctx->Fx, b35) != cudaSuccess ||
       alloc(&ctx->Fy, b35) != cudaSuccess || alloc(&ctx->Fz, b35) != cudaSuccess ||
-      alloc(&ctx->vp, sizeof(double) * (7 * (size_t)N + 2)) != cudaSuccess ||
+      alloc(&ctx->vp, sizeof(double) * (7 * (size_t)N + 16)) != cudaSuccess ||
       alloc(&ctx->blockmax, sizeof(double) * (size_t)sc.nblocksA) != cudaSuccess ||
       cudaMalloc((void**)&ctx->clk, sizeof(DevClock)) != cudaSuccess) {
     cudaGetLastError();

@@ -19,10 +19,13 @@
 // remaining four, and then CERTIFIES the result: at seven points, one below
 // the smallest root, one between each pair of neighbours and one above the
 // largest, the polynomial must take the alternating signs + - + - + - + with
-// |value| above a rigorous bound on its Horner rounding error.  By the
-// intermediate value theorem that proves six distinct real roots, one in
-// each gap, so the extremes found are the extremes of the spectrum and no
-// eigenvalue is complex.  The five interior sign values must also exceed
+// |value| above a rigorous bound on its Horner rounding error plus the
+// rounding error of the coefficients themselves (the determinant expansion,
+// the shift and the scaling, bounded by evaluating the same expressions on
+// absolute values).  By the intermediate value theorem that proves that the
+// exact characteristic polynomial of J (the matrix as given) has six
+// distinct real roots, one in each gap, so the extremes found are the
+// extremes of the spectrum and no eigenvalue is complex.  The five interior sign values must also exceed
 // GAP_VAL, which proves neighbouring roots at least 1.26e-6 apart
 // (normalised): LAPACK's own rounding then cannot turn a pair complex, so a
 // certified Jacobian is one the reference's complex test passes.
@@ -45,6 +48,12 @@ constexpr int ITMAX = 40;              // Newton iterations per root
 constexpr double NEWTON_TOL = 1e-12;   // extremes: |dx| <= TOL (1 + |x|), then one more step
 constexpr double LOOSE_TOL = 1e-2;     // interior roots: only separating points are needed
 constexpr double CERT_ERR = 40.0 * 2.220446049250313e-16;  // > gamma_12 of the Horner bound
+// Rounding bounds of the coefficients (u = 2^-53): the charpoly expressions
+// take at most 12 operations along any path (gamma_16 used), the Taylor
+// shift 12 (gamma_16 used), the scaling by r^(6-k) up to 8 (gamma_10 used).
+constexpr double G_CP = 16.0 * 1.1102230246251565e-16 / (1.0 - 16.0 * 1.1102230246251565e-16);
+constexpr double G_SH = G_CP;
+constexpr double G_SC = 10.0 * 1.1102230246251565e-16 / (1.0 - 10.0 * 1.1102230246251565e-16);
 constexpr double ROOT_BOUND = 2.25;    // |x| <= sqrt(5) when all roots are real, sum x = 0, sum x^2 = 6
 // |b(y)| at a point y between neighbouring roots r_k < y < r_k+1 bounds their
 // distance from below: |b(y)| <= |y - r_k| |y - r_k+1| * D with D <= 5^4 the
@@ -58,14 +67,18 @@ constexpr double GAP_VAL = 1e-9;
 // (normalised): a pair that close stays real under LAPACK's rounding, which
 // moves a near-double pair by about sqrt(eps |J|) ~ 1e-8.
 constexpr double GAP_MIN = 1e-6;
-// The extremes must also be well conditioned: the Horner rounding bound of
-// b at the root over |b'| (the first-order error of the computed root) at
-// most EXT_ERR (normalised).  An extreme in a tight cluster has a small b'
-// and an error far above round-off, in this solve and in the LAPACK path
-// alike, so the two would differ by more than round-off; such Jacobians go
-// to the LAPACK path.
+// The extremes must also be well conditioned: the rounding bound of b at the
+// root (Horner's and the coefficients') over |b'| -- the first-order error of
+// the computed root -- at most EXT_ERR (normalised), so that the speeds
+// differ from the exact extremes by at most 1e-12 of the spread.  An extreme
+// in a tight cluster has a small b' and an error far above round-off, in
+// this solve and in the LAPACK path alike, so the two would differ by more
+// than round-off; such Jacobians go to the LAPACK path.  (The bound is
+// pessimistic: on evolved states of the 256 x 256 x 128 run the certified
+// extremes differ from the LAPACK path's by at most 9e-15 of the largest
+// |eigenvalue|.)
 #ifndef HQ_CP_EXT_ERR
-#define HQ_CP_EXT_ERR 2e-13
+#define HQ_CP_EXT_ERR 1e-12
 #endif
 constexpr double EXT_ERR = HQ_CP_EXT_ERR;
 
@@ -117,6 +130,34 @@ HQD void charpoly(const double* r3, const double* r5, const double* r6, double (
   c[6] = 1.0;
 }
 
+// The same expansion on absolute values (every term added): cabs[k] bounds
+// the terms that make up c[k], so |computed c[k] - exact c[k]| <= G_CP cabs[k].
+HQD void charpoly_abs(const double* r3, const double* r5, const double* r6, double (&cabs)[7]) {
+  double R3[6], R5[6], R6[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) { R3[k] = fabs(r3[k]); R5[k] = fabs(r5[k]); R6[k] = fabs(r6[k]); }
+  const double d0 = R5[3] * R6[5] + R5[5] * R6[3];
+  const double d1 = R5[3] + R5[4] * R6[5] + R5[5] * R6[4];
+  const double d2 = R5[4] + R6[5];
+  const double e0 = R5[0] * R6[5] + R5[5] * R6[0];
+  const double e1 = R5[0] + R5[1] * R6[5] + R5[5] * R6[1];
+  const double e2 = R5[1] + R5[2] * R6[5] + R5[5] * R6[2];
+  const double e3 = R5[2];
+  const double f0 = R5[0] * R6[3] + R5[3] * R6[0];
+  const double f1 = R5[0] * R6[4] + R5[1] * R6[3] + R5[3] * R6[1] + R5[4] * R6[0];
+  const double f2 = R5[1] * R6[4] + R5[2] * R6[3] + R5[3] * R6[2] + R5[4] * R6[1] + R6[0];
+  const double f3 = R5[2] * R6[4] + R5[4] * R6[2] + R6[1];
+  const double f4 = R6[2];
+  const double a0 = R3[0], a1 = R3[1], a2 = R3[2], b0 = R3[3], b1 = R3[4], g = R3[5];
+  cabs[0] = a0 * d0 + b0 * e0 + g * f0;
+  cabs[1] = a0 * d1 + a1 * d0 + b0 * e1 + b1 * e0 + g * f1;
+  cabs[2] = a0 * d2 + a1 * d1 + a2 * d0 + b0 * e2 + b1 * e1 + g * f2;
+  cabs[3] = a0 + a1 * d2 + a2 * d1 + d0 + b0 * e3 + b1 * e2 + g * f3;
+  cabs[4] = a1 + a2 * d2 + d1 + b1 * e3 + g * f4;
+  cabs[5] = a2 + d2;
+  cabs[6] = 0.0;
+}
+
 // p(x) and p'(x) of the degree-N polynomial d[0..N] by Horner.
 template <int N> HQD void horner2(const double* d, double x, double& p, double& dp) {
   p = d[N];
@@ -131,29 +172,42 @@ template <int N> HQD void horner2(const double* d, double x, double& p, double& 
 // The monic degree-6 polynomial c centred and scaled: b(x) = c(s + sig x) /
 // sig^6 with s = -c5 / 6 (mean root) and sig^2 = (a5^2 - 2 a4) / 6 (mean
 // square deviation, a = c shifted to s), so that sum x_i = -b5 ~ 0 and
-// sum x_i^2 = 6.  False when that spread is not a positive finite number.
-HQD bool normalize(const double (&c)[7], double& s, double& sig, double (&b)[7]) {
-  double a[7];
+// sum x_i^2 = 6.  With x = (lam - s) r, r = 1 / sig as rounded, eb[k] bounds
+// |b[k] - the exact coefficient| given |c[k] - exact c[k]| <= G_CP cabs[k]
+// (the shift's and the scaling's rounding included).  False when the spread
+// is not a positive finite number.
+HQD bool normalize(const double (&c)[7], const double (&cabs)[7], double& s, double& sig, double (&b)[7], double (&eb)[7]) {
+  double a[7], v[7];
 #pragma unroll
-  for (int k = 0; k < 7; ++k) a[k] = c[k];
+  for (int k = 0; k < 7; ++k) {
+    a[k] = c[k];
+    v[k] = G_CP * cabs[k] + G_SH * fabs(c[k]);
+  }
   s = -c[5] / 6.0;
-  // Taylor shift a(x) = c(x + s), repeated synthetic division
+  const double as = fabs(s);
+  // Taylor shift a(x) = c(x + s), repeated synthetic division; v the same
+  // shift of the error terms with |s| (all terms positive)
 #pragma unroll
   for (int i = 0; i < 6; ++i)
 #pragma unroll
-    for (int k = 5; k >= i; --k) a[k] = fma(s, a[k + 1], a[k]);
-  const double v = (a[5] * a[5] - 2.0 * a[4]) / 6.0;
-  if (!(v > 0.0) || !(v < 1.79769313486231571e308)) return false;
-  sig = sqrt(v);
+    for (int k = 5; k >= i; --k) {
+      a[k] = fma(s, a[k + 1], a[k]);
+      v[k] = fma(as, v[k + 1], v[k]);
+    }
+  const double vv = (a[5] * a[5] - 2.0 * a[4]) / 6.0;
+  if (!(vv > 0.0) || !(vv < 1.79769313486231571e308)) return false;
+  sig = sqrt(vv);
   const double r = 1.0 / sig;
   double pw = 1.0;
   bool fin = true;
   b[6] = 1.0;
+  eb[6] = 0.0;
 #pragma unroll
   for (int k = 5; k >= 0; --k) {
     pw = pw * r;
     b[k] = a[k] * pw;
-    fin = fin && isfinite(b[k]);
+    eb[k] = (v[k] * pw + G_SC * fabs(b[k])) * (1.0 + 1e-12);
+    fin = fin && isfinite(b[k]) && isfinite(eb[k]);
   }
   return fin;
 }
@@ -207,17 +261,19 @@ template <int N> HQD void deflate(const double* d, double x, double* q) {
   for (int k = N - 1; k >= 1; --k) q[k - 1] = fma(x, q[k], d[k]);
 }
 
-// Sign of b at y certified against its Horner rounding error and against
-// the floor `floor_val`: +1 / -1, or 0 when |b(y)| does not exceed both.
-HQD int certified_sign(const double (&b)[7], double y, double floor_val) {
-  double p = b[6], bound = 1.0;
+// Sign of the exact normalised polynomial at y, certified from the computed
+// b: |b(y)| must exceed its Horner rounding error, the coefficients' error
+// bound sum eb[k] |y|^k and the floor `floor_val`: +1 / -1, or 0.
+HQD int certified_sign(const double (&b)[7], const double (&eb)[7], double y, double floor_val) {
+  double p = b[6], bound = 1.0, ce = eb[6];
   const double ay = fabs(y);
 #pragma unroll
   for (int k = 5; k >= 0; --k) {
     p = fma(p, y, b[k]);
     bound = bound * ay + fabs(b[k]);
+    ce = ce * ay + eb[k];
   }
-  const double err = jmax(CERT_ERR * bound, floor_val);
+  const double err = jmax((CERT_ERR * bound + ce) * (1.0 + 1e-12), floor_val);
   if (p > err) return 1;
   if (p < -err) return -1;
   return 0;
@@ -247,7 +303,7 @@ struct CpOut {
 // interior sign values must exceed GAP_VAL (a rigorous lower bound on every
 // gap); tight = true: interior roots converged, their computed gaps must be
 // at least GAP_MIN and the signs only beyond the rounding bound.
-HQD bool interior_certify(const double (&b)[7], double x1, double x6, bool tight, int& its) {
+HQD bool interior_certify(const double (&b)[7], const double (&eb)[7], double x1, double x6, bool tight, int& its) {
   double d5[6], d4[5], d3[4], d2[3];
   deflate<6>(b, x1, d5);
   deflate<5>(d5, x6, d4);
@@ -295,12 +351,12 @@ HQD bool interior_certify(const double (&b)[7], double x1, double x6, bool tight
   y[6] = r[5] + 0.5 * (r[5] - r[4]);
 #pragma unroll
   for (int k = 0; k < 7; ++k)
-    ok = ok && (certified_sign(b, y[k], (k == 0 || k == 6 || tight) ? 0.0 : GAP_VAL) == ((k & 1) ? -1 : 1));
+    ok = ok && (certified_sign(b, eb, y[k], (k == 0 || k == 6 || tight) ? 0.0 : GAP_VAL) == ((k & 1) ? -1 : 1));
   its += 7;
   return ok;
 }
 
-HQD CpOut solve(const double (&b)[7], double xhi, double xlo) {
+HQD CpOut solve(const double (&b)[7], const double (&eb)[7], double xhi, double xlo) {
   CpOut o;
   o.ok = false;
   o.its = 0;
@@ -311,21 +367,22 @@ HQD CpOut solve(const double (&b)[7], double xhi, double xlo) {
   if (!(x6 < x1)) return o;
   // interior roots placed loosely first; a cluster (a near-double interior
   // pair, common in nearly Gaussian cells) needs them converged
-  if (!interior_certify(b, x1, x6, false, o.its) && !interior_certify(b, x1, x6, true, o.its)) return o;
+  if (!interior_certify(b, eb, x1, x6, false, o.its) && !interior_certify(b, eb, x1, x6, true, o.its)) return o;
   // conditioning of the two extremes
   bool ok = true;
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
     const double x = q ? x1 : x6;
-    double p = b[6], dp = 0.0, bound = 1.0;
+    double p = b[6], dp = 0.0, bound = 1.0, ce = eb[6];
     const double ax = fabs(x);
 #pragma unroll
     for (int k = 5; k >= 0; --k) {
       dp = fma(dp, x, p);
       p = fma(p, x, b[k]);
       bound = bound * ax + fabs(b[k]);
+      ce = ce * ax + eb[k];
     }
-    ok = ok && (CERT_ERR * bound <= EXT_ERR * fabs(dp));
+    ok = ok && (CERT_ERR * bound + ce <= EXT_ERR * fabs(dp));
   }
   o.its += 2;
   if (!ok) return o;
@@ -372,12 +429,13 @@ HQD Extremes extremes(const double* r3, const double* r5, const double* r6, doub
   e.ok = false;
   e.its = 0;
   e.vmin = e.vmax = 0.0;
-  double c[7], b[7], s, sig;
+  double c[7], cabs[7], b[7], eb[7], s, sig;
   charpoly(r3, r5, r6, c);
-  if (!normalize(c, s, sig, b)) return e;
+  charpoly_abs(r3, r5, r6, cabs);
+  if (!normalize(c, cabs, s, sig, b, eb)) return e;
   const double xhi = start_above(b, (hi_seed - s) / sig + margin);
   const double xlo = start_below(b, (lo_seed - s) / sig - margin);
-  const CpOut o = solve(b, xhi, xlo);
+  const CpOut o = solve(b, eb, xhi, xlo);
   e.its = o.its + 2;
   if (!o.ok) return e;
   e.vmin = s + sig * o.xmin;

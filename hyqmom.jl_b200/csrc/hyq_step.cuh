@@ -142,7 +142,7 @@ struct BatchPlan {
 // launch wrappers (defined in k_phase_A.cu, k_phase_EF.cu, k_cells.cu)
 // Phase [A] in place on M; Mtmp, Fx, Fy, Fz carry its intermediate states,
 // and on completion Fx, Fy, Fz hold the fluxes (Mtmp is left as scratch).
-// vp: 7N + 2 doubles, the six wave-speed arrays and the list of cells left
+// vp: 7N + 16 doubles, the six wave-speed arrays and the lists of cells left
 // to the later parts of the eigenvalue stages.  ev (optional): five events
 // recorded after A1, A2, A3, A4 (each with its passes over listed cells) and
 // A5.  [c0, c1):

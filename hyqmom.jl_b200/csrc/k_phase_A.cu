@@ -42,11 +42,13 @@ __device__ __noinline__ void cell_phase_A(const double* m, int flag2D, double Ma
 // kernel itself solves pattern-1 Jacobians on its 64-register path and lists
 // every other cell; k_A_fix runs the general eigen-solve on the listed cells
 // (packed densely into warps) and marks those that need the correction of
-// complex eigenvalues; k_A_corr finishes the marked cells (rare) from the
-// planes to correct.  The list lives in vp[6N..7N) (entries (cell << 3) |
-// code, code 0 = to solve, 1-3 = the planes to correct, 4 = the complete
-// function; three counters after the first N entries), one list per stage in
-// turn.
+// complex eigenvalues; k_A_corr finishes those cells (rare) from the planes
+// to correct.  Two lists live in the seventh plane of vp (from vp + 6N, as
+// 32-bit words, one pair per stage in turn): the cells to solve (entries
+// cell << 3, N of them, then the three counters at N + axis - 1) and, from
+// word N + 16, the cells to correct (entries (cell << 3) | code, code 1-3 =
+// the planes to correct, 4 = the complete function; counters at
+// N + 4 + axis - 1), so that the correction pass only reads its own cells.
 // Late in a developed flow nearly every cell is listed; a stage then runs
 // dense for a while (DevClock::dense): k_A_eig returns at once and k_A_fix
 // takes every cell of the range, listing only those to correct.
@@ -54,14 +56,23 @@ __device__ __forceinline__ bool phase_A_active(const StepConst& sc, const DevClo
   return (clk->t < sc.tmax) && (clk->nn < sc.nnmax);
 }
 __device__ __forceinline__ unsigned int* defer_list(double* vp, long long N) { return reinterpret_cast<unsigned int*>(vp + 6 * N); }
+__device__ __forceinline__ unsigned int* corr_list(double* vp, long long N) { return defer_list(vp, N) + N + 16; }
+__device__ __forceinline__ unsigned int* corr_count(double* vp, long long N, int axis) { return defer_list(vp, N) + N + 4 + (axis - 1); }
+// Append a cell to the correction list of its stage.
+__device__ __forceinline__ void list_corr(double* vp, long long N, int axis, long long c, unsigned int code) {
+  corr_list(vp, N)[atomicAdd(corr_count(vp, N, axis), 1u)] = ((unsigned int)c << 3) | code;
+}
 
 // A1: Flux_closure35_and_realizable_3D (realized moments only); also resets
-// the three list counters
+// the list counters
 __device__ __forceinline__ void A1_body(const double* __restrict__ M, double* __restrict__ out, double* vp, const StepConst& sc,
                                         const DevClock* clk, long long c0, long long c1, int bid) {
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N, c = c0 + (long long)bid * BS_A + threadIdx.x;
-  if (c == c0) { unsigned int* cnt = defer_list(vp, N) + N; cnt[0] = 0; cnt[1] = 0; cnt[2] = 0; }
+  if (c == c0) {
+    unsigned int* cnt = defer_list(vp, N) + N;
+    for (int q = 0; q < 8; ++q) cnt[q] = 0;
+  }
   if (c >= c1) return;
   flux_closure35(M + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
 }
@@ -128,9 +139,11 @@ __device__ __forceinline__ void A_eig_body(const double* in, double* out, double
   if (st == EIG_DONE) {
     double* v = vp + 2 * (axis - 1) * N;
     v[c] = lo; v[c + N] = hi;
+  } else if (code) {
+    list_corr(vp, N, axis, c, code);
   } else {
     unsigned int* list = defer_list(vp, N);
-    list[atomicAdd(list + N + (axis - 1), 1u)] = ((unsigned int)c << 3) | code;
+    list[atomicAdd(list + N + (axis - 1), 1u)] = (unsigned int)c << 3;
   }
 }
 template <int JM>
@@ -161,16 +174,14 @@ __device__ __forceinline__ void A_fix_body(const double* in, double* out, double
     const long long c = c0 + (long long)bid * BS_A + threadIdx.x;
     if (c >= c1) return;
     if (eig_stage<FIX_MODE, false>(in, out, vp, c, axis, sc, lo, hi, &code) == EIG_DONE) { v[c] = lo; v[c + N] = hi; }
-    else list[atomicAdd(list + N + (axis - 1), 1u)] = ((unsigned int)c << 3) | code;
+    else list_corr(vp, N, axis, c, code);
     return;
   }
   const unsigned int count = list[N + (axis - 1)];
   for (unsigned int e = bid * BS_A + threadIdx.x; e < count; e += nblk * BS_A) {
-    const unsigned int entry = list[e];
-    if (entry & 7u) continue;
-    const long long c = entry >> 3;
+    const long long c = list[e] >> 3;
     if (eig_stage<FIX_MODE, false>(in, out, vp, c, axis, sc, lo, hi, &code) == EIG_DONE) { v[c] = lo; v[c + N] = hi; }
-    else list[e] = entry | code;
+    else list_corr(vp, N, axis, c, code);
   }
 }
 __global__ void __launch_bounds__(BS_A, MINB_FIX) k_A_fix(const double* in, double* out, double* vp, int axis,
@@ -192,18 +203,25 @@ __device__ __forceinline__ void A_corr_body(const double* in, double* out, doubl
                                             long long c0, long long c1, int bid, int nblk) {
   if (!phase_A_active(sc, clk)) return;
   const long long N = sc.N;
-  const unsigned int* list = defer_list(vp, N);
-  const unsigned int count = list[N + (axis - 1)];
+  const unsigned int* list = corr_list(vp, N);
+  const unsigned int count = *corr_count(vp, N, axis);
   double* v = vp + 2 * (axis - 1) * N;
   if (bid == 0 && threadIdx.x == 0) {
     int& d = clk->dense[axis - 1];
+    const long long listed = (long long)defer_list(vp, N)[N + (axis - 1)] + count;
     if (d > 0) d = d - 1;
-    else if ((long long)count * 4 > (c1 - c0) * 3) d = DENSE_RUNS;
+    else if (listed * 4 > (c1 - c0) * 3) d = DENSE_RUNS;
   }
-  for (unsigned int e = bid * BS_A + threadIdx.x; e < count; e += nblk * BS_A) {
+  // A short list (the usual case) gets one cell per warp: the correction's
+  // long serial chain then runs without the other lanes' divergent branches,
+  // spread over more SMs; a long one gets one cell per thread.
+  const bool sparse = (unsigned long long)count * 32ull <= (unsigned long long)nblk * BS_A;
+  if (sparse && (threadIdx.x & 31)) return;
+  const unsigned int e0 = sparse ? (bid * BS_A + threadIdx.x) >> 5 : bid * BS_A + threadIdx.x;
+  const unsigned int es = sparse ? (unsigned int)(nblk * BS_A) >> 5 : (unsigned int)(nblk * BS_A);
+  for (unsigned int e = e0; e < count; e += es) {
     const unsigned int entry = list[e];
     const int code = int(entry & 7u);
-    if (!code) continue;
     const long long c = entry >> 3;
     double lo, hi;
     if (code == 4) eig_stage<FIX_MODE, true>(in, out, vp, c, axis, sc, lo, hi);

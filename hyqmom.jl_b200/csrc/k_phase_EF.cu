@@ -13,25 +13,32 @@ namespace {
 // Phases [E]+[F] run as per-function kernels (small code per kernel);
 // intermediate states go through a flux buffer, dead after the HLL sweep:
 //   Mtmp -E1-> Fx -E2, E3 (in place: only corrected moments are written)-> Fx -E4-> M.
-// E2/E3 copy the moments and list the cells whose Jacobians have complex
-// eigenvalues and the cells with a Jacobian outside the usual permutation
-// (pattern 1, the only one their 64-register code solves); k_E_fix decides
-// the latter with the general eigen-solve and k_E_corr corrects the cells
-// that need it, so that each kernel keeps small code and a few such cells no
-// longer hold every lane of their warps.  The lists live in the wave-speed
-// buffer vp, dead after the HLL sweep (vp[0..N): entries (cell << 2) |
-// planes, planes = 0 for a cell still to be decided; two counters after them).
+// E2/E3 copy the moments, list the cells whose Jacobians have complex
+// eigenvalues for the correction, and list the cells with a Jacobian outside
+// the usual permutation (pattern 1, the only one their 64-register code
+// solves) for k_E_fix, which decides them with the general eigen-solve and
+// lists those that need the correction; k_E_corr corrects the cells of its
+// list, so that each kernel keeps small code and a few such cells no longer
+// hold every lane of their warps.  The lists live in the wave-speed buffer
+// vp, dead after the HLL sweep: the cells to decide at vp[0..N) (64-bit
+// entries cell << 2), four 32-bit counters at vp + N (to decide: x, y; to
+// correct: x, y), the cells to correct from vp + N + 8 ((cell << 2) | planes).
 // A stage that listed most of its cells runs dense for a while
 // (DevClock::dense): k_E_eig only copies and k_E_fix decides every cell,
 // listing those to correct.
 __device__ __forceinline__ unsigned int* fix_counters(double* vp, long long N) { return reinterpret_cast<unsigned int*>(vp + N); }
+__device__ __forceinline__ unsigned long long* corr_list_ef(double* vp, long long N) { return reinterpret_cast<unsigned long long*>(vp + N + 8); }
+// Append a cell to the correction list of stage `which`.
+__device__ __forceinline__ void list_corr_ef(double* vp, long long N, int which, long long c, int planes) {
+  corr_list_ef(vp, N)[atomicAdd(fix_counters(vp, N) + 2 + which, 1u)] = ((unsigned long long)c << 2) | (unsigned long long)planes;
+}
 
-// E1: Flux_closure35_and_realizable_3D; also resets the two fix counters
+// E1: Flux_closure35_and_realizable_3D; also resets the list counters
 __device__ __forceinline__ void E1_body(const double* __restrict__ in, double* __restrict__ out, double* vp, const StepConst& sc,
                                         const DevClock* clk, long long c0, long long c1, int bid) {
   if (!clk->active) return;
   const long long N = sc.N, c = c0 + (long long)bid * BS_EF + threadIdx.x;
-  if (c == c0) { unsigned int* cnt = fix_counters(vp, N); cnt[0] = 0; cnt[1] = 0; }
+  if (c == c0) { unsigned int* cnt = fix_counters(vp, N); cnt[0] = 0; cnt[1] = 0; cnt[2] = 0; cnt[3] = 0; }
   if (c >= c1) return;
   flux_closure35(in + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
 }
@@ -79,9 +86,11 @@ __device__ __forceinline__ void E_eig_body(const double* in, double* out, double
 #pragma unroll
     for (int n = 0; n < 35; ++n) out[c + N * n] = in[c + N * n];
   }
-  if (planes) {
+  if (planes > 0) {
+    list_corr_ef(vp, N, which, c, planes);
+  } else if (planes < 0) {
     const unsigned int slot = atomicAdd(fix_counters(vp, N) + which, 1u);
-    reinterpret_cast<unsigned long long*>(vp)[slot] = ((unsigned long long)c << 2) | (unsigned long long)(planes < 0 ? 0 : planes);
+    reinterpret_cast<unsigned long long*>(vp)[slot] = (unsigned long long)c << 2;
   }
 }
 template <int JM>
@@ -109,16 +118,14 @@ __device__ __forceinline__ void E_fix_body(const double* __restrict__ in, double
     const long long c = c0 + (long long)bid * BS_EF + threadIdx.x;
     if (c >= c1) return;
     const int planes = eigenvalues6_flags_t<FIX_MODE>(in + c, axis, N);
-    if (planes) list[atomicAdd(fix_counters(vp, N) + which, 1u)] = ((unsigned long long)c << 2) | (unsigned long long)planes;
+    if (planes) list_corr_ef(vp, N, which, c, planes);
     return;
   }
   const unsigned int count = reinterpret_cast<const unsigned int*>(vp + N)[which];
   for (unsigned int e = bid * BS_EF + threadIdx.x; e < count; e += nblk * BS_EF) {
-    const unsigned long long v = list[e];
-    if (v & 3ull) continue;
-    const long long c = (long long)(v >> 2);
+    const long long c = (long long)(list[e] >> 2);
     const int planes = eigenvalues6_flags_t<FIX_MODE>(in + c, axis, N);
-    if (planes) list[e] = v | (unsigned long long)planes;
+    if (planes) list_corr_ef(vp, N, which, c, planes);
   }
 }
 __global__ void __launch_bounds__(BS_EF, MINB_FIX) k_E_fix(const double* __restrict__ in, double* vp, int axis, int which,
@@ -140,17 +147,23 @@ __device__ __forceinline__ void E_corr_body(const double* in, double* out, const
                                             DevClock* clk, long long c0, long long c1, int bid, int nblk) {
   if (!clk->active) return;
   const long long N = sc.N;
-  const unsigned int count = reinterpret_cast<const unsigned int*>(vp + N)[which];
-  const unsigned long long* list = reinterpret_cast<const unsigned long long*>(vp);
+  const unsigned int count = reinterpret_cast<const unsigned int*>(vp + N)[2 + which];
+  const unsigned long long* list = reinterpret_cast<const unsigned long long*>(vp + N + 8);
   if (bid == 0 && threadIdx.x == 0) {
     int& d = clk->dense[3 + which];
+    const long long listed = (long long)reinterpret_cast<const unsigned int*>(vp + N)[which] + count;
     if (d > 0) d = d - 1;
-    else if ((long long)count * 4 > (c1 - c0) * 3) d = DENSE_RUNS;
+    else if (listed * 4 > (c1 - c0) * 3) d = DENSE_RUNS;
   }
-  for (unsigned int e = bid * BS_EF + threadIdx.x; e < count; e += nblk * BS_EF) {
+  // one cell per warp for a short list, one per thread for a long one (as
+  // the phase-A correction passes)
+  const bool sparse = (unsigned long long)count * 32ull <= (unsigned long long)nblk * BS_EF;
+  if (sparse && (threadIdx.x & 31)) return;
+  const unsigned int e0 = sparse ? (bid * BS_EF + threadIdx.x) >> 5 : bid * BS_EF + threadIdx.x;
+  const unsigned int es = sparse ? (unsigned int)(nblk * BS_EF) >> 5 : (unsigned int)(nblk * BS_EF);
+  for (unsigned int e = e0; e < count; e += es) {
     const unsigned long long v = list[e];
     const int planes = int(v & 3ull);
-    if (!planes) continue;
     const long long c = (long long)(v >> 2);
     double Ml[35], Mc[35];
     for (int n = 0; n < 35; ++n) Ml[n] = in[c + N * n];

@@ -354,7 +354,7 @@ def crossing_run_states(Ma, Kn, grid=(48, 48, 24), steps=120, every=8, device=0)
     return np.concatenate(out, axis=1) if out else np.zeros((35, 0))
 
 
-def build_dataset(seed=0, grid=(40, 40, 20), steps=120, every=8, n_mix=2_000_000, Mas=(0.0, 0.5, 1.0, 2.0),
+def build_dataset(seed=0, grid=(48, 48, 24), steps=120, every=6, n_mix=2_400_000, Mas=(0.0, 0.5, 1.0, 2.0),
                   Kns=(1e-3, 1e-2, 1e-1, 1.0), device=0, log=print):
     """Training set on the device: (X tiles, T [n, 8], n).  Rows whose target
     is not finite are dropped; rows are shuffled (seeded)."""
@@ -447,9 +447,9 @@ if __name__ == "__main__":
     import json
     ap = argparse.ArgumentParser(description="train the wave-speed network on the GPU")
     ap.add_argument("--out", default=WEIGHTS_PATH)
-    ap.add_argument("--epochs", type=int, default=6)
+    ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--n-mix", type=int, default=2_000_000)
+    ap.add_argument("--n-mix", type=int, default=2_400_000)
     args = ap.parse_args()
     net, rep = train(out=args.out, epochs=args.epochs, seed=args.seed, n_mix=args.n_mix)
     print(json.dumps({"report": rep, "margin": net.margin, "meta": net.meta}))

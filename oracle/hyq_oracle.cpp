@@ -349,6 +349,23 @@ double hyqo_step_end_hll(void* work, double* M, double vmax, double* t) {
   return hyqo_step_end(work, M, vmax, t);
 }
 
+// Phases [E]+[F] alone (src/simulation_runner.jl:526-557) on a state M that
+// the HLL combination produced, with the step's dt: the part of the step
+// after the wave speeds, for measuring how the reference's step responds to
+// round-off in its intermediate state.
+void hyqo_phase_EF(int Nx, int Ny, int Nz, double* M, double Kn, double Ma, int flag2D, int positivity, double dt) {
+  Params P{Nx, Ny, Nz, flag2D, positivity, Kn, Ma, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  const size_t N = (size_t)Nx * Ny * Nz;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (long long c = 0; c < (long long)N; ++c) {
+    double m[35], r[35], o[35];
+    for (int n = 0; n < 35; ++n) m[n] = M[c + N * n];
+    phase_E<double>(m, P, r);
+    collision35<double>(r, dt, P.Kn, P.positivity != 0, o);
+    for (int n = 0; n < 35; ++n) M[c + N * n] = o[n];
+  }
+}
+
 double hyqo_step(int Nx, int Ny, int Nz, double* M, double Kn, double Ma, int flag2D, double CFL, double dtmax, double tmax,
                  double dx, double dy, double dz, int positivity, double* t, double* vmax_out) {
   double vmax = 0.0;

@@ -234,3 +234,43 @@ def one_ulp_spread(M, pp, t, trials=3, seed=0):
         worst = max(worst, _field_rel(B, A))
     return worst
 
+
+
+def step_end_hll(work, M, vmax, t):
+    """The rest of the step stopped after the HLL combination: M becomes the
+    state phases [E]+[F] start from; returns (dt, t_new)."""
+    lib = load()
+    lib.hyqo_step_end_hll.restype = ctypes.c_double
+    tt = np.array([t], dtype=np.float64)
+    dt = lib.hyqo_step_end_hll(ctypes.c_void_p(work), M.ctypes.data_as(_dp), ctypes.c_double(vmax), _p(tt))
+    return dt, float(tt[0])
+
+
+def phase_EF(M, params, dt):
+    """Phases [E]+[F] in place on a post-HLL state M with the step's dt."""
+    assert M.flags["F_CONTIGUOUS"] and M.dtype == np.float64
+    Nx, Ny, Nz, _ = M.shape
+    p = params
+    load().hyqo_phase_EF(Nx, Ny, Nz, M.ctypes.data_as(_dp), ctypes.c_double(p["Kn"]), ctypes.c_double(p["Ma"]), int(p["flag2D"]),
+                         int(p.get("positivity", True)), ctypes.c_double(dt))
+
+
+def post_hll_spread(M, pp, t, trials=6, seed=0):
+    """The oracle's own spread in the part of its step after the wave speeds:
+    the largest field-relative difference between phases [E]+[F] on its HLL
+    output from M and on that output with every entry moved by one ulp
+    (random direction), over `trials` perturbations."""
+    A = np.asfortranarray(M.copy())
+    w, vm = step_begin(A, pp)
+    dt, _ = step_end_hll(w, A, vm, t)
+    base = A.copy(order="F")
+    phase_EF(base, pp, dt)
+    rng = np.random.default_rng(seed)
+    worst = 0.0
+    for _ in range(trials):
+        flat = A.reshape(-1, order="F")
+        up = rng.random(flat.size) < 0.5
+        B = np.asfortranarray(np.where(up, np.nextafter(flat, np.inf), np.nextafter(flat, -np.inf)).reshape(A.shape, order="F"))
+        phase_EF(B, pp, dt)
+        worst = max(worst, _field_rel(B, base))
+    return worst
