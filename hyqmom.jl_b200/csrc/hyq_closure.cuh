@@ -413,8 +413,13 @@ HQD int f5_of(int i, int j, int k) { return T_F5[i * 36 + j * 6 + k]; }
 // is read from M4[n * ist] and written to Mr[n * mst], Fx[n * fst], ...: the
 // step kernels pass the cell's entry of the moment-major fields (stride N)
 // so that nothing is staged through per-thread arrays.
-HQN void flux_closure35(const double* M4, int flag2D, double Ma, double* Fx, double* Fy, double* Fz, double* Mr, long long ist = 1,
-                        long long mst = 1, long long fst = 1) {
+// FLUX = false (no flux wanted): the fifth-order closure and the raw
+// fifth-order moments are skipped; the order <= 4 entries of the raw-moment
+// transform only read order <= 4 entries, in the same order, so Mr has the
+// same bits either way.
+template <bool FLUX>
+HQN void flux_closure35_t(const double* M4, int flag2D, double Ma, double* Fx, double* Fy, double* Fz, double* Mr, long long ist,
+                          long long mst, long long fst) {
   const double s3max = 4.0 + fabs(Ma) / 2.0;
   const double h2min = 1e-8;
   const double M000 = M4[0];
@@ -456,8 +461,8 @@ HQN void flux_closure35(const double* M4, int flag2D, double Ma, double* Fx, dou
     s[s202] = 1.0; s[s022] = 1.0; s[s112] = s[s110]; s[s121] = 0.0; s[s211] = 0.0; s[s103] = 0.0; s[s013] = 0.0;
     s[s301] = 0.0; s[s031] = 0.0;
   }
-  double f[21];
-  hyqmom_3D(s, f);
+  double f[FLUX ? 21 : 1];
+  if constexpr (FLUX) hyqmom_3D(s, f);
   // S -> C (S_to_C_batch) on the 56-entry store, then C -> raw (C5toM5_3D)
   const double sx = sqrt(jmax(EPS, C200)), sy = sqrt(jmax(EPS, C020)), sz = sqrt(jmax(EPS, C002));
   double px[6], py[6], pz[6];
@@ -467,9 +472,10 @@ HQN void flux_closure35(const double* M4, int flag2D, double Ma, double* Fx, dou
   px[3] = sx * sx * sx; py[3] = sy * sy * sy; pz[3] = sz * sz * sz;
   px[4] = pow4(sx); py[4] = pow4(sy); pz[4] = pow4(sz);
   px[5] = pow5(sx); py[5] = pow5(sy); pz[5] = pow5(sz);
-  double A[56];
+  constexpr int NA = FLUX ? 56 : 35;
+  double A[NA];
 #pragma unroll
-  for (int q = 0; q < 56; ++q) {
+  for (int q = 0; q < NA; ++q) {
     const int i = T_EX56I[q], j = T_EX56J[q], k = T_EX56K[q];
     const int o = i + j + k;
     double val;
@@ -479,7 +485,7 @@ HQN void flux_closure35(const double* M4, int flag2D, double Ma, double* Fx, dou
     else if (o == 2 && j == 2) val = C020;
     else if (o == 2 && k == 2) val = C002;
     else {
-      double d = (q >= 35) ? f[q - 35] : s[T_S28OF56[q]];
+      double d = (q >= 35) ? f[FLUX ? q - 35 : 0] : s[T_S28OF56[q]];
       if (i) d = d * px[i];
       if (j) d = d * py[j];
       if (k) d = d * pz[k];
@@ -487,14 +493,23 @@ HQN void flux_closure35(const double* M4, int flag2D, double Ma, double* Fx, dou
     }
     A[q] = val;
   }
-  central_to_raw_r<56>(M000, u, v, w, A);
+  central_to_raw_r<NA>(M000, u, v, w, A);
 #pragma unroll
   for (int n = 0; n < 35; ++n) {
     Mr[n * mst] = A[n];
-    if (Fx) Fx[n * fst] = A[T_FX[n]];
-    if (Fy) Fy[n * fst] = A[T_FY[n]];
-    if (Fz) Fz[n * fst] = A[T_FZ[n]];
+    if constexpr (FLUX) {
+      if (Fx) Fx[n * fst] = A[T_FX[n]];
+      if (Fy) Fy[n * fst] = A[T_FY[n]];
+      if (Fz) Fz[n * fst] = A[T_FZ[n]];
+    }
   }
+}
+// Flux_closure35_and_realizable_3D; null Fx, Fy and Fz (the realized moments
+// only) select the variant without the fifth-order work.
+HQD void flux_closure35(const double* M4, int flag2D, double Ma, double* Fx, double* Fy, double* Fz, double* Mr, long long ist = 1,
+                        long long mst = 1, long long fst = 1) {
+  if (Fx || Fy || Fz) flux_closure35_t<true>(M4, flag2D, Ma, Fx, Fy, Fz, Mr, ist, mst, fst);
+  else flux_closure35_t<false>(M4, flag2D, Ma, nullptr, nullptr, nullptr, Mr, ist, mst, fst);
 }
 
 }  // namespace hyq

@@ -89,8 +89,13 @@ constexpr int EIG_MODE = HQ_EIG_MODE;
 // DENSE_RUNS runs, then tries the pattern-1 kernel again.
 constexpr int DENSE_RUNS = 16;
 // The correction passes (few cells, or none) stride over their list with at
-// most one wave of blocks.
+// most one wave of blocks of CORR_BS threads: one warp per block, so that a
+// short list spreads one cell per SM-resident warp and each lone lane's work
+// arrays stay in L1 (a lone lane touches a separate cache line per word of
+// its local memory).
 constexpr int CORR_BLOCKS = 148 * 4;
+constexpr int CORR_BS = 32;
+constexpr int CORR_SPLIT = 128 / CORR_BS;  // blocks per 128-cell block of the grid
 
 constexpr int BS_A = 128;
 constexpr int BS_EF = 128;
@@ -116,7 +121,7 @@ constexpr int DK_MAX_MEMBERS = 4096;
 inline void dom_blocks(long long N, int hll_bs, int hll_g, int corr_cap, int* nb) {
   const int g = grid_of(N, BS_A);
   nb[DK_CELLS] = g;
-  nb[DK_CORR] = g < corr_cap ? g : corr_cap;
+  nb[DK_CORR] = (g < corr_cap ? g : corr_cap) * CORR_SPLIT;
   nb[DK_HLL] = grid_of(N, hll_bs) * hll_g;
   nb[DK_ONE] = 1;
   const int gd = grid_of(N, 256);

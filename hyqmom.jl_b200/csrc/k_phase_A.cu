@@ -215,10 +215,10 @@ __device__ __forceinline__ void A_corr_body(const double* in, double* out, doubl
   // A short list (the usual case) gets one cell per warp: the correction's
   // long serial chain then runs without the other lanes' divergent branches,
   // spread over more SMs; a long one gets one cell per thread.
-  const bool sparse = (unsigned long long)count * 32ull <= (unsigned long long)nblk * BS_A;
+  const bool sparse = (unsigned long long)count * 32ull <= (unsigned long long)nblk * CORR_BS;
   if (sparse && (threadIdx.x & 31)) return;
-  const unsigned int e0 = sparse ? (bid * BS_A + threadIdx.x) >> 5 : bid * BS_A + threadIdx.x;
-  const unsigned int es = sparse ? (unsigned int)(nblk * BS_A) >> 5 : (unsigned int)(nblk * BS_A);
+  const unsigned int e0 = sparse ? (bid * CORR_BS + threadIdx.x) >> 5 : bid * CORR_BS + threadIdx.x;
+  const unsigned int es = sparse ? (unsigned int)(nblk * CORR_BS) >> 5 : (unsigned int)(nblk * CORR_BS);
   for (unsigned int e = e0; e < count; e += es) {
     const unsigned int entry = list[e];
     const int code = int(entry & 7u);
@@ -231,11 +231,11 @@ __device__ __forceinline__ void A_corr_body(const double* in, double* out, doubl
     v[c] = lo; v[c + N] = hi;
   }
 }
-__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A_corr(const double* in, double* out, double* vp,
+__global__ void __launch_bounds__(CORR_BS, MINB_CLOSURE * CORR_SPLIT) k_A_corr(const double* in, double* out, double* vp,
                                                               int axis, const StepConst sc, DevClock* clk, long long c0, long long c1) {
   A_corr_body(in, out, vp, axis, sc, clk, c0, c1, blockIdx.x, gridDim.x);
 }
-__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A_corr_b(const Batch bt, int r_in, int r_out, int axis) {
+__global__ void __launch_bounds__(CORR_BS, MINB_CLOSURE * CORR_SPLIT) k_A_corr_b(const Batch bt, int r_in, int r_out, int axis) {
   const int m = member_of(bt, blockIdx.x);
   const Dom& d = bt.dom[m];
   const StepConst sc = d.sc;
@@ -303,7 +303,7 @@ void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, do
   if (c1 < 0) c1 = N;
   const int g = grid_of(c1 - c0, BS_A);
   const int gfix = g;  // one thread per possible list entry: blocks past the count exit at once
-  const int gcorr = g < CORR_BLOCKS ? g : CORR_BLOCKS;
+  const int gcorr = (g < CORR_BLOCKS ? g : CORR_BLOCKS) * CORR_SPLIT;
   k_A1_closure<<<g, BS_A, 0, s>>>(M, Fx, vp, sc, clk, c0, c1);
   if (sc.mode == MODE_LEARNED) launch_wavespeed_seeds(sc, Fx, net, sc.seeds, clk, s, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
@@ -313,7 +313,7 @@ void launch_phase_A(const StepConst& sc, double* M, double* Mtmp, double* Fx, do
     if (sc.mode == MODE_PLAIN) k_A_eig<EIG_MODE><<<g, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
     else k_A_eig<JAC_CP><<<g, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
     k_A_fix<<<gfix, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
-    k_A_corr<<<gcorr, BS_A, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
+    k_A_corr<<<gcorr, CORR_BS, 0, s>>>(ins[axis - 1], outs[axis - 1], vp, axis, sc, clk, c0, c1);
     if (ev) cudaEventRecord(ev[axis], s);
   }
   k_A5_flux<<<g, BS_A, 0, s>>>(Mtmp, M, Fx, Fy, Fz, vp, blockmax, sc, clk, c0, c1);
@@ -330,7 +330,7 @@ void launch_phase_A_batch(const BatchPlan& bp, int mode, cudaStream_t s, void (*
     if (mode == MODE_PLAIN) k_A_eig_b<EIG_MODE><<<g, BS_A, 0, s>>>(cells, ins[axis - 1], outs[axis - 1], axis);
     else k_A_eig_b<JAC_CP><<<g, BS_A, 0, s>>>(cells, ins[axis - 1], outs[axis - 1], axis);
     k_A_fix_b<<<g, BS_A, 0, s>>>(cells, ins[axis - 1], outs[axis - 1], axis);
-    k_A_corr_b<<<gc, BS_A, 0, s>>>(corr, ins[axis - 1], outs[axis - 1], axis);
+    k_A_corr_b<<<gc, CORR_BS, 0, s>>>(corr, ins[axis - 1], outs[axis - 1], axis);
   }
   k_A5_flux_b<<<g, BS_A, 0, s>>>(cells);
 }

@@ -157,10 +157,10 @@ __device__ __forceinline__ void E_corr_body(const double* in, double* out, const
   }
   // one cell per warp for a short list, one per thread for a long one (as
   // the phase-A correction passes)
-  const bool sparse = (unsigned long long)count * 32ull <= (unsigned long long)nblk * BS_EF;
+  const bool sparse = (unsigned long long)count * 32ull <= (unsigned long long)nblk * CORR_BS;
   if (sparse && (threadIdx.x & 31)) return;
-  const unsigned int e0 = sparse ? (bid * BS_EF + threadIdx.x) >> 5 : bid * BS_EF + threadIdx.x;
-  const unsigned int es = sparse ? (unsigned int)(nblk * BS_EF) >> 5 : (unsigned int)(nblk * BS_EF);
+  const unsigned int e0 = sparse ? (bid * CORR_BS + threadIdx.x) >> 5 : bid * CORR_BS + threadIdx.x;
+  const unsigned int es = sparse ? (unsigned int)(nblk * CORR_BS) >> 5 : (unsigned int)(nblk * CORR_BS);
   for (unsigned int e = e0; e < count; e += es) {
     const unsigned long long v = list[e];
     const int planes = int(v & 3ull);
@@ -171,12 +171,12 @@ __device__ __forceinline__ void E_corr_body(const double* in, double* out, const
     for (int n = 0; n < 35; ++n) out[c + N * n] = Mc[n];
   }
 }
-__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E_corr(const double* in, double* out, const double* vp,
+__global__ void __launch_bounds__(CORR_BS, MINB_CLOSURE * CORR_SPLIT) k_E_corr(const double* in, double* out, const double* vp,
                                                                 int axis, int which, const StepConst sc, DevClock* clk, long long c0,
                                                                 long long c1) {
   E_corr_body(in, out, vp, axis, which, sc, clk, c0, c1, blockIdx.x, gridDim.x);
 }
-__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E_corr_b(const Batch bt, int axis, int which) {
+__global__ void __launch_bounds__(CORR_BS, MINB_CLOSURE * CORR_SPLIT) k_E_corr_b(const Batch bt, int axis, int which) {
   const int m = member_of(bt, blockIdx.x);
   const Dom& d = bt.dom[m];
   const StepConst sc = d.sc;
@@ -214,18 +214,18 @@ void launch_phase_EF(const StepConst& sc, const double* Min, double* Mout, doubl
   if (c1 < 0) c1 = sc.N;
   const int g = grid_of(c1 - c0, BS_EF);
   const int gfix = g;  // one thread per possible list entry: blocks past the count exit at once
-  const int gcorr = g < CORR_BLOCKS ? g : CORR_BLOCKS;
+  const int gcorr = (g < CORR_BLOCKS ? g : CORR_BLOCKS) * CORR_SPLIT;
   k_E1_closure<<<g, BS_EF, 0, s>>>(Min, Fx, vp, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[0], s);
   if (sc.mode == MODE_PLAIN) k_E_eig<EIG_MODE><<<g, BS_EF, 0, s>>>(Fx, Fx, vp, 1, 0, sc, clk, c0, c1);
   else k_E_eig<JAC_CP><<<g, BS_EF, 0, s>>>(Fx, Fx, vp, 1, 0, sc, clk, c0, c1);
   k_E_fix<<<gfix, BS_EF, 0, s>>>(Fx, vp, 1, 0, sc, clk, c0, c1);
-  k_E_corr<<<gcorr, BS_EF, 0, s>>>(Fx, Fx, vp, 1, 0, sc, clk, c0, c1);
+  k_E_corr<<<gcorr, CORR_BS, 0, s>>>(Fx, Fx, vp, 1, 0, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[1], s);
   if (sc.mode == MODE_PLAIN) k_E_eig<EIG_MODE><<<g, BS_EF, 0, s>>>(Fx, Fx, vp, 2, 1, sc, clk, c0, c1);
   else k_E_eig<JAC_CP><<<g, BS_EF, 0, s>>>(Fx, Fx, vp, 2, 1, sc, clk, c0, c1);
   k_E_fix<<<gfix, BS_EF, 0, s>>>(Fx, vp, 2, 1, sc, clk, c0, c1);
-  k_E_corr<<<gcorr, BS_EF, 0, s>>>(Fx, Fx, vp, 2, 1, sc, clk, c0, c1);
+  k_E_corr<<<gcorr, CORR_BS, 0, s>>>(Fx, Fx, vp, 2, 1, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[2], s);
   k_E4_closure_bgk<<<g, BS_EF, 0, s>>>(Fx, Mout, sc, clk, c0, c1);
   if (ev) cudaEventRecord(ev[3], s);
@@ -240,7 +240,7 @@ void launch_phase_EF_batch(const BatchPlan& bp, int mode, cudaStream_t s) {
     if (mode == MODE_PLAIN) k_E_eig_b<EIG_MODE><<<g, BS_EF, 0, s>>>(cells, axis, which);
     else k_E_eig_b<JAC_CP><<<g, BS_EF, 0, s>>>(cells, axis, which);
     k_E_fix_b<<<g, BS_EF, 0, s>>>(cells, axis, which);
-    k_E_corr_b<<<gc, BS_EF, 0, s>>>(corr, axis, which);
+    k_E_corr_b<<<gc, CORR_BS, 0, s>>>(corr, axis, which);
   }
   k_E4_closure_bgk_b<<<g, BS_EF, 0, s>>>(cells);
 }

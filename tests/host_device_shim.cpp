@@ -14,6 +14,9 @@ static inline double __longlong_as_double(long long x) { double d; std::memcpy(&
 using namespace hyq;
 extern "C" {
 void sh_flux(const double* m, int flag2D, double Ma, double* Fx, double* Fy, double* Fz, double* Mr) { flux_closure35(m, flag2D, Ma, Fx, Fy, Fz, Mr); }
+// the realized moments alone (no flux wanted: the variant without the
+// fifth-order work)
+void sh_realized(const double* m, int flag2D, double Ma, double* Mr) { flux_closure35(m, flag2D, Ma, nullptr, nullptr, nullptr, Mr); }
 void sh_eig(const double* m, int axis, int flag2D, double Ma, int pos, double* v, double* Mr) {
   if (axis == 3) eigenvalues6z(m, flag2D, Ma, pos, v[0], v[1], Mr); else eigenvalues6(m, axis, flag2D, Ma, v[0], v[1], Mr);
 }

@@ -50,6 +50,9 @@ def test_per_cell_functions_bitwise(shim, states):
         shim.sh_flux(P(m), 0, ctypes.c_double(0.0), *[P(x) for x in o])
         for a, b in zip(o, ol.flux_closure35(m, 0, 0.0)):
             assert np.array_equal(a, b, equal_nan=True), c
+        r = np.zeros(35)
+        shim.sh_realized(P(m), 0, ctypes.c_double(0.0), P(r))  # the closure without the flux work
+        assert np.array_equal(r, o[3], equal_nan=True), c
         for ax in (1, 2, 3):
             v, Mr = np.zeros(2), np.zeros(35)
             shim.sh_eig(P(m), ax, 0, ctypes.c_double(0.0), 1, P(v), P(Mr))
