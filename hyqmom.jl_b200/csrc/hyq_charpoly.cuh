@@ -364,42 +364,6 @@ HQD bool interior_certify(const double (&b)[7], const double (&eb)[7], double x1
   return ok;
 }
 
-HQD CpOut solve(const double (&b)[7], const double (&eb)[7], double xhi, double xlo) {
-  CpOut o;
-  o.ok = false;
-  o.its = 0;
-  o.xmin = o.xmax = 0.0;
-  double x1 = xhi, x6 = xlo;
-  if (!newton<6>(b, x1, NEWTON_TOL, o.its)) return o;
-  if (!newton<6>(b, x6, NEWTON_TOL, o.its)) return o;
-  if (!(x6 < x1)) return o;
-  // interior roots placed loosely first; a cluster (a near-double interior
-  // pair, common in nearly Gaussian cells) needs them converged
-  if (!interior_certify(b, eb, x1, x6, false, o.its) && !interior_certify(b, eb, x1, x6, true, o.its)) return o;
-  // conditioning of the two extremes
-  bool ok = true;
-#pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    const double x = q ? x1 : x6;
-    double p = b[6], dp = 0.0, bound = 1.0, ce = eb[6];
-    const double ax = fabs(x);
-#pragma unroll
-    for (int k = 5; k >= 0; --k) {
-      dp = fma(dp, x, p);
-      p = fma(p, x, b[k]);
-      bound = bound * ax + fabs(b[k]);
-      ce = ce * ax + eb[k];
-    }
-    ok = ok && (CERT_ERR * bound + ce <= EXT_ERR * fabs(dp));
-  }
-  o.its += 2;
-  if (!ok) return o;
-  o.xmin = x6;
-  o.xmax = x1;
-  o.ok = true;
-  return o;
-}
-
 // How far the plane's moments are from a Gaussian's: the largest deviation
 // of the standardized moments of orders 3 and 4 from their Gaussian values
 // (0; 3, 3 rho, 1 + 2 rho^2 with rho the correlation).  s: the 15 plane
@@ -407,9 +371,10 @@ HQD CpOut solve(const double (&b)[7], const double (&eb)[7], double xhi, double 
 // m20 m21 m22 m30 m31 m40, first index along the flux).  For a Gaussian the
 // 2-D closure's Jacobian has a double eigenvalue at the mean velocity
 // (u +- sqrt(3) sigma, u +- sigma, u, u), so a plane this close to one has an
-// interior pair the certificate cannot separate; such Jacobians go straight
-// to the LAPACK path instead of failing the certificate after a full search
-// (a routing decision only: the LAPACK path decides them either way).
+// interior pair the certificate cannot separate: when the loose pass fails
+// on such a plane, the solve gives up instead of converging the pair in the
+// tight pass (a routing decision only: the LAPACK path decides the Jacobian
+// either way).
 // NaN when the moments cannot be standardized.
 constexpr double NEAR_GAUSS = 1e-7;
 HQD double gauss_defect(const double* s) {
@@ -462,6 +427,46 @@ HQD double gauss_defect(const double* s) {
   return (sx > 0.0 && sy > 0.0 && d == d) ? d : qnan();
 }
 
+HQD CpOut solve(const double (&b)[7], const double (&eb)[7], double xhi, double xlo, const double* plane = nullptr) {
+  CpOut o;
+  o.ok = false;
+  o.its = 0;
+  o.xmin = o.xmax = 0.0;
+  double x1 = xhi, x6 = xlo;
+  if (!newton<6>(b, x1, NEWTON_TOL, o.its)) return o;
+  if (!newton<6>(b, x6, NEWTON_TOL, o.its)) return o;
+  if (!(x6 < x1)) return o;
+  // interior roots placed loosely first; a cluster (a near-double interior
+  // pair, common in nearly Gaussian cells) needs them converged
+  if (!interior_certify(b, eb, x1, x6, false, o.its)) {
+    // a nearly Gaussian plane's close pair is beyond the tight pass
+    if (plane && !(gauss_defect(plane) >= NEAR_GAUSS)) return o;
+    if (!interior_certify(b, eb, x1, x6, true, o.its)) return o;
+  }
+  // conditioning of the two extremes
+  bool ok = true;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const double x = q ? x1 : x6;
+    double p = b[6], dp = 0.0, bound = 1.0, ce = eb[6];
+    const double ax = fabs(x);
+#pragma unroll
+    for (int k = 5; k >= 0; --k) {
+      dp = fma(dp, x, p);
+      p = fma(p, x, b[k]);
+      bound = bound * ax + fabs(b[k]);
+      ce = ce * ax + eb[k];
+    }
+    ok = ok && (CERT_ERR * bound + ce <= EXT_ERR * fabs(dp));
+  }
+  o.its += 2;
+  if (!ok) return o;
+  o.xmin = x6;
+  o.xmax = x1;
+  o.ok = true;
+  return o;
+}
+
 // A seed x (in the normalised variable) is used as the start of the search
 // for the largest root when b has no root at or above it: the coefficients of
 // b(x + y) as a polynomial in y (the Taylor coefficients b^(k)(x) / k!) are
@@ -494,7 +499,8 @@ struct Extremes {
   int its;
   bool ok;
 };
-HQD Extremes extremes(const double* r3, const double* r5, const double* r6, double lo_seed, double hi_seed, double margin) {
+HQD Extremes extremes(const double* r3, const double* r5, const double* r6, double lo_seed, double hi_seed, double margin,
+                      const double* plane = nullptr) {
   Extremes e;
   e.ok = false;
   e.its = 0;
@@ -505,7 +511,7 @@ HQD Extremes extremes(const double* r3, const double* r5, const double* r6, doub
   if (!normalize(c, cabs, s, sig, b, eb)) return e;
   const double xhi = start_above(b, (hi_seed - s) / sig + margin);
   const double xlo = start_below(b, (lo_seed - s) / sig - margin);
-  const CpOut o = solve(b, eb, xhi, xlo);
+  const CpOut o = solve(b, eb, xhi, xlo, plane);
   e.its = o.its + 2;
   if (!o.ok) return e;
   e.vmin = s + sig * o.xmin;
