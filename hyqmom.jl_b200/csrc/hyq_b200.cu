@@ -249,25 +249,25 @@ __device__ __forceinline__ void hll_body(const double* __restrict__ M, const dou
       Mout[c + mo] = acc[q] + mz - 2.0 * Mn[c];
     }
 }
-template <int BS, int GROUPS>
-__global__ void __launch_bounds__(BS, HQ_MINB_HLL * 256 / BS) k_hll(const double* __restrict__ M, const double* __restrict__ Fx,
+template <int BS, int GROUPS, int MINB = HQ_MINB_HLL * 256 / BS>
+__global__ void __launch_bounds__(BS, MINB) k_hll(const double* __restrict__ M, const double* __restrict__ Fx,
                                                                     const double* __restrict__ Fy, const double* __restrict__ Fz,
                                                                     const double* __restrict__ vp, double* __restrict__ Mout,
                                                                     const StepConst sc, const DevClock* clk) {
   hll_body<BS, GROUPS>(M, Fx, Fy, Fz, vp, Mout, sc, clk, blockIdx.x);
 }
-template <int BS, int GROUPS>
-__global__ void __launch_bounds__(BS, HQ_MINB_HLL * 256 / BS) k_hll_b(const Batch bt) {
+template <int BS, int GROUPS, int MINB = HQ_MINB_HLL * 256 / BS>
+__global__ void __launch_bounds__(BS, MINB) k_hll_b(const Batch bt) {
   const int m = member_of(bt, blockIdx.x);
   const Dom& d = bt.dom[m];
   const StepConst sc = d.sc;
   hll_body<BS, GROUPS>(d.buf[DB_M], d.buf[DB_FX], d.buf[DB_FY], d.buf[DB_FZ], d.buf[DB_VP], d.buf[DB_MTMP], sc, d.clk,
                        blockIdx.x - __ldg(bt.blk0 + m));
 }
-template <int BS, int GROUPS>
+template <int BS, int GROUPS, int MINB = HQ_MINB_HLL * 256 / BS>
 void hll_launch(const double* M, const double* Fx, const double* Fy, const double* Fz, const double* vp, double* Mout, const StepConst& sc,
                 const DevClock* clk, cudaStream_t s) {
-  k_hll<BS, GROUPS><<<grid_of(sc.N, BS) * GROUPS, BS, 0, s>>>(M, Fx, Fy, Fz, vp, Mout, sc, clk);
+  k_hll<BS, GROUPS, MINB><<<grid_of(sc.N, BS) * GROUPS, BS, 0, s>>>(M, Fx, Fy, Fz, vp, Mout, sc, clk);
 }
 void hll_variant(int variant, const double* M, const double* Fx, const double* Fy, const double* Fz, const double* vp, double* Mout,
                  const StepConst& sc, const DevClock* clk, cudaStream_t s) {
@@ -277,6 +277,8 @@ void hll_variant(int variant, const double* M, const double* Fx, const double* F
     case 3: hll_launch<128, 5>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
     case 4: hll_launch<128, 7>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
     case 5: hll_launch<128, 1>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
+    case 6: hll_launch<256, 7, 6>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
+    case 7: hll_launch<256, 5, 5>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
     default: hll_launch<256, 1>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
   }
 }
@@ -289,6 +291,8 @@ void hll_variant_b(int variant, const Batch& bt, int nblk, cudaStream_t s) {
     case 3: k_hll_b<128, 5><<<nblk, 128, 0, s>>>(bt); break;
     case 4: k_hll_b<128, 7><<<nblk, 128, 0, s>>>(bt); break;
     case 5: k_hll_b<128, 1><<<nblk, 128, 0, s>>>(bt); break;
+    case 6: k_hll_b<256, 7, 6><<<nblk, 256, 0, s>>>(bt); break;
+    case 7: k_hll_b<256, 5, 5><<<nblk, 256, 0, s>>>(bt); break;
     default: k_hll_b<256, 1><<<nblk, 256, 0, s>>>(bt); break;
   }
 }

@@ -45,13 +45,6 @@ namespace hyq {
 namespace cp {
 
 constexpr int ITMAX = 40;              // Newton iterations per root
-// Newton iterations per interior root in the tight pass: a pair closer than
-// GAP_MIN converges only linearly (halving the error) from the loose
-// estimate and cannot be certified anyway, so its search stops early
-#ifndef HQ_CP_ITMAX_TIGHT
-#define HQ_CP_ITMAX_TIGHT 40
-#endif
-constexpr int ITMAX_TIGHT = HQ_CP_ITMAX_TIGHT;
 constexpr double NEWTON_TOL = 1e-12;   // extremes: |dx| <= TOL (1 + |x|), then one more step
 constexpr double LOOSE_TOL = 1e-2;     // interior roots: only separating points are needed
 constexpr double CERT_ERR = 40.0 * 2.220446049250313e-16;  // > gamma_12 of the Horner bound
@@ -222,9 +215,9 @@ HQD bool normalize(const double (&c)[7], const double (&cabs)[7], double& s, dou
 // Newton's method on the degree-N polynomial d from x; true once a step is
 // below tol (one more step is then taken), false when it does not converge
 // within ITMAX steps or meets a zero / non-finite derivative.
-template <int N> HQD bool newton(const double* d, double& x, double tol, int& its, int itmax = ITMAX) {
+template <int N> HQD bool newton(const double* d, double& x, double tol, int& its) {
 #pragma unroll 1
-  for (int it = 0; it < itmax; ++it) {
+  for (int it = 0; it < ITMAX; ++it) {
     double p, dp;
     horner2<N>(d, x, p, dp);
     ++its;
@@ -319,12 +312,11 @@ HQD bool interior_certify(const double (&b)[7], const double (&eb)[7], double x1
   // of the deflated polynomial's roots (read off its monic coefficients)
   // when that is below the previous root
   double x2 = jmin(x1, upper_bound<4>(d4));
-  const int itmax = tight ? ITMAX_TIGHT : ITMAX;
-  if (!newton<4>(d4, x2, tol, its, itmax)) return false;
+  if (!newton<4>(d4, x2, tol, its)) return false;
   if (tight) x2 = polish(b, x2, its);
   deflate<4>(d4, x2, d3);
   double x3 = jmin(x2, upper_bound<3>(d3));
-  if (!newton<3>(d3, x3, tol, its, itmax)) return false;
+  if (!newton<3>(d3, x3, tol, its)) return false;
   if (tight) x3 = polish(b, x3, its);
   deflate<3>(d3, x3, d2);
   // the last two from the quadratic, in the cancellation-free form
@@ -364,70 +356,7 @@ HQD bool interior_certify(const double (&b)[7], const double (&eb)[7], double x1
   return ok;
 }
 
-// How far the plane's moments are from a Gaussian's: the largest deviation
-// of the standardized moments of orders 3 and 4 from their Gaussian values
-// (0; 3, 3 rho, 1 + 2 rho^2 with rho the correlation).  s: the 15 plane
-// moments in the flux Jacobian's order (m00 m01 m02 m03 m04 m10 m11 m12 m13
-// m20 m21 m22 m30 m31 m40, first index along the flux).  For a Gaussian the
-// 2-D closure's Jacobian has a double eigenvalue at the mean velocity
-// (u +- sqrt(3) sigma, u +- sigma, u, u), so a plane this close to one has an
-// interior pair the certificate cannot separate: when the loose pass fails
-// on such a plane, the solve gives up instead of converging the pair in the
-// tight pass (a routing decision only: the LAPACK path decides the Jacobian
-// either way).
-// NaN when the moments cannot be standardized.
-constexpr double NEAR_GAUSS = 1e-7;
-HQD double gauss_defect(const double* s) {
-  double m[5][5];  // m[i][j] for i + j <= 4, normalised by the density
-  const double r = 1.0 / s[0];
-  int q = 0;
-#pragma unroll
-  for (int i = 0; i <= 4; ++i)
-#pragma unroll
-    for (int j = 0; j <= 4 - i; ++j) m[i][j] = s[q++] * r;
-  const double u = m[1][0], v = m[0][1];
-  // central moments c[i][j] = sum_a sum_b C(i,a) C(j,b) (-u)^(i-a) (-v)^(j-b) m[a][b]
-  double c[5][5];
-#pragma unroll
-  for (int i = 0; i <= 4; ++i)
-#pragma unroll
-    for (int j = 0; j <= 4 - i; ++j) {
-      double t[5];  // shift along the first index for each b <= j
-#pragma unroll
-      for (int b = 0; b <= j; ++b) {
-        double acc = 0.0, pw = 1.0;
-#pragma unroll
-        for (int a = i; a >= 0; --a) {
-          acc = acc + double(T_BIN[i * 7 + a]) * pw * m[a][b];
-          pw = pw * (-u);
-        }
-        t[b] = acc;
-      }
-      double acc = 0.0, pw = 1.0;
-#pragma unroll
-      for (int b = j; b >= 0; --b) {
-        acc = acc + double(T_BIN[j * 7 + b]) * pw * t[b];
-        pw = pw * (-v);
-      }
-      c[i][j] = acc;
-    }
-  const double sx = sqrt(c[2][0]), sy = sqrt(c[0][2]);
-  const double ix = 1.0 / sx, iy = 1.0 / sy;
-  const double rho = c[1][1] * ix * iy;
-  double d = 0.0;
-  d = fmax(d, fabs(c[3][0] * ix * ix * ix));
-  d = fmax(d, fabs(c[0][3] * iy * iy * iy));
-  d = fmax(d, fabs(c[2][1] * ix * ix * iy));
-  d = fmax(d, fabs(c[1][2] * ix * iy * iy));
-  d = fmax(d, fabs(c[4][0] * (ix * ix) * (ix * ix) - 3.0));
-  d = fmax(d, fabs(c[0][4] * (iy * iy) * (iy * iy) - 3.0));
-  d = fmax(d, fabs(c[3][1] * (ix * ix * ix) * iy - 3.0 * rho));
-  d = fmax(d, fabs(c[1][3] * ix * (iy * iy * iy) - 3.0 * rho));
-  d = fmax(d, fabs(c[2][2] * (ix * ix) * (iy * iy) - (1.0 + 2.0 * rho * rho)));
-  return (sx > 0.0 && sy > 0.0 && d == d) ? d : qnan();
-}
-
-HQD CpOut solve(const double (&b)[7], const double (&eb)[7], double xhi, double xlo, const double* plane = nullptr) {
+HQD CpOut solve(const double (&b)[7], const double (&eb)[7], double xhi, double xlo) {
   CpOut o;
   o.ok = false;
   o.its = 0;
@@ -438,11 +367,7 @@ HQD CpOut solve(const double (&b)[7], const double (&eb)[7], double xhi, double 
   if (!(x6 < x1)) return o;
   // interior roots placed loosely first; a cluster (a near-double interior
   // pair, common in nearly Gaussian cells) needs them converged
-  if (!interior_certify(b, eb, x1, x6, false, o.its)) {
-    // a nearly Gaussian plane's close pair is beyond the tight pass
-    if (plane && !(gauss_defect(plane) >= NEAR_GAUSS)) return o;
-    if (!interior_certify(b, eb, x1, x6, true, o.its)) return o;
-  }
+  if (!interior_certify(b, eb, x1, x6, false, o.its) && !interior_certify(b, eb, x1, x6, true, o.its)) return o;
   // conditioning of the two extremes
   bool ok = true;
 #pragma unroll
@@ -499,8 +424,7 @@ struct Extremes {
   int its;
   bool ok;
 };
-HQD Extremes extremes(const double* r3, const double* r5, const double* r6, double lo_seed, double hi_seed, double margin,
-                      const double* plane = nullptr) {
+HQD Extremes extremes(const double* r3, const double* r5, const double* r6, double lo_seed, double hi_seed, double margin) {
   Extremes e;
   e.ok = false;
   e.its = 0;
@@ -511,7 +435,7 @@ HQD Extremes extremes(const double* r3, const double* r5, const double* r6, doub
   if (!normalize(c, cabs, s, sig, b, eb)) return e;
   const double xhi = start_above(b, (hi_seed - s) / sig + margin);
   const double xlo = start_below(b, (lo_seed - s) / sig - margin);
-  const CpOut o = solve(b, eb, xhi, xlo, plane);
+  const CpOut o = solve(b, eb, xhi, xlo);
   e.its = o.its + 2;
   if (!o.ok) return e;
   e.vmin = s + sig * o.xmin;

@@ -479,7 +479,7 @@ template <int MODE> HQN EigOut jac_eigs_t(const double* ma, const Seeds sd) {
     if (!eig_real_jac_p1(h, wr, wi)) { o.deferred = true; return o; }
   } else if (MODE == JAC_CP) {
     if (!eig_real_jac_p1(h, wr, wi)) {
-      const cp::Extremes e = cp::extremes(r3, r5, r6, sd.lo, sd.hi, sd.margin, ma);
+      const cp::Extremes e = cp::extremes(r3, r5, r6, sd.lo, sd.hi, sd.margin);
       if (!e.ok) { o.deferred = true; return o; }
       o.vmin = e.vmin;
       o.vmax = e.vmax;

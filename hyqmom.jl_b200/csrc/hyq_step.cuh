@@ -190,9 +190,11 @@ void launch_hll(const double* M, const double* Fx, const double* Fy, const doubl
                 const DevClock* clk, cudaStream_t s, int variant = 0);
 // The HLL kernel's launch shapes: cells per block and moment groups (the 35
 // moments split over that many blocks of the same cells).
-constexpr int HLL_VARIANTS = 6;
+// Variants 6 and 7 trade registers for occupancy (6 and 5 blocks of 256
+// per SM instead of 4).
+constexpr int HLL_VARIANTS = 8;
 inline void hll_shape(int variant, int& bs, int& groups) {
-  static const int tab[HLL_VARIANTS][2] = {{256, 1}, {256, 5}, {256, 7}, {128, 5}, {128, 7}, {128, 1}};
+  static const int tab[HLL_VARIANTS][2] = {{256, 1}, {256, 5}, {256, 7}, {128, 5}, {128, 7}, {128, 1}, {256, 7}, {256, 5}};
   const int v = (variant >= 0 && variant < HLL_VARIANTS) ? variant : 0;
   bs = tab[v][0];
   groups = tab[v][1];

@@ -105,14 +105,6 @@ void sh_cp_extremes(const double* A, double lo_seed, double hi_seed, double marg
   const cp::Extremes e = cp::extremes(A + 12, A + 24, A + 30, lo_seed, hi_seed, margin);
   out[0] = e.ok ? 1.0 : 0.0; out[1] = e.vmin; out[2] = e.vmax; out[3] = e.its;
 }
-// certified extremes with the plane's moments (the step's form: a nearly
-// Gaussian plane gives up after the loose pass): out = {ok, vmin, vmax, its}
-void sh_cp_extremes_plane(const double* A, const double* plane, double lo_seed, double hi_seed, double margin, double* out) {
-  const cp::Extremes e = cp::extremes(A + 12, A + 24, A + 30, lo_seed, hi_seed, margin, plane);
-  out[0] = e.ok ? 1.0 : 0.0; out[1] = e.vmin; out[2] = e.vmax; out[3] = e.its;
-}
-// the Gaussian defect of 15 plane moments (the certified path's routing test)
-double sh_gauss_defect(const double* s) { return cp::gauss_defect(s); }
 // the step's own exp and cbrt (hyq_cell.cuh) on n arguments
 void sh_hexp_n(const double* x, double* y, long long n) { for (long long i = 0; i < n; ++i) y[i] = hexp(x[i]); }
 void sh_hcbrt_n(const double* x, double* y, long long n) { for (long long i = 0; i < n; ++i) y[i] = hcbrt(x[i]); }

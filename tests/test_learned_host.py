@@ -203,64 +203,3 @@ def test_mixture_moments_are_realizable():
         mom = np.array([[m[0], m[1], m[5], m[15]], [m[1], m[2], m[6], m[16]], [m[5], m[6], m[9], m[25]],
                         [m[15], m[16], m[25], m[19]]])
         assert np.linalg.eigvalsh(mom).min() > 0
-
-
-def test_gauss_defect_routes_near_gaussian_planes(shim):
-    """The certified path's routing test: a Gaussian plane has defect ~0 (its
-    Jacobian has a double eigenvalue at the mean velocity, which the
-    certificate cannot separate), a perturbed one a defect of the
-    perturbation's size, a mixture a large one; and on the headline-like
-    evolved states the planes routed to the LAPACK path (defect < 1e-7)
-    are ones the certificate would not have certified."""
-    shim.sh_gauss_defect.restype = ctypes.c_double
-    rng = np.random.default_rng(11)
-    lib = ol.load()
-    for _ in range(5):
-        mu = rng.normal(size=3)
-        A = rng.normal(size=(3, 5)) / np.sqrt(5.0)
-        M = wavenet.gaussian_raw_moments(mu[None, :], (A @ A.T)[None, :, :])[:, 0]
-        for sl in SLICES:
-            a = np.ascontiguousarray(M[sl])
-            assert shim.sh_gauss_defect(_p(a)) < 1e-12
-            J = np.zeros(36)
-            lib.hyqo_jacobian6(_p(a), _p(J))
-            assert not cp_extremes(shim, J.reshape(6, 6))[0]
-            b = a.copy()
-            b[13] *= 1.0 + 1e-4  # m31
-            assert 1e-6 < shim.sh_gauss_defect(_p(b)) < 1e-2
-    mix = wavenet.mixture_moments(200, rng, Ma=1.0)
-    d = [shim.sh_gauss_defect(_p(np.ascontiguousarray(mix[SLICES[0], c]))) for c in range(200)]
-    assert np.median(d) > 1e-2
-
-
-def test_routed_planes_would_not_certify(shim):
-    """Planes within the routing threshold of a Gaussian (random Gaussians,
-    every moment perturbed by up to 1e-9 relative): the certificate fails on
-    (nearly) all of them, so giving up before the tight pass only saves the
-    failed search; the solve given the plane's moments does, with fewer
-    polynomial evaluations, and certifies the same Jacobians."""
-    shim.sh_gauss_defect.restype = ctypes.c_double
-    rng = np.random.default_rng(12)
-    lib = ol.load()
-    routed = certified = 0
-    saved = 0.0
-    for _ in range(200):
-        mu = rng.normal(size=3)
-        A = rng.normal(size=(3, 5)) / np.sqrt(5.0)
-        M = wavenet.gaussian_raw_moments(mu[None, :], (A @ A.T)[None, :, :])[:, 0]
-        for sl in SLICES:
-            a = np.ascontiguousarray(M[sl] * (1.0 + 1e-9 * rng.uniform(-1.0, 1.0, size=15)))
-            if not shim.sh_gauss_defect(_p(a)) < 1e-7:
-                continue
-            J = np.zeros(36)
-            lib.hyqo_jacobian6(_p(a), _p(J))
-            routed += 1
-            full = cp_extremes(shim, J.reshape(6, 6))
-            out = np.zeros(4)
-            shim.sh_cp_extremes_plane(_p(J), _p(a), ctypes.c_double(np.nan), ctypes.c_double(np.nan), ctypes.c_double(0.0), _p(out))
-            certified += int(full[0])
-            saved += full[3] - out[3]
-            assert bool(out[0]) == full[0] or not full[0]
-    print(f"planes routed: {routed}, of which the full certificate would have certified {certified}; "
-          f"evaluations saved per routed plane {saved / max(1, routed):.1f}")
-    assert routed > 300 and certified <= 0.01 * routed and saved > 0
