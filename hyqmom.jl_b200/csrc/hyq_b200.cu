@@ -172,14 +172,18 @@ __device__ __forceinline__ double hll_flux(const HllFace& f, double mj, double m
 
 // The x, y or z update of one moment of the cell (pas_HLL for that line);
 // M, F already offset to the moment.
-__device__ __forceinline__ double hll_update(const double* __restrict__ M, const double* __restrict__ F, const HllLine& L) {
-  if (L.two) return M[L.base + L.st];
-  const long long o = L.base;
-  const double mL = M[o], mC = M[o + L.st], mR = M[o + 2 * L.st];
-  const double fL = F[o], fC = F[o + L.st], fR = F[o + 2 * L.st];
+// Mp, Fp: the moment and flux at cell L of the line (or at the line start
+// when Np == 2), neighbours mst and fst apart (global memory or shared tiles).
+__device__ __forceinline__ double hll_update_at(const double* Mp, const double* Fp, long long mst, long long fst, const HllLine& L) {
+  if (L.two) return Mp[mst];
+  const double mL = Mp[0], mC = Mp[mst], mR = Mp[2 * mst];
+  const double fL = Fp[0], fC = Fp[fst], fR = Fp[2 * fst];
   const double f1 = hll_flux(L.f1, mC, mR, fC, fR, fC, L.sh1 ? fC : fR, mC, mR);
   const double f0 = L.sh0 ? hll_flux(L.f0, mC, mR, fC, fR, fC, fC, mL, mC) : hll_flux(L.f0, mL, mC, fL, fC, fL, fC, mL, mC);
   return mC - L.r * (f1 - f0);
+}
+__device__ __forceinline__ double hll_update(const double* __restrict__ M, const double* __restrict__ F, const HllLine& L) {
+  return hll_update_at(M + L.base, F + L.base, L.st, L.st, L);
 }
 
 // One thread per cell and moment group: the face speeds of the x, y and z
@@ -264,6 +268,95 @@ __global__ void __launch_bounds__(BS, MINB) k_hll_b(const Batch bt) {
   hll_body<BS, GROUPS>(d.buf[DB_M], d.buf[DB_FX], d.buf[DB_FY], d.buf[DB_FZ], d.buf[DB_VP], d.buf[DB_MTMP], sc, d.clk,
                        blockIdx.x - __ldg(bt.blk0 + m));
 }
+// The HLL sweep on 32 x TY cell tiles of one layer, one group of five
+// moments per block: the group's M (with two cells of halo along x and y),
+// Fx and Fy tiles are staged in shared memory once, then one line of faces
+// at a time reads its three cells from there (z from global memory), the
+// sums formed in the same order as the per-cell kernels, ((mx + my) + mz) -
+// 2 M, from the same values.
+constexpr int HT_X = 32, HT_K = 5, HT_G = 7;
+template <int TY>
+__device__ __forceinline__ void hll_tile_body(const double* __restrict__ M, const double* __restrict__ Fx, const double* __restrict__ Fy,
+                                              const double* __restrict__ Fz, const double* __restrict__ vp, double* __restrict__ Mout,
+                                              const StepConst& sc, const DevClock* clk, int bid) {
+  constexpr int MX = HT_X + 4, MY = TY + 4, SZM = MY * MX, SZX = TY * MX, SZY = MY * HT_X, BS = HT_X * TY;
+  __shared__ double sM[HT_K * SZM], sFx[HT_K * SZX], sFy[HT_K * SZY];
+  if (!clk->active) return;  // uniform over the block
+  const long long N = sc.N;
+  const int Nx = sc.Nx, Ny = sc.Ny, Nz = sc.Nz;
+  const int tiles_x = (Nx + HT_X - 1) / HT_X, tiles_y = (Ny + TY - 1) / TY;
+  const int grp = bid % HT_G;
+  int t = bid / HT_G;
+  const int tx0 = (t % tiles_x) * HT_X;
+  t /= tiles_x;
+  const int ty0 = (t % tiles_y) * TY;
+  const int k = t / tiles_y;
+  const int lx = threadIdx.x % HT_X, ly = threadIdx.x / HT_X;
+  const int i = tx0 + lx, j = ty0 + ly;
+  const long long plane = (long long)Nx * Ny * k;
+  const int n0 = HT_K * grp;
+  // stage the group's tiles (clamped coordinates: every load in range)
+#pragma unroll 1
+  for (int q = 0; q < HT_K; ++q) {
+    const long long mo = N * (n0 + q) + plane;
+    for (int e = threadIdx.x; e < SZM; e += BS) {
+      const int r = e / MX, w = e % MX;
+      sM[q * SZM + e] = M[mo + (long long)Nx * min(max(ty0 - 2 + r, 0), Ny - 1) + min(max(tx0 - 2 + w, 0), Nx - 1)];
+    }
+    for (int e = threadIdx.x; e < SZX; e += BS) {
+      const int r = e / MX, w = e % MX;
+      sFx[q * SZX + e] = Fx[mo + (long long)Nx * min(ty0 + r, Ny - 1) + min(max(tx0 - 2 + w, 0), Nx - 1)];
+    }
+    for (int e = threadIdx.x; e < SZY; e += BS) {
+      const int r = e / HT_X, w = e % HT_X;
+      sFy[q * SZY + e] = Fy[mo + (long long)Nx * min(max(ty0 - 2 + r, 0), Ny - 1) + min(tx0 + w, Nx - 1)];
+    }
+  }
+  __syncthreads();
+  if (!(i < Nx && j < Ny)) return;
+  const long long c = plane + (long long)Nx * j + i;
+  const double dt = clk->dt;
+  double acc[HT_K];
+  {
+    const HllLine X = hll_setup(vp, vp + N, c - i, 1, Nx, i, dt / sc.dx);
+    const int colX = int(X.base - (c - i)) - (tx0 - 2);  // cell L of the x line in the tile
+#pragma unroll
+    for (int q = 0; q < HT_K; ++q) acc[q] = hll_update_at(sM + q * SZM + (ly + 2) * MX + colX, sFx + q * SZX + ly * MX + colX, 1, 1, X);
+  }
+  {
+    const HllLine Y = hll_setup(vp + 2 * N, vp + 3 * N, c - (long long)j * Nx, Nx, Ny, j, dt / sc.dy);
+    const int rowY = int((Y.base - (c - (long long)j * Nx)) / Nx) - (ty0 - 2);  // cell L of the y line
+#pragma unroll
+    for (int q = 0; q < HT_K; ++q)
+      acc[q] = acc[q] + hll_update_at(sM + q * SZM + rowY * MX + lx + 2, sFy + q * SZY + rowY * HT_X + lx, MX, HT_X, Y);
+  }
+  HllLine Z;
+  if (Nz > 1) Z = hll_setup(vp + 4 * N, vp + 5 * N, c - (long long)k * Nx * Ny, Nx * Ny, Nz, k, dt / sc.dz);
+#pragma unroll
+  for (int q = 0; q < HT_K; ++q) {
+    const long long mo = N * (n0 + q);
+    const double mc = sM[q * SZM + (ly + 2) * MX + lx + 2];
+    const double mz = (Nz == 1) ? mc : hll_update(M + mo, Fz + mo, Z);
+    Mout[c + mo] = acc[q] + mz - 2.0 * mc;
+  }
+}
+
+template <int TY, int MINB>
+__global__ void __launch_bounds__(HT_X * TY, MINB) k_hll_tile(const double* __restrict__ M, const double* __restrict__ Fx,
+                                                         const double* __restrict__ Fy, const double* __restrict__ Fz,
+                                                         const double* __restrict__ vp, double* __restrict__ Mout, const StepConst sc,
+                                                         const DevClock* clk) {
+  hll_tile_body<TY>(M, Fx, Fy, Fz, vp, Mout, sc, clk, blockIdx.x);
+}
+template <int TY, int MINB>
+__global__ void __launch_bounds__(HT_X * TY, MINB) k_hll_tile_b(const Batch bt) {
+  const int m = member_of(bt, blockIdx.x);
+  const Dom& d = bt.dom[m];
+  const StepConst sc = d.sc;
+  hll_tile_body<TY>(d.buf[DB_M], d.buf[DB_FX], d.buf[DB_FY], d.buf[DB_FZ], d.buf[DB_VP], d.buf[DB_MTMP], sc, d.clk,
+                    blockIdx.x - __ldg(bt.blk0 + m));
+}
+
 template <int BS, int GROUPS, int MINB = HQ_MINB_HLL * 256 / BS>
 void hll_launch(const double* M, const double* Fx, const double* Fy, const double* Fz, const double* vp, double* Mout, const StepConst& sc,
                 const DevClock* clk, cudaStream_t s) {
@@ -279,12 +372,12 @@ void hll_variant(int variant, const double* M, const double* Fx, const double* F
     case 5: hll_launch<128, 1>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
     case 6: hll_launch<256, 7, 6>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
     case 7: hll_launch<256, 5, 5>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
+    case 8: k_hll_tile<8, 4><<<hll_blocks(8, sc.Nx, sc.Ny, sc.Nz), HT_X * 8, 0, s>>>(M, Fx, Fy, Fz, vp, Mout, sc, clk); break;
+    case 9: k_hll_tile<4, 6><<<hll_blocks(9, sc.Nx, sc.Ny, sc.Nz), HT_X * 4, 0, s>>>(M, Fx, Fy, Fz, vp, Mout, sc, clk); break;
     default: hll_launch<256, 1>(M, Fx, Fy, Fz, vp, Mout, sc, clk, s); break;
   }
 }
 void hll_variant_b(int variant, const Batch& bt, int nblk, cudaStream_t s) {
-  int bs, g;
-  hll_shape(variant, bs, g);
   switch (variant) {
     case 1: k_hll_b<256, 5><<<nblk, 256, 0, s>>>(bt); break;
     case 2: k_hll_b<256, 7><<<nblk, 256, 0, s>>>(bt); break;
@@ -293,6 +386,8 @@ void hll_variant_b(int variant, const Batch& bt, int nblk, cudaStream_t s) {
     case 5: k_hll_b<128, 1><<<nblk, 128, 0, s>>>(bt); break;
     case 6: k_hll_b<256, 7, 6><<<nblk, 256, 0, s>>>(bt); break;
     case 7: k_hll_b<256, 5, 5><<<nblk, 256, 0, s>>>(bt); break;
+    case 8: k_hll_tile_b<8, 4><<<nblk, HT_X * 8, 0, s>>>(bt); break;
+    case 9: k_hll_tile_b<4, 6><<<nblk, HT_X * 4, 0, s>>>(bt); break;
     default: k_hll_b<256, 1><<<nblk, 256, 0, s>>>(bt); break;
   }
 }
@@ -1096,8 +1191,6 @@ int batch_plan(hyq_batch* b) {
   const int n = (int)b->sims.size();
   std::vector<Dom> dom(n);
   std::vector<int> blk((size_t)DK_NKIND * (n + 1), 0);
-  int hbs, hg;
-  hll_shape(b->hll_variant, hbs, hg);
   for (int m = 0; m < n; ++m) {
     const hyq_ctx* c = b->sims[m];
     Dom& d = dom[m];
@@ -1106,7 +1199,7 @@ int batch_plan(hyq_batch* b) {
     d.buf[DB_M] = c->M; d.buf[DB_MTMP] = c->Mtmp; d.buf[DB_FX] = c->Fx; d.buf[DB_FY] = c->Fy; d.buf[DB_FZ] = c->Fz;
     d.buf[DB_VP] = c->vp; d.buf[DB_BMAX] = c->blockmax;
     int nb[DK_NKIND];
-    dom_blocks(c->N, hbs, hg, CORR_CAPS[b->corr_variant], nb);
+    dom_blocks(c->sc.Nx, c->sc.Ny, c->sc.Nz, b->hll_variant, CORR_CAPS[b->corr_variant], nb);
     for (int k = 0; k < DK_NKIND; ++k) {
       const long long next = (long long)blk[(size_t)k * (n + 1) + m] + nb[k];
       if (next > 0x7fffffffLL) return fail(nullptr, HYQ_EINVAL, "fused batch: too many blocks in one launch");

@@ -104,6 +104,19 @@ constexpr int BS_CELLS = 128;
 
 inline int grid_of(long long n, int bs) { return int((n + bs - 1) / bs); }
 
+// The HLL kernel's launch shapes: cells per block and moment groups (the 35
+// moments split over that many blocks of the same cells).
+// Variants 6 and 7 trade registers for occupancy (6 and 5 blocks of 256
+// per SM instead of 4); 8 and 9 stage 32 x 8 and 32 x 4 cell tiles of a
+// layer in shared memory, seven groups of five moments (their grids count
+// tiles: hll_blocks).
+constexpr int HLL_VARIANTS = 10;
+inline void hll_shape(int variant, int& bs, int& groups) {
+  static const int tab[HLL_VARIANTS][2] = {{256, 1}, {256, 5}, {256, 7}, {128, 5}, {128, 7}, {128, 1}, {256, 7}, {256, 5}, {256, 7}, {128, 7}};
+  const int v = (variant >= 0 && variant < HLL_VARIANTS) ? variant : 0;
+  bs = tab[v][0];
+  groups = tab[v][1];
+}
 // ---- fused batches: many independent domains in one launch per kernel ----
 // A member as the fused kernels see it: its constants, clock and buffers.
 enum DomBuf { DB_M = 0, DB_MTMP, DB_FX, DB_FY, DB_FZ, DB_VP, DB_BMAX, DB_NBUF };
@@ -118,11 +131,21 @@ enum DomKind { DK_CELLS = 0, DK_CORR, DK_HLL, DK_ONE, DK_DIAG, DK_NKIND };
 constexpr int DK_MAX_MEMBERS = 4096;
 // The block counts of member m's launch of each kind (hll_g: the HLL
 // kernel's moment groups; corr_cap: the correction passes' blocks per member).
-inline void dom_blocks(long long N, int hll_bs, int hll_g, int corr_cap, int* nb) {
+// The HLL kernel's blocks for a grid: cell blocks x moment groups, or for
+// the tiled variants (8, 9) 32 x 8 or 32 x 4 tiles per layer x layers x groups.
+inline int hll_blocks(int variant, int Nx, int Ny, int Nz) {
+  int bs, g;
+  hll_shape(variant, bs, g);
+  if (variant == 8) return ((Nx + 31) / 32) * ((Ny + 7) / 8) * Nz * g;
+  if (variant == 9) return ((Nx + 31) / 32) * ((Ny + 3) / 4) * Nz * g;
+  return grid_of((long long)Nx * Ny * Nz, bs) * g;
+}
+inline void dom_blocks(int Nx, int Ny, int Nz, int hll_variant, int corr_cap, int* nb) {
+  const long long N = (long long)Nx * Ny * Nz;
   const int g = grid_of(N, BS_A);
   nb[DK_CELLS] = g;
   nb[DK_CORR] = (g < corr_cap ? g : corr_cap) * CORR_SPLIT;
-  nb[DK_HLL] = grid_of(N, hll_bs) * hll_g;
+  nb[DK_HLL] = hll_blocks(hll_variant, Nx, Ny, Nz);
   nb[DK_ONE] = 1;
   const int gd = grid_of(N, 256);
   nb[DK_DIAG] = gd < 64 ? gd : 64;
@@ -188,17 +211,6 @@ void launch_maxdiff(const double* M, const StepConst& sc, DevClock* clk, cudaStr
 // same bits
 void launch_hll(const double* M, const double* Fx, const double* Fy, const double* Fz, const double* vp, double* Mout, const StepConst& sc,
                 const DevClock* clk, cudaStream_t s, int variant = 0);
-// The HLL kernel's launch shapes: cells per block and moment groups (the 35
-// moments split over that many blocks of the same cells).
-// Variants 6 and 7 trade registers for occupancy (6 and 5 blocks of 256
-// per SM instead of 4).
-constexpr int HLL_VARIANTS = 8;
-inline void hll_shape(int variant, int& bs, int& groups) {
-  static const int tab[HLL_VARIANTS][2] = {{256, 1}, {256, 5}, {256, 7}, {128, 5}, {128, 7}, {128, 1}, {256, 7}, {256, 5}};
-  const int v = (variant >= 0 && variant < HLL_VARIANTS) ? variant : 0;
-  bs = tab[v][0];
-  groups = tab[v][1];
-}
 // Fused batches (one launch per kernel for all members of the plan):
 // phase [A] (after_a1, when set, runs after the first closure: the learned
 // path's per-member network launches), the CFL reduction, the diagnostics and

@@ -313,7 +313,9 @@ int hyq_batch_advance(hyq_batch* b, int64_t max_steps, int32_t* ndone, int32_t* 
  * workload and keeps the choice per device.
  *   HYQ_KERNEL_HLL: cells per block x moment groups of the HLL sweep
  *     (0: 256 x 1, 1: 256 x 5, 2: 256 x 7, 3: 128 x 5, 4: 128 x 7, 5: 128 x 1;
- *     6: 256 x 7 and 7: 256 x 5 with fewer registers for more resident blocks);
+ *     6: 256 x 7 and 7: 256 x 5 with fewer registers for more resident blocks;
+ *     8, 9: 32 x 8 and 32 x 4 cell tiles of a layer staged in shared memory,
+ *     7 groups of 5 moments);
  *     per context (hyq_set_variant) or for every member of a batch.
  *   HYQ_KERNEL_CORR: blocks per member of a fused batch's correction passes
  *     (0: 64, 1: 16, 2: 4, 3: 592); batches only. */

@@ -125,10 +125,14 @@ def test_learned_members_in_a_fused_batch():
         b.close()
 
 
-def test_hll_variants_give_the_same_bits():
+@pytest.mark.parametrize("shape", [(20, 18, 10), (33, 9, 2), (2, 3, 1), (40, 2, 3)])
+def test_hll_variants_give_the_same_bits(shape):
+    """Every HLL launch shape, the shared-memory tiles included, on grids with
+    partial tiles, two-cell lines (pas_HLL's Np == 2 rule) and one layer."""
     cuda()
     from hyqmom.runner import Solver, variant_count
-    p = ic.with_jets(ic.default_params(Nx=20, Ny=18, Nz=10, Ma=1.0, Kn=0.1, CFL=0.5, tmax=10.0, nnmax=100), "crossing")
+    Nx, Ny, Nz = shape
+    p = ic.with_jets(ic.default_params(Nx=Nx, Ny=Ny, Nz=Nz, Ma=1.0, Kn=0.1, CFL=0.5, tmax=10.0, nnmax=100), "crossing")
     out = []
     for v in range(variant_count("hll")):
         s = Solver(p)
@@ -139,9 +143,9 @@ def test_hll_variants_give_the_same_bits():
             out.append(s.get_state())
         finally:
             s.close()
-    assert len(out) == variant_count("hll") == 8
-    for M in out[1:]:
-        assert np.array_equal(M, out[0])
+    assert len(out) == variant_count("hll") == 10
+    for v, M in enumerate(out[1:], 1):
+        assert np.array_equal(M, out[0], equal_nan=True), v
 
 
 def test_autotuner_keeps_the_run_and_caches(tmp_path):
@@ -156,7 +160,7 @@ def test_autotuner_keeps_the_run_and_caches(tmp_path):
         s.advance(2)
         before = s.get_state()
         got = autotune.tune_solver(s, path=path)
-        assert not got["cached"] and 0 <= got["hll"] < 8
+        assert not got["cached"] and 0 <= got["hll"] < 10
         assert np.array_equal(s.get_state(), before) and s.stats()["nn"] == 2
         again = autotune.tune_solver(s, path=path)
         assert again["cached"] and again["hll"] == got["hll"]
