@@ -139,13 +139,18 @@ def test_hll_variants_give_the_same_bits(shape):
         try:
             s.set_variant("hll", v)
             s.set_state(ic.initial_state(p))
-            s.advance(4)
-            out.append(s.get_state())
+            # some of these small grids meet a non-finite wave speed within
+            # a few steps (reported, not raised here): every variant must
+            # then report the same step and leave the same bits, NaNs included
+            s.advance_async(4)
+            s.synchronize()
+            out.append((s.get_state(), s.stats()["status"], s.stats()["nn"]))
         finally:
             s.close()
     assert len(out) == variant_count("hll") == 10
-    for v, M in enumerate(out[1:], 1):
-        assert np.array_equal(M, out[0], equal_nan=True), v
+    for v, (M, status, nn) in enumerate(out[1:], 1):
+        assert (status, nn) == out[0][1:], v
+        assert np.array_equal(M, out[0][0], equal_nan=True), v
 
 
 def test_autotuner_keeps_the_run_and_caches(tmp_path):
