@@ -62,13 +62,14 @@ MODES = ("plain", "certified", "learned")
 E2E_SLABS = 4
 
 
-RUN_STEPS = {"c5": 500, "c5s": 500, "c2": 200, "c2s": 200, "c1": 100}
+RUN_STEPS = {"c5": 500, "c5s": 500, "c3": 200, "c2": 200, "c2s": 200, "c1": 100}
 
 
 def workload(name="c5"):
     """Crossing jets (the reference's IC generator): c5 256x256x128 Ma=1
     Kn=0.01 (the headline, 500 steps); c5s the c5 case on 128x128x64
-    (profiling captures); c2 160x160x80 Ma=1 Kn=1 (200 steps);
+    (profiling captures); c3 160x160x80 Ma=1 Kn=0.1 (the learned path's
+    evaluation case, 200 steps); c2 160x160x80 Ma=1 Kn=1 (200 steps);
     c2s the c2 case on 96x96x48 (profiling captures); c1 20^3 Ma=0 Kn=1.
     CFL 0.5 for c5/c2/c2s: at the named 0.7 the scheme turns a flux Jacobian
     non-finite within a few steps of this IC (the reference's eigvals throws
@@ -78,6 +79,8 @@ def workload(name="c5"):
         p = ic.default_params(Nx=256, Ny=256, Nz=128, Ma=1.0, Kn=0.01, CFL=0.5, tmax=1e9, nnmax=1000000)
     elif name == "c5s":
         p = ic.default_params(Nx=128, Ny=128, Nz=64, Ma=1.0, Kn=0.01, CFL=0.5, tmax=1e9, nnmax=1000000)
+    elif name == "c3":
+        p = ic.default_params(Nx=160, Ny=160, Nz=80, Ma=1.0, Kn=0.1, CFL=0.5, tmax=1e9, nnmax=1000000)
     elif name == "c2":
         p = ic.default_params(Nx=160, Ny=160, Nz=80, Ma=1.0, Kn=1.0, CFL=0.5, tmax=1e9, nnmax=1000000)
     elif name == "c2s":
@@ -630,7 +633,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20, help="steps timed, spread evenly over the run")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c5", choices=["c1", "c2", "c2s", "c4", "c5", "c5s"])
+    ap.add_argument("--config", default="c5", choices=["c1", "c2", "c2s", "c3", "c4", "c5", "c5s"])
     ap.add_argument("--profile", nargs=3, metavar=("MODE", "BEFORE", "AFTER"),
                     help="launch sequence for ncu captures: MODE plain|certified|learned|hll")
     ap.add_argument("--no-cpu-baseline", action="store_true")
