@@ -13,27 +13,8 @@ namespace hyqk {
 namespace {
 
 
-// One cell: in m[35]; out Fx, Fy, Fz, Mr (35 each) and vp[6].
-__device__ __noinline__ void cell_phase_A(const double* m, int flag2D, double Ma, int positivity, double* Fx, double* Fy, double* Fz, double* Mr,
-                                          double* vp) {
-  double a[35], b[35];
-  flux_closure35(m, flag2D, Ma, nullptr, nullptr, nullptr, a);
-  double v6xmin, v6xmax, v6ymin, v6ymax, v6zmin, v6zmax;
-  eigenvalues6(a, 1, flag2D, Ma, v6xmin, v6xmax, b);
-  eigenvalues6(b, 2, flag2D, Ma, v6ymin, v6ymax, a);
-  eigenvalues6z(a, flag2D, Ma, positivity, v6zmin, v6zmax, b);
-  flux_closure35(b, flag2D, Ma, Fx, Fy, Fz, Mr);
-  double v5xmin, v5xmax, v5ymin, v5ymax, v5zmin, v5zmax;
-  closure_eigs(Mr[0], Mr[1], Mr[2], Mr[3], Mr[4], v5xmin, v5xmax);
-  closure_eigs(Mr[0], Mr[5], Mr[9], Mr[12], Mr[14], v5ymin, v5ymax);
-  closure_eigs(Mr[0], Mr[15], Mr[19], Mr[22], Mr[24], v5zmin, v5zmax);
-  vp[0] = jmin(v5xmin, v6xmin); vp[1] = jmax(v5xmax, v6xmax);
-  vp[2] = jmin(v5ymin, v6ymin); vp[3] = jmax(v5ymax, v6ymax);
-  vp[4] = jmin(v5zmin, v6zmin); vp[5] = jmax(v5zmax, v6zmax);
-}
-
 // Phase [A] runs as five kernels, one per-cell function each, so that every
-// kernel's code stays small (the fused cell_phase_A kernel was bound by
+// kernel's code stays small (one kernel for the whole phase was bound by
 // instruction fetch); the intermediate states go through buffers that are
 // dead during phase A:  M -A1-> Fx -A2, A3 (in place)-> Fx -A4-> Mtmp -A5-> M,
 // with the Jacobian speeds of A2-A4 parked in vp and combined in A5 (A2 and A3
@@ -284,15 +265,26 @@ __global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A5_flux_b(const Batch bt
           blockIdx.x - __ldg(bt.blk0 + m));
 }
 
-__global__ void __launch_bounds__(BS_CELLS) k_cells_phase_A(const double* __restrict__ M, long long n, int flag2D, double Ma, int positivity,
-                                                             double* Fx, double* Fy, double* Fz, double* Mr, double* vp) {
+// The last part of the per-cell phase [A]: the closure with fluxes of the
+// z stage's output (read from Fz, which it then overwrites: each thread reads
+// its cell's 35 moments before it writes any output), the 1-D closure speeds,
+// and the six wave speeds from the Jacobian speeds parked in vp.
+__global__ void __launch_bounds__(BS_CELLS) k_cells_phase_A_end(long long n, int flag2D, double Ma, double* Fx, double* Fy, double* Fz,
+                                                                 double* Mr, double* vp) {
   const long long c = (long long)blockIdx.x * BS_CELLS + threadIdx.x;
   if (c >= n) return;
-  double m[35], fx[35], fy[35], fz[35], r[35], v[6];
-  for (int q = 0; q < 35; ++q) m[q] = M[c + n * q];
-  cell_phase_A(m, flag2D, Ma, positivity, fx, fy, fz, r, v);
+  double m[35], fx[35], fy[35], fz[35], r[35];
+  for (int q = 0; q < 35; ++q) m[q] = Fz[c + n * q];
+  flux_closure35(m, flag2D, Ma, fx, fy, fz, r);
+  double v5[6];
+  closure_eigs(r[0], r[1], r[2], r[3], r[4], v5[0], v5[1]);
+  closure_eigs(r[0], r[5], r[9], r[12], r[14], v5[2], v5[3]);
+  closure_eigs(r[0], r[15], r[19], r[22], r[24], v5[4], v5[5]);
+  for (int q = 0; q < 6; q += 2) {
+    vp[c + n * q] = jmin(v5[q], vp[c + n * q]);
+    vp[c + n * (q + 1)] = jmax(v5[q + 1], vp[c + n * (q + 1)]);
+  }
   for (int q = 0; q < 35; ++q) { Fx[c + n * q] = fx[q]; Fy[c + n * q] = fy[q]; Fz[c + n * q] = fz[q]; Mr[c + n * q] = r[q]; }
-  for (int q = 0; q < 6; ++q) vp[c + n * q] = v[q];
 }
 
 }  // namespace
@@ -334,9 +326,19 @@ void launch_phase_A_batch(const BatchPlan& bp, int mode, cudaStream_t s, void (*
   }
   k_A5_flux_b<<<g, BS_A, 0, s>>>(cells);
 }
+// The per-cell phase [A] (the step's phase A for independent cells, without
+// the HLL neighbours) as a chain of per-function kernels, with the caller's
+// outputs as the intermediate states: closure M -> Mr, x stage Mr -> Fx, y
+// stage Fx -> Mr, z stage Mr -> Fz (Jacobian speeds into vp), then the
+// closure with fluxes.  Small kernels, as in the step: one kernel calling the
+// whole chain per thread faulted on the GPU.
 void launch_cells_phase_A(const double* M, long long n, int flag2D, double Ma, int positivity, double* Fx, double* Fy, double* Fz,
                           double* Mr, double* vp, cudaStream_t s) {
-  k_cells_phase_A<<<grid_of(n, BS_CELLS), BS_CELLS, 0, s>>>(M, n, flag2D, Ma, positivity, Fx, Fy, Fz, Mr, vp);
+  launch_cells_flux(M, n, flag2D, Ma, nullptr, nullptr, nullptr, Mr, s);
+  launch_cells_eig(Mr, n, 1, flag2D, Ma, positivity, vp, Fx, s);
+  launch_cells_eig(Fx, n, 2, flag2D, Ma, positivity, vp + 2 * n, Mr, s);
+  launch_cells_eig(Mr, n, 3, flag2D, Ma, positivity, vp + 4 * n, Fz, s);
+  k_cells_phase_A_end<<<grid_of(n, BS_CELLS), BS_CELLS, 0, s>>>(n, flag2D, Ma, Fx, Fy, Fz, Mr, vp);
 }
 
 }  // namespace hyqk
