@@ -94,6 +94,8 @@ HQN int realizable_3D(double* s) {
   }
 
   const double beta = 1.0;
+  // one projection store for the whole function: each projection below is
+  // formed, read and dropped before the next (a smaller per-thread frame)
   Delta D;
   delta2star_p(s, 0, D);
   int fE11 = 0, fE22 = 0, fE33 = 0, fE44 = 0, fE55 = 0, fE66 = 0;
@@ -162,10 +164,9 @@ HQN int realizable_3D(double* s) {
       keep(0, D);
       continue;
     }
-    Delta Dp;
-    delta2star_p(s, p, Dp);
-    d2[p] = lead_det_k<2>(Dp);
-    keep(p, Dp);
+    delta2star_p(s, p, D);  // D is not needed after projection 0
+    d2[p] = lead_det_k<2>(D);
+    keep(p, D);
   }
   bool fresh = true;  // d2..Ee are those of the current s
   int flag310 = 0;
@@ -205,11 +206,10 @@ HQN int realizable_3D(double* s) {
   if (flag310) {
     double dm = 0.0;
     for (int p = 0; p < 6; ++p) {
-      Delta Dp;
-      delta2star_p(s, p, Dp);
-      const double d = lead_det_k<2>(Dp);
+      delta2star_p(s, p, D);
+      const double d = lead_det_k<2>(D);
       dm = (p == 0) ? d : jmin(dm, d);
-      keep(p, Dp);
+      keep(p, D);
     }
     if (dm < 0.0) flag220 = 1;
   }
@@ -259,7 +259,7 @@ HQN int realizable_3D(double* s) {
     const int p = (q == 0) ? 0 : (q == 1) ? 2 : (q == 2) ? 1 : (q == 3) ? 3 : (q == 4) ? 4 : 5;
     lo[q] = cur[q]; hi[q] = cur[q];
     if (fresh && !(d4[p] < 0.0)) continue;  // its projection is the kept one
-    Delta E;
+    Delta& E = D;
     delta2star_p(s, p, E);
     if (lead_det_k<4>(E) < 0.0) {
       flag220 = 1;
