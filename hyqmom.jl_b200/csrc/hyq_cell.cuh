@@ -442,13 +442,18 @@ __device__ constexpr int PERM[6][28] = {
 // and the Schur complement E = M22 - Q, for the moments g[] of one
 // permutation.  M11 = 1 (+) R, R the 3x3 correlation matrix; R^-1 by
 // cofactors.  Basis order {x2, xy, xz, y2, yz, z2}.
+// Only the entries the realizability check reads are kept (12 of each
+// triangle): E on the leading 4x4 block and the last two diagonal entries,
+// Q at the diagonal lower bounds and the bound_minor1 values.  The tables
+// give each (a, b) its slot, -1 for an entry that is not kept (never read).
 struct Delta {
-  double e[21];  // upper triangle of E, row-major (0,0),(0,1)..(0,5),(1,1)..
-  double q[21];
+  double e[12];
+  double q[12];
 };
-// explicit table: index of (a,b), a<=b
-__device__ constexpr int TRI[6][6] = {{0, 1, 2, 3, 4, 5}, {1, 6, 7, 8, 9, 10}, {2, 7, 11, 12, 13, 14},
-                                      {3, 8, 12, 15, 16, 17}, {4, 9, 13, 16, 18, 19}, {5, 10, 14, 17, 19, 20}};
+__device__ constexpr int TRI_E[6][6] = {{0, 1, 2, 3, -1, -1}, {1, 4, 5, 6, -1, -1}, {2, 5, 7, 8, -1, -1},
+                                        {3, 6, 8, 9, -1, -1}, {-1, -1, -1, -1, 10, -1}, {-1, -1, -1, -1, -1, 11}};
+__device__ constexpr int TRI_Q[6][6] = {{-1, 0, 1, -1, 2, -1}, {0, 3, -1, 4, -1, 5}, {1, -1, 6, 7, -1, 8},
+                                        {-1, 4, 7, -1, 9, -1}, {2, -1, -1, 9, 10, 11}, {-1, 5, 8, -1, 11, -1}};
 
 HQN void delta2star_p(const double* s, int P, Delta& D) {
   // arguments of delta2star3D for permutation P (named by the argument slot)
@@ -481,13 +486,15 @@ HQN void delta2star_p(const double* s, int P, Delta& D) {
   for (int a = 0; a < 6; ++a)
 #pragma unroll
     for (int b = a; b < 6; ++b) {
+      if (TRI_E[a][b] < 0 && TRI_Q[a][b] < 0) continue;
       const double qv = mu[a] * mu[b] + (w[a][0] * z[b][0] + w[a][1] * z[b][1] + w[a][2] * z[b][2]);
-      D.q[TRI[a][b]] = qv;
-      D.e[TRI[a][b]] = m22[TRI[a][b]] - qv;
+      if (TRI_Q[a][b] >= 0) D.q[TRI_Q[a][b]] = qv;
+      if (TRI_E[a][b] >= 0) D.e[TRI_E[a][b]] = m22[a * 6 + b - a * (a + 1) / 2] - qv;
     }
 }
 
-HQD double E_(const Delta& D, int a, int b) { return D.e[TRI[a][b]]; }
+HQD double E_(const Delta& D, int a, int b) { return D.e[TRI_E[a][b]]; }
+HQD double Q_(const Delta& D, int a, int b) { return D.q[TRI_Q[a][b]]; }
 
 // Leading K x K minor determinant with Julia det semantics (triangular
 // shortcut, else LU with partial pivoting and reciprocal row scaling); K is

@@ -114,7 +114,7 @@ HQN int realizable_3D(double* s) {
   double S220_diag = s[s220], S202_diag = s[s202], S022_diag = s[s022];
   // lower_bound_S220: projection diagonal of the current moments
   if (written) delta2star_p(s, 0, D);
-  const double lb0 = D.q[TRI[1][1]], lb1 = D.q[TRI[2][2]], lb2 = D.q[TRI[4][4]];
+  const double lb0 = Q_(D, 1, 1), lb1 = Q_(D, 2, 2), lb2 = Q_(D, 4, 4);
   if (s[s220] < lb0) { S220_diag = lb0; fE22 = 1; flag220 = 1; }
   if (s[s202] < lb1) { S202_diag = lb1; fE33 = 1; flag220 = 1; }
   if (s[s022] < lb2) { S022_diag = lb2; fE55 = 1; flag220 = 1; }
@@ -127,9 +127,9 @@ HQN int realizable_3D(double* s) {
   if (E_(D, 5, 5) < diagmin) fE66 = 1;
   if (fE11 | fE22 | fE33 | fE44 | fE55 | fE66) {
     // bound_minor1 values from the projection
-    const double S310b = D.q[TRI[0][1]], S301b = D.q[TRI[0][2]], S130b = D.q[TRI[1][3]], S103b = D.q[TRI[2][5]];
-    const double S031b = D.q[TRI[3][4]], S013b = D.q[TRI[4][5]];
-    const double S211b = D.q[TRI[0][4]], S121b = D.q[TRI[2][3]], S112b = D.q[TRI[1][5]];
+    const double S310b = Q_(D, 0, 1), S301b = Q_(D, 0, 2), S130b = Q_(D, 1, 3), S103b = Q_(D, 2, 5);
+    const double S031b = Q_(D, 3, 4), S013b = Q_(D, 4, 5);
+    const double S211b = Q_(D, 0, 4), S121b = Q_(D, 2, 3), S112b = Q_(D, 1, 5);
     if (fE11) { s[s310] = S310b; s[s301] = S301b; s[s211] = S211b; }
     if (fE22) { s[s310] = S310b; s[s130] = S130b; s[s211] = S211b; s[s121] = S121b; s[s112] = S112b; }
     if (fE33) { s[s301] = S301b; s[s103] = S103b; s[s211] = S211b; s[s121] = S121b; s[s112] = S112b; }

@@ -60,6 +60,11 @@ struct StepConst {
 #ifndef HQ_MINB_CLOSURE
 #define HQ_MINB_CLOSURE 4
 #endif
+// The closures without fluxes (A1, E1) run best at 3 blocks (168 registers),
+// measured on step 151 of the 128x128x64 crossing-jets run.
+#ifndef HQ_MINB_REALIZE
+#define HQ_MINB_REALIZE 3
+#endif
 #ifndef HQ_MINB_EIG
 #define HQ_MINB_EIG 8
 #endif
@@ -72,6 +77,7 @@ struct StepConst {
 #define HQ_MINB_FIX 8
 #endif
 constexpr int MINB_CLOSURE = HQ_MINB_CLOSURE;
+constexpr int MINB_REALIZE = HQ_MINB_REALIZE;
 constexpr int MINB_EIG = HQ_MINB_EIG;
 constexpr int MINB_FIX = HQ_MINB_FIX;
 // Eigen-solve code of those passes (hyq::JacMode; 2 = the general code only)

@@ -57,13 +57,13 @@ __device__ __forceinline__ void A1_body(const double* __restrict__ M, double* __
   if (c >= c1) return;
   flux_closure35(M + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
 }
-__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure(const double* __restrict__ M, double* __restrict__ out, double* vp,
+__global__ void __launch_bounds__(BS_A, MINB_REALIZE) k_A1_closure(const double* __restrict__ M, double* __restrict__ out, double* vp,
                                                               const StepConst sc, const DevClock* clk, long long c0, long long c1) {
   A1_body(M, out, vp, sc, clk, c0, c1, blockIdx.x);
 }
 // The fused-batch form of each kernel: the block's member from the table,
 // then the same body on that member's buffers over all its cells.
-__global__ void __launch_bounds__(BS_A, MINB_CLOSURE) k_A1_closure_b(const Batch bt) {
+__global__ void __launch_bounds__(BS_A, MINB_REALIZE) k_A1_closure_b(const Batch bt) {
   const int m = member_of(bt, blockIdx.x);
   const Dom& d = bt.dom[m];
   const StepConst sc = d.sc;

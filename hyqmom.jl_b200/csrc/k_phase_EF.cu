@@ -42,13 +42,13 @@ __device__ __forceinline__ void E1_body(const double* __restrict__ in, double* _
   if (c >= c1) return;
   flux_closure35(in + c, sc.flag2D, sc.Ma, nullptr, nullptr, nullptr, out + c, N, N);
 }
-__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E1_closure(const double* __restrict__ in, double* __restrict__ out, double* vp,
+__global__ void __launch_bounds__(BS_EF, MINB_REALIZE) k_E1_closure(const double* __restrict__ in, double* __restrict__ out, double* vp,
                                                                 const StepConst sc, const DevClock* clk, long long c0, long long c1) {
   E1_body(in, out, vp, sc, clk, c0, c1, blockIdx.x);
 }
 // The fused-batch form of each kernel: the block's member from the table,
 // then the same body on that member's buffers over all its cells.
-__global__ void __launch_bounds__(BS_EF, MINB_CLOSURE) k_E1_closure_b(const Batch bt) {
+__global__ void __launch_bounds__(BS_EF, MINB_REALIZE) k_E1_closure_b(const Batch bt) {
   const int m = member_of(bt, blockIdx.x);
   const Dom& d = bt.dom[m];
   const StepConst sc = d.sc;
