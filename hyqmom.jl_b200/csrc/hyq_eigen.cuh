@@ -550,7 +550,7 @@ HQN void correct_for_real(const double* M, int pa_i, int pa_j, int pb_i, int pb_
   const double M000 = M[0];
   const double u = M[1] / M000, v = M[5] / M000, w = M[15] / M000;
   double C[35], S[35];
-  raw_to_central(M, C);
+  raw_to_central_r(M, 1, C);
   central_to_std(C, S);
   const double Cd[3] = {C[2], C[9], C[19]};
   const double S3[3] = {S[3], S[12], S[22]}, S4v[3] = {S[4], S[14], S[24]};
@@ -562,7 +562,7 @@ HQN void correct_for_real(const double* M, int pa_i, int pa_j, int pb_i, int pb_
   if (planes & 1) corr(pa_i, pa_j);
   if (planes & 2) corr(pb_i, pb_j);
   C[0] = 1.0;
-  central_to_raw(M000, u, v, w, C, 35);
+  central_to_raw_r<35>(M000, u, v, w, C);
   flux_closure35(C, flag2D, Ma, nullptr, nullptr, nullptr, Mout);
 }
 
@@ -840,8 +840,9 @@ HQD void collision35(double* M, double dt, double Kn, int positivity) {
     C[n] = zi * zj * zk * pw[i] * pw[j] * pw[k];
   }
   C[0] = 1.0;
-  central_to_raw(rho, u, v, w, C, 35);
+  central_to_raw_r<35>(rho, u, v, w, C);
   const double e = hexp(-dt / tc);
+#pragma unroll
   for (int n = 0; n < 35; ++n) M[n] = C[n] - e * (C[n] - M[n]);
 }
 
