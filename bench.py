@@ -53,8 +53,8 @@ KERNELS = ["A1_closure", "A2_eig_x", "A3_eig_y", "A4_eig_z", "A5_flux_speeds", "
 # network), from ncu captures of steps 151-152 of crossing jets 128 x 128 x 64
 # (Ma=1, Kn=0.01), scaled to a launch by its cells; the HLL slot per launch
 # variant.
-TRAFFIC_PER_CELL = {"A1_closure": 1374.6, "A2_eig_x": 837.6, "A3_eig_y": 863.2, "A4_eig_z": 1797.3, "A5_flux_speeds": 2840.3,
-                    "E1_closure": 1072.3, "E2_eig_x": 676.3, "E3_eig_y": 663.3, "E4_closure_bgk": 2363.3}
+TRAFFIC_PER_CELL = {"A1_closure": 1356.1, "A2_eig_x": 831.4, "A3_eig_y": 853.4, "A4_eig_z": 1818.4, "A5_flux_speeds": 2845.4,
+                    "E1_closure": 1055.0, "E2_eig_x": 663.4, "E3_eig_y": 652.5, "E4_closure_bgk": 1953.7}
 TRAFFIC_HLL = {0: 1732.6, 1: 1540.5, 2: 1514.4, 3: 1540.1, 4: 1514.9, 5: 1739.5, 6: 1743.6, 7: 1715.1, 8: 1544.4, 9: 1506.7}
 TRAFFIC_SOURCE = ("ncu dram__bytes_read+write per cell, learned path, steps 151-152 of crossing jets 128x128x64 (Ma=1, Kn=0.01), "
                   "scaled to this launch's cells")
