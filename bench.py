@@ -59,7 +59,7 @@ TRAFFIC_HLL = {0: 1732.6, 1: 1540.5, 2: 1514.4, 3: 1540.1, 4: 1514.9, 5: 1739.5,
 TRAFFIC_SOURCE = ("ncu dram__bytes_read+write per cell, learned path, steps 151-152 of crossing jets 128x128x64 (Ma=1, Kn=0.01), "
                   "scaled to this launch's cells")
 MODES = ("plain", "certified", "learned")
-E2E_SLABS = 4
+E2E_SLABS = 6
 
 
 RUN_STEPS = {"c5": 500, "c5s": 500, "c3": 200, "c2": 200, "c2s": 200, "c1": 100}

@@ -1037,6 +1037,29 @@ int hyq_advance(hyq_ctx* ctx, int64_t max_steps, double* t, int64_t* nn, int32_t
   return HYQ_OK;
 }
 
+namespace {
+constexpr double STEP_HOST_RATIO_A = 1.6, STEP_HOST_RATIO_EF = 0.8;
+// Slab boundaries (cells) of S slabs of whole BS_A-cell blocks, slab k's share
+// of the nblk blocks in proportion to ratio^k, at least one block each.
+void slab_cuts(long long N, long long nblk, int S, double ratio, std::vector<long long>& cut) {
+  cut.assign(S + 1, 0);
+  double tot = 0.0, w = 1.0;
+  for (int k = 0; k < S; ++k, w *= ratio) tot += w;
+  long long prev = 0;
+  double acc = 0.0;
+  w = 1.0;
+  for (int k = 1; k < S; ++k, w *= ratio) {
+    acc += w;
+    long long b = (long long)llround((double)nblk * acc / tot);
+    b = std::max(b, prev + 1);
+    b = std::min(b, nblk - (S - k));
+    cut[k] = b * BS_A;
+    prev = b;
+  }
+  cut[S] = N;
+}
+}  // namespace
+
 int hyq_step_host(hyq_ctx* ctx, const double* M_in, double* M_out, int32_t nslabs, double* t, int64_t* nn, int32_t* done) {
   if (!ctx || !M_in || !M_out || nslabs < 1) return fail(ctx, HYQ_EINVAL, "bad argument");
   HQ_CHECK(ctx, cudaSetDevice(ctx->device));
@@ -1052,8 +1075,13 @@ int hyq_step_host(hyq_ctx* ctx, const double* M_in, double* M_out, int32_t nslab
     ctx->up.push_back(a);
     ctx->down.push_back(b);
   }
-  std::vector<long long> cut(S + 1);
-  for (int k = 0; k <= S; ++k) cut[k] = (k == S) ? N : ((nblk * k) / S) * BS_A;
+  // Only the first upload and the last download are not hidden under
+  // compute, so the slabs are unequal: phase A's grow by STEP_HOST_RATIO_A
+  // (the next slab uploads while phase A runs on this one, and phase A costs
+  // about twice the upload), phases E+F's shrink by STEP_HOST_RATIO_EF.
+  std::vector<long long> cut, cute;
+  slab_cuts(N, nblk, S, STEP_HOST_RATIO_A, cut);
+  slab_cuts(N, nblk, S, STEP_HOST_RATIO_EF, cute);
   const size_t pitch = sizeof(double) * (size_t)N;
   cudaStream_t s = ctx->stream, cs = ctx->cstream;
   // upload slab k, then phase A on slab k while slab k+1 is uploading
@@ -1070,7 +1098,7 @@ int hyq_step_host(hyq_ctx* ctx, const double* M_in, double* M_out, int32_t nslab
   hll_variant(ctx->hll_variant, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->Mtmp, ctx->sc, ctx->clk, s);
   // phases E+F slab by slab, each slab downloaded as soon as it is done
   for (int k = 0; k < S; ++k) {
-    const long long c0 = cut[k], c1 = cut[k + 1];
+    const long long c0 = cute[k], c1 = cute[k + 1];
     launch_phase_EF(ctx->sc, ctx->Mtmp, ctx->M, ctx->Fx, ctx->Fy, ctx->Fz, ctx->vp, ctx->clk, s, nullptr, c0, c1);
     HQ_CHECK(ctx, cudaEventRecord(ctx->down[k], s));
     HQ_CHECK(ctx, cudaStreamWaitEvent(cs, ctx->down[k], 0));

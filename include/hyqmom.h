@@ -237,9 +237,11 @@ int hyq_stats_get(hyq_ctx* ctx, hyq_stats* out);
 
 /* One step of the reference loop on a host state, the host<->device copies
  * overlapped with the per-cell phases: the state goes up in `nslabs` chunks
- * of whole z-planes' cells while phase [A] runs on the chunks already there,
+ * of whole 128-cell blocks while phase [A] runs on the chunks already there,
  * and comes back chunk by chunk as phases [E]+[F] finish them (the CFL
- * reduction and the HLL sweep need every cell and run in between).  M_in and
+ * reduction and the HLL sweep need every cell and run in between).  The
+ * chunks are graded: the uploads grow and the downloads shrink, so that only
+ * a small first upload and a small last download are not hidden.  M_in and
  * M_out are host (Nx,Ny,Nz,35) column-major buffers and may be the same; in
  * pinned memory the copies run asynchronously.  The step uses the context's
  * clock (t, nn) like hyq_advance(ctx, 1, ...), with the same outputs and
