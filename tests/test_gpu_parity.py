@@ -1,6 +1,6 @@
 """CUDA path vs the CPU oracle (FP64 throughout).
 
-Tolerances: <= 1e-12 relative for one step and per-cell
+Tolerances (the parity bar of the plain path): <= 1e-12 relative for one step and per-cell
 functions, <= 1e-8 relative on all 35 moments after 100 steps.  "Relative" is
 max |gpu - oracle| / max |oracle| over each moment field (a per-field scale:
 the 35 moments span many orders of magnitude, and near-zero odd moments of a
