@@ -1040,17 +1040,22 @@ int hyq_advance(hyq_ctx* ctx, int64_t max_steps, double* t, int64_t* nn, int32_t
 namespace {
 constexpr double STEP_HOST_RATIO_A = 1.6, STEP_HOST_RATIO_EF = 0.8;
 // Slab boundaries (cells) of S slabs of whole BS_A-cell blocks, slab k's share
-// of the nblk blocks in proportion to ratio^k, at least one block each.
+// of the nblk blocks in proportion to ratio^k, at least one block each.  The
+// share of slabs 0..k-1 is the geometric sum's fraction, written so that no
+// power overflows however many slabs are asked for.
 void slab_cuts(long long N, long long nblk, int S, double ratio, std::vector<long long>& cut) {
   cut.assign(S + 1, 0);
-  double tot = 0.0, w = 1.0;
-  for (int k = 0; k < S; ++k, w *= ratio) tot += w;
+  auto frac = [&](int k) {
+    if (ratio == 1.0) return (double)k / S;
+    if (ratio > 1.0) {
+      const double a = pow(ratio, (double)(k - S)), b = pow(ratio, (double)-S);
+      return (a - b) / (1.0 - b);
+    }
+    return (1.0 - pow(ratio, (double)k)) / (1.0 - pow(ratio, (double)S));
+  };
   long long prev = 0;
-  double acc = 0.0;
-  w = 1.0;
-  for (int k = 1; k < S; ++k, w *= ratio) {
-    acc += w;
-    long long b = (long long)llround((double)nblk * acc / tot);
+  for (int k = 1; k < S; ++k) {
+    long long b = (long long)llround((double)nblk * frac(k));
     b = std::max(b, prev + 1);
     b = std::min(b, nblk - (S - k));
     cut[k] = b * BS_A;
