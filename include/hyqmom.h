@@ -366,7 +366,9 @@ int hyq_cells_closure_eigs(const double* mom, int64_t n, double* v, void* stream
 /* collision35 (src/numerics/collision35.jl:154). */
 int hyq_cells_collision(const double* M, int64_t n, double dt, double Kn, int32_t positivity, double* out, void* stream);
 /* Phase [A] of the step (src/simulation_runner.jl:357-379): fluxes, realizable
- * moments and the six wave-speed arrays vp[6n] = (xmin,xmax,ymin,ymax,zmin,zmax). */
+ * moments and the six wave-speed arrays vp[6n] = (xmin,xmax,ymin,ymax,zmin,zmax).
+ * Runs as a chain of per-function kernels on `stream` that keep their
+ * intermediate states in the output arrays, so M must not overlap them. */
 int hyq_cells_phase_A(const double* M, int64_t n, int32_t flag2D, double Ma, int32_t positivity, double* Fx, double* Fy,
                       double* Fz, double* Mr, double* vp, void* stream);
 
