@@ -1,0 +1,158 @@
+"""The reference's own property tests of the wave speeds, on this code.
+
+test/test_eigenvalue_ordering.jl and test/test_z_eigenvalue_fix.jl of the
+reference check eigenvalues6_hyperbolic_3D, eigenvalues6z_hyperbolic_3D and
+closure_and_eigenvalues on Gaussian moment sets (InitializeM4_35) for their
+ordering, symmetry, bounds and high-Mach stability.  The same cases and the
+same assertions run here on the oracle; the device code compiled for the host
+and the GPU's per-cell entry points must give the oracle's numbers bit for
+bit on every case.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle_lib as ol
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(os.path.dirname(HERE), "hyqmom.jl_b200", "csrc")
+SQ3 = np.sqrt(3.0)
+
+
+def gaussian(u, v, w, rho=1.0, T=1.0):
+    """InitializeM4_35(rho, u, v, w, T, 0, 0, T, 0, T) (isotropic Gaussian)."""
+    return ol.initialize_m4_35(rho, u, v, w, T, 0.0, 0.0, T, 0.0, T)
+
+
+def speeds(M, Ma):
+    """(x, y, z) extreme speeds of the oracle, flag2D = 0, positivity on."""
+    x = ol.eigenvalues6(M, 1, 0, Ma)[:2]
+    y = ol.eigenvalues6(M, 2, 0, Ma)[:2]
+    z = ol.eigenvalues6z(M, 0, Ma)[:2]
+    return x, y, z
+
+
+# (u, v, w, Ma) of every eigenvalue case of the two reference files
+CASES = {
+    "ordering": (5.0, 3.0, -2.0, 6.0),
+    "symmetric": (50.0, 50.0, 50.0, SQ3 * 50.0),
+    "bounded": (10.0, 0.0, 0.0, 10.0),
+    "high_mach": (100.0, 0.0, 0.0, 100.0),
+    "rest": (0.0, 0.0, 0.0, 0.0),
+    "sign_pos": (20.0, 0.0, 0.0, 20.0),
+    "sign_neg": (-20.0, 0.0, 0.0, 20.0),
+    "z_consistency": (10.0, 5.0, 15.0, float(np.sqrt(10.0 ** 2 + 5.0 ** 2 + 15.0 ** 2))),
+    "z_fix": (40.0, 40.0, -40.0, 70.0),
+    "z_high_mach": (150.0 / SQ3, 150.0 / SQ3, -150.0 / SQ3, 150.0),
+}
+
+
+def test_eigenvalue_ordering_properties():
+    """test/test_eigenvalue_ordering.jl, each testset's assertions."""
+    # eigenvalues sorted correctly
+    for lo, hi in speeds(gaussian(5.0, 3.0, -2.0), 6.0):
+        assert lo <= hi
+    # symmetric flow: the three directions within 10 %
+    (xl, xh), (yl, yh), (zl, zh) = speeds(gaussian(50.0, 50.0, 50.0), SQ3 * 50.0)
+    for a, b in ((xh, yh), (xh, zh), (yh, zh), (xl, yl), (xl, zl), (yl, zl)):
+        assert np.isclose(a, b, rtol=0.1, atol=0.0)
+    # bounded by the flow velocity and the sound speed
+    u, c = 10.0, 1.0
+    lo, hi = ol.eigenvalues6(gaussian(u, 0.0, 0.0), 1, 0, 10.0)[:2]
+    assert u < hi < 5.0 * (abs(u) + c)
+    assert -5.0 * (abs(u) + c) < lo < u
+    # high Mach number: finite, not pathological
+    lo, hi = ol.eigenvalues6(gaussian(100.0, 0.0, 0.0), 1, 0, 100.0)[:2]
+    assert np.isfinite(lo) and np.isfinite(hi) and abs(hi) < 1e4 and abs(lo) < 1e4
+    # at rest: symmetric about zero, of the order of the sound speed
+    lo, hi = ol.eigenvalues6(gaussian(0.0, 0.0, 0.0), 1, 0, 0.0)[:2]
+    assert abs(lo + hi) < 1.0 and abs(hi) < 5.0
+    # sign consistency
+    assert ol.eigenvalues6(gaussian(20.0, 0.0, 0.0), 1, 0, 20.0)[1] > 0.0
+    assert ol.eigenvalues6(gaussian(-20.0, 0.0, 0.0), 1, 0, 20.0)[0] < 0.0
+    # z consistent with x and y
+    u, v, w, Ma = CASES["z_consistency"]
+    sp = speeds(gaussian(u, v, w), Ma)
+    assert all(np.isfinite(s).all() for s in sp)
+    mx = [abs(s[1]) for s in sp]
+    assert max(mx) / min(mx) < 10.0
+
+
+def test_closure_eigenvalues_bounded_by_velocity():
+    """test/test_eigenvalue_ordering.jl, "1D closure eigenvalues"."""
+    rho, u, T = 1.0, 5.0, 1.0
+    mom = [rho, rho * u, rho * (u * u + T), rho * (u ** 3 + 3 * u * T), rho * (u ** 4 + 6 * u * u * T + 3 * T * T)]
+    _, lo, hi = ol.closure_and_eigenvalues(mom)
+    assert np.isfinite(lo) and np.isfinite(hi) and lo <= hi
+    assert hi > u and lo < u
+
+
+def test_z_eigenvalue_regression_properties():
+    """test/test_z_eigenvalue_fix.jl: the WV Jacobian's moment ordering keeps
+    the z speeds physical (the reference's bug gave ~3.3e5)."""
+    u, v, w, Ma = CASES["z_fix"]
+    (xl, xh), (yl, yh), (zl, zh) = speeds(gaussian(u, v, w), Ma)
+    assert np.isfinite(zl) and np.isfinite(zh)
+    assert abs(zh) < 5000.0 and abs(zl) < 5000.0 and abs(zh) < 5.0 * abs(Ma)
+    assert abs(xh) < 5000.0 and abs(yh) < 5000.0
+    mx = [abs(xh), abs(yh), abs(zh)]
+    if min(mx) > 1.0:
+        assert max(mx) / min(mx) < 10.0
+    u, v, w, Ma = CASES["z_high_mach"]
+    zl, zh = ol.eigenvalues6z(gaussian(u, v, w), 0, Ma)[:2]
+    assert np.isfinite(zh) and abs(zh) < 1e4 and abs(zh) < 50.0 * Ma
+
+
+@pytest.fixture(scope="module")
+def shim(tmp_path_factory):
+    out = tmp_path_factory.mktemp("shim_props") / "libshim.so"
+    subprocess.check_call(["/usr/bin/g++", "-O2", "-std=c++17", "-fno-fast-math", "-ffp-contract=off", "-fPIC", "-shared",
+                           "-I", CSRC, "-o", str(out), os.path.join(HERE, "host_device_shim.cpp")])
+    return ctypes.CDLL(str(out))
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def test_device_code_on_host_gives_the_oracle_speeds(shim):
+    """The device source compiled for the host, on every case and axis: the
+    oracle's speeds and realized moments, bit for bit."""
+    for name, (u, v, w, Ma) in CASES.items():
+        M = np.ascontiguousarray(gaussian(u, v, w))
+        for axis in (1, 2, 3):
+            vv, Mr = np.zeros(2), np.zeros(35)
+            shim.sh_eig(_p(M), ctypes.c_int(axis), ctypes.c_int(0), ctypes.c_double(Ma), ctypes.c_int(1), _p(vv), _p(Mr))
+            lo, hi, Mo = ol.eigenvalues6z(M, 0, Ma) if axis == 3 else ol.eigenvalues6(M, axis, 0, Ma)
+            assert vv[0] == lo and vv[1] == hi, (name, axis, vv, lo, hi)
+            assert np.array_equal(Mr, Mo), (name, axis)
+
+
+@pytest.mark.gpu
+def test_gpu_cells_give_the_oracle_speeds():
+    """hyq_cells_eigenvalues on all cases at once (one cell each): the
+    oracle's speeds and realized moments, bit for bit."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from hyqmom import _lib
+    lib = _lib.load()
+    names = list(CASES)
+    for Ma in sorted({c[3] for c in CASES.values()}):
+        rows = [n for n in names if CASES[n][3] == Ma]
+        states = np.array([gaussian(*CASES[n][:3]) for n in rows])
+        n = len(rows)
+        dM = torch.tensor(np.ascontiguousarray(states.T), dtype=torch.float64, device="cuda")
+        for axis in (1, 2, 3):
+            v = torch.empty(2, n, dtype=torch.float64, device="cuda")
+            Mr = torch.empty_like(dM)
+            assert lib.hyq_cells_eigenvalues(dM.data_ptr(), n, axis, 0, Ma, 1, v.data_ptr(), Mr.data_ptr(), None) == 0
+            torch.cuda.synchronize()
+            gv, gM = v.cpu().numpy(), Mr.cpu().numpy().T
+            for k, name in enumerate(rows):
+                lo, hi, Mo = ol.eigenvalues6z(states[k], 0, Ma) if axis == 3 else ol.eigenvalues6(states[k], axis, 0, Ma)
+                assert gv[0, k] == lo and gv[1, k] == hi, (name, axis)
+                assert np.array_equal(gM[k], Mo), (name, axis)
