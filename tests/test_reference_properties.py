@@ -1,12 +1,14 @@
-"""The reference's own property tests of the wave speeds, on this code.
+"""The reference's own property tests of the per-cell functions, on this code.
 
 test/test_eigenvalue_ordering.jl and test/test_z_eigenvalue_fix.jl of the
 reference check eigenvalues6_hyperbolic_3D, eigenvalues6z_hyperbolic_3D and
 closure_and_eigenvalues on Gaussian moment sets (InitializeM4_35) for their
-ordering, symmetry, bounds and high-Mach stability.  The same cases and the
-same assertions run here on the oracle; the device code compiled for the host
-and the GPU's per-cell entry points must give the oracle's numbers bit for
-bit on every case.
+ordering, symmetry, bounds and high-Mach stability; test/test_closures.jl and
+test/test_realizability.jl check the closure's output, its mass and the
+realizability_S2 projection.  The same cases and the same assertions run here
+on the oracle; the device code compiled for the host and the GPU's per-cell
+entry points must give the oracle's numbers bit for bit on the wave-speed
+cases.
 """
 import ctypes
 import os
@@ -104,6 +106,45 @@ def test_z_eigenvalue_regression_properties():
     u, v, w, Ma = CASES["z_high_mach"]
     zl, zh = ol.eigenvalues6z(gaussian(u, v, w), 0, Ma)[:2]
     assert np.isfinite(zh) and abs(zh) < 1e4 and abs(zh) < 50.0 * Ma
+
+
+def test_closure_properties():
+    """test/test_closures.jl, each testset's assertions."""
+    _, lo, hi = ol.closure_and_eigenvalues([1.0, 0.1, 1.2, 0.15, 3.5])
+    assert np.isfinite(lo) and np.isfinite(hi) and lo <= hi
+    # the closure's output is finite (3-D and 2-D mode) and keeps the mass
+    for rho, (u, v, w), T, flag2D, Ma in ((1.0, (0.1, 0.0, 0.0), 1.0, 0, 2.0), (0.8, (0.0, 0.1, 0.0), 1.2, 1, 0.5)):
+        M4 = gaussian(u, v, w, rho=rho, T=T)
+        for out in ol.flux_closure35(M4, flag2D, Ma):
+            assert out.shape == (35,) and np.isfinite(out).all()
+    M4 = gaussian(0.0, 0.0, 0.0, rho=2.0, T=1.5)
+    assert abs(ol.flux_closure35(M4, 0, 2.0)[3][0] - M4[0]) <= 1e-10
+    # eigenvalues along each axis (axis 3 is the y pair, as in the
+    # reference's compute_eigenvalues_for_axis) and in 2-D mode
+    lo, hi = ol.eigenvalues6(gaussian(0.1, 0.2, 0.3), 1, 0, 2.0)[:2]
+    assert np.isfinite(lo) and np.isfinite(hi) and lo <= hi
+    M4 = gaussian(0.2, -0.1, 0.05, T=0.8)
+    for axis in (1, 2, 3):
+        for flag2D in (0, 1):
+            lo, hi = ol.eigenvalues6(M4, axis, flag2D, 1.5)[:2]
+            assert np.isfinite(lo) and np.isfinite(hi) and lo <= hi
+    assert ol.eigenvalues6(M4, 3, 0, 1.5)[:2] == ol.eigenvalues6(M4, 2, 0, 1.5)[:2]
+
+
+def test_realizability_S2_properties():
+    """test/test_realizability.jl: realizability_S2 basic, Gaussian moments
+    unchanged, finiteness near the corner."""
+    tol = 1e-10
+    for corr in ((0.5, 0.3, 0.4), (-0.8, -0.6, -0.7), (0.99, 0.98, 0.97)):
+        r = ol.realizability_S2(*corr)
+        assert np.isfinite(r).all() and all(abs(x) <= 1.0 + tol for x in r[:3]) and r[3] >= 0.0
+    r = ol.realizability_S2(0.0, 0.0, 0.0)
+    assert r[0] == 0.0 and r[1] == 0.0 and r[2] == 0.0 and np.isfinite(r[3])
+    assert np.isfinite(ol.realizability_S2(1.5, 1.5, 1.5)).all()
+    _, S4 = ol.m2cs4_35(gaussian(0.0, 0.0, 0.0))
+    S110, S101, S011 = S4[6], S4[16], S4[25]
+    r = ol.realizability_S2(S110, S101, S011)
+    assert abs(r[0] - S110) <= tol and abs(r[1] - S101) <= tol and abs(r[2] - S011) <= tol
 
 
 @pytest.fixture(scope="module")
