@@ -5,7 +5,9 @@ reference check eigenvalues6_hyperbolic_3D, eigenvalues6z_hyperbolic_3D and
 closure_and_eigenvalues on Gaussian moment sets (InitializeM4_35) for their
 ordering, symmetry, bounds and high-Mach stability; test/test_closures.jl and
 test/test_realizability.jl check the closure's output, its mass and the
-realizability_S2 projection.  The same cases and the same assertions run here
+realizability_S2 projection; test/test_numerical_schemes.jl the HLL update
+of a row and the BGK collision; test/test_moment_conversions.jl the central
+and standardized moments of Gaussians.  The same cases and the same assertions run here
 on the oracle; the device code compiled for the host and the GPU's per-cell
 entry points must give the oracle's numbers bit for bit on the wave-speed
 cases.
@@ -145,6 +147,42 @@ def test_realizability_S2_properties():
     S110, S101, S011 = S4[6], S4[16], S4[25]
     r = ol.realizability_S2(S110, S101, S011)
     assert abs(r[0] - S110) <= tol and abs(r[1] - S101) <= tol and abs(r[2] - S011) <= tol
+
+
+def test_numerical_schemes_properties():
+    """test/test_numerical_schemes.jl: pas_HLL on a uniform row (the
+    reference's 5 moments become the step's 35), collision35 keeps the mass
+    and moves a perturbed moment."""
+    Nx = 10
+    M = np.ones((Nx, 35))
+    Mp = ol.pas_hll(M, 0.1 * M, 0.01, 0.1, -np.ones(Nx), np.ones(Nx))
+    assert Mp.shape == M.shape and np.isfinite(Mp).all()
+    M = gaussian(0.1, 0.2, 0.3)
+    for dt, Kn in ((0.001, 0.01), (0.01, 0.001)):  # the reference test passes (Kn, dt) positionally
+        Mn = ol.collision35(M, dt, Kn)
+        assert Mn.shape == (35,) and np.isfinite(Mn).all() and abs(Mn[0] - M[0]) <= 1e-10
+    M = gaussian(0.0, 0.0, 0.0)
+    M[10] += 0.1  # the reference's M[11] (1-based)
+    assert abs(ol.collision35(M, 0.1, 0.01)[10] - M[10]) > 0.0
+
+
+def test_moment_conversion_properties():
+    """test/test_moment_conversions.jl: M2CS4_35 of Gaussians (variances T,
+    S400 = S040 = S004 = 3, correlations within [-1, 1]), finite for
+    correlated covariances, InitializeM4_35 with correlations."""
+    tol = 1e-10
+    T = 1.5
+    C4, S4 = ol.m2cs4_35(gaussian(0.1, 0.2, 0.3, T=T))
+    assert abs(C4[2] - T) <= tol and abs(C4[9] - T) <= tol and abs(C4[19] - T) <= tol
+    assert abs(S4[4] - 3.0) <= tol and abs(S4[14] - 3.0) <= tol and abs(S4[24] - 3.0) <= tol
+    _, S4 = ol.m2cs4_35(gaussian(0.0, 0.0, 0.0))
+    assert all(abs(S4[k]) <= 1.0 + tol for k in (6, 16, 25))
+    M = ol.initialize_m4_35(1.5, 0.3, -0.2, 0.4, 1.2, 0.3, -0.1, 1.5, 0.2, 1.8)
+    C4, S4 = ol.m2cs4_35(M)
+    assert abs(M[0] - 1.5) <= tol and np.isfinite(C4).all() and np.isfinite(S4).all()
+    for r in (0.0, 0.3, 0.6, 0.9, -0.3, -0.6):
+        M = ol.initialize_m4_35(1.0, 0.0, 0.0, 0.0, 1.0, r, r, 1.0, r, 1.0)
+        assert M.shape == (35,) and np.isfinite(M).all() and abs(M[0] - 1.0) <= tol
 
 
 @pytest.fixture(scope="module")
