@@ -6,8 +6,8 @@ closure_and_eigenvalues on Gaussian moment sets (InitializeM4_35) for their
 ordering, symmetry, bounds and high-Mach stability; test/test_closures.jl and
 test/test_realizability.jl check the closure's output, its mass and the
 realizability_S2 projection; test/test_numerical_schemes.jl the HLL update
-of a row and the BGK collision; test/test_moment_conversions.jl the central
-and standardized moments of Gaussians.  The same cases and the same assertions run here
+of a row and the BGK collision; test/test_moment_conversions.jl and
+test/test_realizability_bounds.jl the moments of Gaussians.  The same cases and the same assertions run here
 on the oracle; the device code compiled for the host and the GPU's per-cell
 entry points must give the oracle's numbers bit for bit on the wave-speed
 cases.
@@ -183,6 +183,31 @@ def test_moment_conversion_properties():
     for r in (0.0, 0.3, 0.6, 0.9, -0.3, -0.6):
         M = ol.initialize_m4_35(1.0, 0.0, 0.0, 0.0, 1.0, r, r, 1.0, r, 1.0)
         assert M.shape == (35,) and np.isfinite(M).all() and abs(M[0] - 1.0) <= tol
+
+
+def test_realizability_bounds_properties():
+    """test/test_realizability_bounds.jl: InitializeM4_35 moments (density,
+    variances, Cauchy-Schwarz, fourth moments, ordering, zero velocity) and
+    the 1-D closure's fifth moment."""
+    M = gaussian(10.0, 5.0, -3.0, rho=1.5)
+    assert M[0] > 0 and M[0] == 1.5
+    T = 2.0
+    M = gaussian(10.0, 5.0, -3.0, T=T)
+    for k, vel in ((2, 10.0), (9, 5.0), (19, -3.0)):  # M200, M020, M002
+        var = M[k] - vel ** 2
+        assert var > 0 and abs(var - T) <= 1e-10 * T
+    M = gaussian(10.0, 5.0, 0.0)
+    assert M[6] ** 2 <= M[2] * M[9] and M[16] ** 2 <= M[2] * M[19] and M[25] ** 2 <= M[9] * M[19]
+    M = gaussian(5.0, 0.0, 0.0)
+    assert np.isfinite(M).all() and M[4] > 0 and M[14] > 0 and M[24] > 0
+    M = gaussian(10.0, 0.0, 0.0)
+    assert M[1] / M[0] > 1.0 and M[2] / M[1] > 1.0
+    M = gaussian(0.0, 0.0, 0.0)
+    assert abs(M[0] - 1.0) <= 1e-12 and all(abs(M[k]) <= 1e-10 for k in (1, 5, 15))
+    assert all(abs(M[k] - 1.0) <= 1e-12 for k in (2, 9, 19))
+    u, T = 5.0, 1.0
+    Mp, lo, hi = ol.closure_and_eigenvalues([1.0, u, u * u + T, u ** 3 + 3 * u * T, u ** 4 + 6 * u * u * T + 3 * T * T])
+    assert Mp >= 0 and np.isfinite(Mp) and np.isfinite(lo) and np.isfinite(hi)
 
 
 @pytest.fixture(scope="module")
