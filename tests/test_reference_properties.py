@@ -7,7 +7,9 @@ ordering, symmetry, bounds and high-Mach stability; test/test_closures.jl and
 test/test_realizability.jl check the closure's output, its mass and the
 realizability_S2 projection; test/test_numerical_schemes.jl the HLL update
 of a row and the BGK collision; test/test_moment_conversions.jl and
-test/test_realizability_bounds.jl the moments of Gaussians.  The same cases and the same assertions run here
+test/test_realizability_bounds.jl the moments of Gaussians;
+test/test_numerical_accuracy.jl determinism, mirror symmetry of the speeds
+and tiny or large states.  The same cases and the same assertions run here
 on the oracle; the device code compiled for the host and the GPU's per-cell
 entry points must give the oracle's numbers bit for bit on the wave-speed
 cases.
@@ -208,6 +210,27 @@ def test_realizability_bounds_properties():
     u, T = 5.0, 1.0
     Mp, lo, hi = ol.closure_and_eigenvalues([1.0, u, u * u + T, u ** 3 + 3 * u * T, u ** 4 + 6 * u * u * T + 3 * T * T])
     assert Mp >= 0 and np.isfinite(Mp) and np.isfinite(lo) and np.isfinite(hi)
+
+
+def test_numerical_accuracy_properties():
+    """test/test_numerical_accuracy.jl: small perturbations stay small,
+    tiny and large states stay finite, the speeds are deterministic and
+    mirror-symmetric (max at +u = -min at -u), convex mixtures of Gaussians
+    keep a positive density and variance."""
+    M1 = gaussian(5.0, 0.0, 0.0)
+    M2 = ol.initialize_m4_35(1.0 + 1e-14, 5.0, 0.0, 0.0, 1.0, 0.0, 0.0, 1.0, 0.0, 1.0)
+    assert np.max(np.abs(M2 - M1)) < 1e-10
+    for M in (gaussian(0.0, 0.0, 0.0, rho=1e-10), gaussian(1000.0, 0.0, 0.0)):
+        assert np.isfinite(M).all() and M[0] > 0
+    M = gaussian(10.0, 0.0, 0.0)
+    a, b = ol.eigenvalues6(M, 1, 0, 10.0)[:2], ol.eigenvalues6(M, 1, 0, 10.0)[:2]
+    assert a == b
+    lo_p, hi_p = ol.eigenvalues6(gaussian(5.0, 0.0, 0.0), 1, 0, 5.0)[:2]
+    lo_n, hi_n = ol.eigenvalues6(gaussian(-5.0, 0.0, 0.0), 1, 0, 5.0)[:2]
+    assert np.isclose(hi_p, -lo_n, rtol=1e-10, atol=0.0) and np.isclose(lo_p, -hi_n, rtol=1e-10, atol=0.0)
+    M1, M2 = gaussian(3.0, 0.0, 0.0), gaussian(7.0, 0.0, 0.0, rho=1.5)
+    Mm = 0.6 * M1 + 0.4 * M2
+    assert Mm[0] > 0 and np.isfinite(Mm).all() and Mm[2] / Mm[0] - (Mm[1] / Mm[0]) ** 2 > 0
 
 
 @pytest.fixture(scope="module")
