@@ -41,7 +41,7 @@ def speeds(M, Ma):
     return x, y, z
 
 
-# (u, v, w, Ma) of every eigenvalue case of the two reference files
+# (u, v, w, Ma) of the eigenvalue cases of the reference's property tests
 CASES = {
     "ordering": (5.0, 3.0, -2.0, 6.0),
     "symmetric": (50.0, 50.0, 50.0, SQ3 * 50.0),
@@ -53,6 +53,9 @@ CASES = {
     "z_consistency": (10.0, 5.0, 15.0, float(np.sqrt(10.0 ** 2 + 5.0 ** 2 + 15.0 ** 2))),
     "z_fix": (40.0, 40.0, -40.0, 70.0),
     "z_high_mach": (150.0 / SQ3, 150.0 / SQ3, -150.0 / SQ3, 150.0),
+    "mirror_pos": (5.0, 0.0, 0.0, 5.0),
+    "mirror_neg": (-5.0, 0.0, 0.0, 5.0),
+    "large": (1000.0, 0.0, 0.0, 1000.0),
 }
 
 
