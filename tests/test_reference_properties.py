@@ -9,7 +9,8 @@ realizability_S2 projection; test/test_numerical_schemes.jl the HLL update
 of a row and the BGK collision; test/test_moment_conversions.jl and
 test/test_realizability_bounds.jl the moments of Gaussians;
 test/test_numerical_accuracy.jl determinism, mirror symmetry of the speeds
-and tiny or large states.  The same cases and the same assertions run here
+and tiny or large states; test/test_initial_conditions.jl the IC regions
+(here on the host IC module, hyqmom.ic).  The same cases and the same assertions run here
 on the oracle; the device code compiled for the host and the GPU's per-cell
 entry points must give the oracle's numbers bit for bit on the wave-speed
 cases.
@@ -234,6 +235,32 @@ def test_numerical_accuracy_properties():
     M1, M2 = gaussian(3.0, 0.0, 0.0), gaussian(7.0, 0.0, 0.0, rho=1.5)
     Mm = 0.6 * M1 + 0.4 * M2
     assert Mm[0] > 0 and np.isfinite(Mm).all() and Mm[2] / Mm[0] - (Mm[1] / Mm[0]) ** 2 > 0
+
+
+def test_initial_condition_region_properties():
+    """test/test_initial_conditions.jl: CubicRegion's default temperature,
+    region_to_moments (density kept, finite with correlations) and
+    cell_overlaps_cube (strict overlap; an infinite background overlaps
+    everything), with the reference's cases."""
+    from hyqmom import ic
+    inf = float("inf")
+    assert ic.CubicRegion((0.0, 0.0, 0.0), (0.1, 0.1, 0.1), 1.0, (0.0, 0.0, 0.0)).temperature == 1.0
+    region = ic.CubicRegion((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), 1.0, (0.0, 0.0, 0.0), 1.0)
+    Mr = ic.region_to_moments(region, 0.0, 0.0, 0.0)
+    assert len(Mr) == 35 and np.isfinite(Mr).all() and np.isclose(Mr[0], 1.0)
+    moving = ic.CubicRegion((0.0, 0.0, 0.0), (1.0, 1.0, 1.0), 2.0, (1.0, 0.5, 0.0), 0.5)
+    Mr = ic.region_to_moments(moving, 0.0, 0.0, 0.0)
+    assert len(Mr) == 35 and np.isfinite(Mr).all() and np.isclose(Mr[0], 2.0)
+    assert np.isfinite(ic.region_to_moments(region, 0.1, 0.2, 0.3)).all()
+    cube = ic.CubicRegion((0.0, 0.0, 0.0), (0.2, 0.2, 0.2), 1.0, (0.0, 0.0, 0.0), 1.0)
+    cs = (0.1, 0.1, 0.1)
+    assert ic.cell_overlaps_cube((0.0, 0.0, 0.0), cs, cube)
+    assert ic.cell_overlaps_cube((0.05, 0.05, 0.05), cs, cube)
+    assert ic.cell_overlaps_cube((0.15, 0.0, 0.0), cs, cube)
+    assert not ic.cell_overlaps_cube((0.5, 0.0, 0.0), cs, cube)
+    assert not ic.cell_overlaps_cube((0.0, 0.5, 0.0), cs, cube)
+    background = ic.CubicRegion((0.0, 0.0, 0.0), (inf, inf, inf), 0.01, (0.0, 0.0, 0.0), 1.0)
+    assert ic.cell_overlaps_cube((100.0, 100.0, 100.0), cs, background)
 
 
 @pytest.fixture(scope="module")
