@@ -9,7 +9,7 @@ realizability_S2 projection; test/test_numerical_schemes.jl the HLL update
 of a row and the BGK collision; test/test_moment_conversions.jl and
 test/test_realizability_bounds.jl the moments of Gaussians;
 test/test_numerical_accuracy.jl determinism, mirror symmetry of the speeds
-and tiny or large states; test/test_initial_conditions.jl the IC regions
+and tiny or large states; test/test_initialization.jl InitializeM4_35; test/test_initial_conditions.jl the IC regions
 (here on the host IC module, hyqmom.ic).  The same cases and the same assertions run here
 on the oracle; the device code compiled for the host and the GPU's per-cell
 entry points must give the oracle's numbers bit for bit on the wave-speed
@@ -261,6 +261,28 @@ def test_initial_condition_region_properties():
     assert not ic.cell_overlaps_cube((0.0, 0.5, 0.0), cs, cube)
     background = ic.CubicRegion((0.0, 0.0, 0.0), (inf, inf, inf), 0.01, (0.0, 0.0, 0.0), 1.0)
     assert ic.cell_overlaps_cube((100.0, 100.0, 100.0), cs, background)
+
+
+def test_initialization_properties():
+    """test/test_initialization.jl: InitializeM4_35's mean, variances,
+    correlation, kurtosis 3 and vanishing odd standardized moments."""
+    tol = 1e-10
+    rho, u, v, w, T = 1.5, 0.1, 0.2, 0.3, 2.0
+    M = ol.initialize_m4_35(rho, u, v, w, T, 0.0, 0.0, T, 0.0, T)
+    assert abs(M[0] - rho) <= tol and abs(M[1] / M[0] - u) <= tol and abs(M[5] / M[0] - v) <= tol and abs(M[15] / M[0] - w) <= tol
+    _, S4 = ol.m2cs4_35(M)
+    assert all(abs(S4[k] - 3.0) <= tol for k in (4, 14, 24))
+    C200, C020, C002, C110, C101, C011 = 1.0, 1.5, 2.0, 0.5, 0.3, 0.6
+    C4, S4 = ol.m2cs4_35(ol.initialize_m4_35(1.0, 0.0, 0.0, 0.0, C200, C110, C101, C020, C011, C002))
+    assert abs(C4[2] - C200) <= tol and abs(C4[9] - C020) <= tol and abs(C4[19] - C002) <= tol
+    assert abs(S4[6] - C110 / np.sqrt(C200 * C020)) <= tol
+    assert abs(ol.initialize_m4_35(3.0, 0.0, 0.0, 0.0, 1.5, 0.0, 0.0, 1.5, 0.0, 1.5)[0] - 3.0) <= tol
+    _, S4 = ol.m2cs4_35(gaussian(0.0, 0.0, 0.0))
+    odd = [4, 8, 9, 11, 13, 18, 19, 21, 23, 24, 27, 28, 29, 30, 31, 32, 33, 34]  # the reference's 1-based list
+    assert all(abs(S4[k - 1]) < tol for k in odd)
+    M = gaussian(0.5, -0.3, 0.1, rho=2.0)
+    C4, _ = ol.m2cs4_35(M)
+    assert M[0] > 0 and np.isfinite(M).all() and C4[2] > 0 and C4[9] > 0 and C4[19] > 0
 
 
 @pytest.fixture(scope="module")
