@@ -283,6 +283,10 @@ def test_initialization_properties():
     M = gaussian(0.5, -0.3, 0.1, rho=2.0)
     C4, _ = ol.m2cs4_35(M)
     assert M[0] > 0 and np.isfinite(M).all() and C4[2] > 0 and C4[9] > 0 and C4[19] > 0
+    # test/test_conservation.jl, "Symmetry preservation": equal velocities give
+    # equal second moments
+    M = gaussian(5.0, 5.0, 5.0)
+    assert np.isclose(M[2], M[9], rtol=1e-10, atol=0.0) and np.isclose(M[2], M[19], rtol=1e-10, atol=0.0)
 
 
 @pytest.fixture(scope="module")
