@@ -48,3 +48,15 @@ def test_timed_steps_spread_over_the_run():
     assert bench.timed_steps(500, 1) == [500]
     assert bench.timed_steps(200, 3) == [67, 133, 200]
     assert bench.timed_steps(10, 50) == list(range(1, 11))
+
+
+def test_traffic_tables_cover_every_slot_and_launch_variant():
+    """The roofline's DRAM-traffic tables have an entry for every timed slot
+    with per-cell kernels and for every HLL launch variant the library offers
+    (the autotuner may pick any of them on the bench's workload)."""
+    from hyqmom import _lib
+    lib = _lib.load()
+    per_cell = set(bench.KERNELS) - {"cfl", "hll"}
+    assert set(bench.TRAFFIC_PER_CELL) == per_cell
+    assert set(bench.TRAFFIC_HLL) == set(range(lib.hyq_variant_count(_lib.KERNEL_HLL)))
+    assert all(v > bench.B_ALG / 2 for v in bench.TRAFFIC_PER_CELL.values())
